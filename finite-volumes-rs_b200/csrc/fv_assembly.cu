@@ -1,0 +1,472 @@
+// Mesh upload, CSR pattern and matrix assembly on the device.
+//
+// Reference: fvm::assembly::assemble (src/fvm/assembly.rs:11-78), the pattern
+// of DistributedMatrix::from_cut_sparsity over Mesh::cell_to_cell
+// (src/linalg/dmatrix.rs:38-50, src/core/mesh/compute.rs:135-152), the terms
+// laplacian/convection/source (src/fvm/terms/*.rs) with the Orthogonal and
+// Upwind schemes (src/fvm/schemes/facengrad/orthogonal.rs:26-46,
+// src/fvm/schemes/faceinterp/upwind.rs:26-33).
+//
+// Design: one thread per cell assembles its whole CSR row.  The cell's faces
+// are visited in ascending face id -- the order in which the reference's face
+// loop touches that row -- so the diagonal, the off-diagonals and the rhs get
+// exactly the reference's sequence of additions, with no atomics and no
+// face->nnz map.  A face's coefficients are recomputed by both of its cells
+// (identical arithmetic, identical bits); the second read of its data hits L2
+// because face ids follow element order.
+#include <algorithm>
+#include <cub/device/device_scan.cuh>
+#include <vector>
+
+#include "fv_internal.cuh"
+
+namespace {
+
+template <int MAXF>
+__device__ __forceinline__ int row_pattern(int i, int s, int e, const int32_t *__restrict__ cf_other,
+                                           int (&c)[MAXF + 1]) {
+    int n = 0;
+    c[n++] = i;
+    for (int k = s; k < e; ++k) {
+        int j = cf_other[k];
+        if (j < 0) continue;
+        bool dup = false;
+        for (int q = 1; q < n; ++q) dup |= (c[q] == j);
+        if (!dup && n < MAXF + 1) c[n++] = j;
+    }
+    for (int a = 1; a < n; ++a) {  // insertion sort, n <= MAXF+1
+        int v = c[a];
+        int b = a - 1;
+        while (b >= 0 && c[b] > v) {
+            c[b + 1] = c[b];
+            --b;
+        }
+        c[b + 1] = v;
+    }
+    return n;
+}
+
+template <int MAXF>
+__global__ void k_row_count(int64_t n, const int32_t *__restrict__ cf_ptr, const int32_t *__restrict__ cf_other,
+                            int32_t *__restrict__ len) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[MAXF + 1];
+    len[i] = row_pattern<MAXF>((int)i, cf_ptr[i], cf_ptr[i + 1], cf_other, c);
+}
+
+template <int MAXF>
+__global__ void k_row_fill(int64_t n, const int32_t *__restrict__ cf_ptr, const int32_t *__restrict__ cf_other,
+                           const int32_t *__restrict__ row_ptr, int32_t *__restrict__ cols) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[MAXF + 1];
+    int m = row_pattern<MAXF>((int)i, cf_ptr[i], cf_ptr[i + 1], cf_other, c);
+    int32_t *out = cols + row_ptr[i];
+    for (int q = 0; q < m; ++q) out[q] = c[q];
+}
+
+struct AssembleArgs {
+    int64_t n, fb0;
+    const int32_t *cf_ptr, *cf_face, *cf_other;
+    const double4 *cell, *bfc;
+    const double *area, *kappa, *flux, *src, *bndi, *bnde;
+    double c_lap, c_conv, c_src;
+    const int32_t *row_ptr;
+    double *vals, *rhs;
+};
+
+// Face coefficients (li, lj) before the area factor, exactly as the
+// reference's term tree evaluates them.
+__device__ __forceinline__ void face_terms(double t, double kappa, double F, double c_lap, double c_conv,
+                                           double &li, double &lj) {
+    double lap0 = 0.0, lap1 = 0.0, conv0 = 0.0, conv1 = 0.0;
+    if (c_lap != 0.0) {
+        lap0 = kappa * (-t);
+        lap1 = kappa * t;
+    }
+    if (c_conv != 0.0) {
+        if (F > 0.0) {
+            conv0 = 1.0 * F;
+            conv1 = 0.0 * F;
+        } else {
+            conv0 = 0.0 * F;
+            conv1 = 1.0 * F;
+        }
+    }
+    if (c_conv != 0.0 && c_lap != 0.0) {
+        li = c_conv * conv0 + c_lap * lap0;
+        lj = c_conv * conv1 + c_lap * lap1;
+    } else if (c_lap != 0.0) {
+        li = c_lap * lap0;
+        lj = c_lap * lap1;
+    } else {
+        li = c_conv * conv0;
+        lj = c_conv * conv1;
+    }
+}
+
+template <int DIM, int MAXF>
+__global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int s = a.cf_ptr[i], e = a.cf_ptr[i + 1];
+    int c[MAXF + 1];
+    const int m = row_pattern<MAXF>((int)i, s, e, a.cf_other, c);
+    double v[MAXF + 1];
+#pragma unroll
+    for (int q = 0; q < MAXF + 1; ++q) v[q] = 0.0;
+    int pd = 0;
+    for (int q = 0; q < m; ++q)
+        if (c[q] == (int)i) pd = q;
+    const double4 ci4 = a.cell[i];
+    const double V = ci4.w;
+    // cell loop (assembly.rs:26-32): no term in scope carries a cell lhs
+    const double lcell = 0.0;
+    const double rcell = a.c_src != 0.0 ? a.c_src * (-a.src[i]) : 0.0;
+    double diag = lcell * V;
+    double rhs = rcell * V;
+    for (int k = s; k < e; ++k) {
+        const int32_t fe = a.cf_face[k];
+        const bool is_nb = fe < 0;
+        const int f = fe & 0x7fffffff;
+        const int j = a.cf_other[k];
+        double3 pi, pj;  // owner centre, neighbour centre (or boundary face centre)
+        if (j >= 0) {
+            const double4 o4 = a.cell[j];
+            if (is_nb) {
+                pi = make_double3(o4.x, o4.y, o4.z);
+                pj = make_double3(ci4.x, ci4.y, ci4.z);
+            } else {
+                pi = make_double3(ci4.x, ci4.y, ci4.z);
+                pj = make_double3(o4.x, o4.y, o4.z);
+            }
+        } else {
+            const double4 b4 = a.bfc[f - a.fb0];
+            pi = make_double3(ci4.x, ci4.y, ci4.z);
+            pj = make_double3(b4.x, b4.y, b4.z);
+        }
+        double d2 = 0.0;
+        {
+            double dd = pj.x - pi.x;
+            d2 += dd * dd;
+            dd = pj.y - pi.y;
+            d2 += dd * dd;
+            if (DIM == 3) {
+                dd = pj.z - pi.z;
+                d2 += dd * dd;
+            }
+        }
+        const double t = 1.0 / sqrt(d2);
+        double li, lj;
+        face_terms(t, a.c_lap != 0.0 ? a.kappa[f] : 0.0, a.c_conv != 0.0 ? a.flux[f] : 0.0, a.c_lap, a.c_conv,
+                   li, lj);
+        const double A = a.area[f];
+        li = li * A;
+        lj = lj * A;
+        const double ra = 0.0 * A;
+        if (j < 0) {
+            const double bi = a.bndi[f - a.fb0], be = a.bnde[f - a.fb0];
+            diag += li;
+            diag += lj * bi;
+            rhs += ra - lj * be;
+        } else {
+            int pj_slot = 0;
+            for (int q = 0; q < m; ++q)
+                if (c[q] == j) pj_slot = q;
+            if (!is_nb) {  // this cell owns the face: lhs[[i,i]] += li; lhs[[i,j]] += lj; rhs[i] += r
+                diag += li;
+                for (int q = 0; q < MAXF + 1; ++q)
+                    if (q == pj_slot) v[q] += lj;
+                rhs += ra;
+            } else {  // neighbour side: lhs[[j,i]] -= li; lhs[[j,j]] -= lj; rhs[j] -= r
+                for (int q = 0; q < MAXF + 1; ++q)
+                    if (q == pj_slot) v[q] -= li;
+                diag -= lj;
+                rhs -= ra;
+            }
+        }
+    }
+    double *out = a.vals + a.row_ptr[i];
+    for (int q = 0; q < m; ++q) out[q] = (q == pd) ? diag : v[q];
+    a.rhs[i] = rhs;
+}
+
+template <int DIM, int MAXF>
+void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
+    const int B = 128;
+    k_assemble<DIM, MAXF><<<(unsigned)((a.n + B - 1) / B), B, 0, st>>>(a);
+}
+
+}  // namespace
+
+static thread_local char g_last_error[256];
+void fv_internal_set_cuda_error(cudaError_t e, const char *what) {
+    snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(e));
+}
+
+extern "C" const char *fv_last_error(void) { return g_last_error; }
+
+extern "C" const char *fv_status_string(fv_status s) {
+    switch (s) {
+    case FV_OK: return "FV_OK";
+    case FV_ERR_ALLOC: return "FV_ERR_ALLOC";
+    case FV_ERR_INVALID: return "FV_ERR_INVALID";
+    case FV_ERR_SINGULAR_PIVOT: return "FV_ERR_SINGULAR_PIVOT";
+    case FV_ERR_BREAKDOWN: return "FV_ERR_BREAKDOWN";
+    case FV_ERR_TIMEOUT: return "FV_ERR_TIMEOUT";
+    case FV_ERR_NOT_SYMMETRIC: return "FV_ERR_NOT_SYMMETRIC";
+    case FV_ERR_CUDA: return "FV_ERR_CUDA";
+    case FV_ERR_UNSUPPORTED: return "FV_ERR_UNSUPPORTED";
+    }
+    return "FV_ERR_UNKNOWN";
+}
+
+extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
+    if (!m) return FV_OK;
+    cudaFree(m->face_cells);
+    cudaFree(m->face_area);
+    cudaFree(m->bface_center);
+    cudaFree(m->cell);
+    cudaFree(m->cf_ptr);
+    cudaFree(m->cf_face);
+    cudaFree(m->cf_other);
+    cudaFree(m->row_ptr);
+    cudaFree(m->cols);
+    delete m;
+    return FV_OK;
+}
+
+extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh **out) {
+    if (!d || !out || (d->dim != 2 && d->dim != 3) || d->n_cells <= 0 || d->n_faces <= 0 || d->n_boundary_faces < 0 ||
+        d->n_boundary_faces > d->n_faces || !d->face_owner || !d->face_neighbor || !d->face_area ||
+        !d->cell_center || !d->cell_volume || (d->n_boundary_faces > 0 && !d->face_center) ||
+        d->n_cells >= 0x7fffffffLL || d->n_faces >= 0x7fffffffLL)
+        return FV_ERR_INVALID;
+    *out = nullptr;
+    const int dim = d->dim;
+    const int64_t N = d->n_cells, F = d->n_faces, Fb = d->n_boundary_faces, fb0 = F - Fb;
+    // validate connectivity; boundary faces must be the tail of the face list
+    std::vector<int32_t> cnt((size_t)N + 1, 0);
+    for (int64_t f = 0; f < F; ++f) {
+        int32_t o = d->face_owner[f], nb = d->face_neighbor[f];
+        if (o < 0 || o >= N || nb < -1 || nb >= N) return FV_ERR_INVALID;
+        if ((nb < 0) != (f >= fb0)) return FV_ERR_INVALID;
+        cnt[o + 1]++;
+        if (nb >= 0) cnt[nb + 1]++;
+    }
+    for (int64_t c = 0; c < N; ++c) cnt[c + 1] += cnt[c];
+    const int64_t ncf = cnt[N];
+    std::vector<int32_t> cff((size_t)ncf), cfo((size_t)ncf), fill(cnt.begin(), cnt.end() - 1);
+    for (int64_t f = 0; f < F; ++f) {  // ascending face id per cell by construction
+        int32_t o = d->face_owner[f], nb = d->face_neighbor[f];
+        int32_t k = fill[o]++;
+        cff[k] = (int32_t)f;
+        cfo[k] = nb;
+        if (nb >= 0) {
+            k = fill[nb]++;
+            cff[k] = (int32_t)f | (int32_t)0x80000000;
+            cfo[k] = o;
+        }
+    }
+    int maxf = 0;
+    for (int64_t c = 0; c < N; ++c) maxf = std::max(maxf, cnt[c + 1] - cnt[c]);
+    if (maxf > 16) return FV_ERR_UNSUPPORTED;
+    std::vector<double4> cell((size_t)N);
+    for (int64_t c = 0; c < N; ++c) {
+        const double *p = d->cell_center + c * dim;
+        cell[c] = make_double4(p[0], p[1], dim == 3 ? p[2] : 0.0, d->cell_volume[c]);
+    }
+    std::vector<double4> bfc((size_t)(Fb > 0 ? Fb : 1));
+    for (int64_t b = 0; b < Fb; ++b) {
+        const double *p = d->face_center + (fb0 + b) * dim;
+        bfc[b] = make_double4(p[0], p[1], dim == 3 ? p[2] : 0.0, 0.0);
+    }
+    std::vector<int2> fc((size_t)F);
+    for (int64_t f = 0; f < F; ++f) fc[f] = make_int2(d->face_owner[f], d->face_neighbor[f]);
+
+    fv_mesh *m = new fv_mesh();
+    m->dim = dim;
+    m->n_cells = N;
+    m->n_faces = F;
+    m->n_bfaces = Fb;
+    m->maxf = maxf;
+    cudaStream_t st = fv_stream(stream);
+    cudaError_t e = cudaSuccess;
+    e = cudaMalloc(&m->face_cells, sizeof(int2) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_area, sizeof(double) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->bface_center, sizeof(double4) * bfc.size());
+    if (e == cudaSuccess) e = cudaMalloc(&m->cell, sizeof(double4) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_ptr, sizeof(int32_t) * (N + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_face, sizeof(int32_t) * (ncf ? ncf : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_other, sizeof(int32_t) * (ncf ? ncf : 1));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->face_cells, fc.data(), sizeof(int2) * F, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->face_area, d->face_area, sizeof(double) * F, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->bface_center, bfc.data(), sizeof(double4) * bfc.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->cell, cell.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->cf_ptr, cnt.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && ncf)
+        e = cudaMemcpyAsync(m->cf_face, cff.data(), sizeof(int32_t) * ncf, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && ncf)
+        e = cudaMemcpyAsync(m->cf_other, cfo.data(), sizeof(int32_t) * ncf, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging vectors go out of scope
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "fv_mesh_upload");
+        fv_mesh_destroy(m);
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    *out = m;
+    return FV_OK;
+}
+
+// CSR pattern of cell_to_cell, rows sorted (DistributedMatrix::from_cut_sparsity).
+static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
+    const int64_t N = m->n_cells;
+    const int B = 256;
+    const unsigned G = (unsigned)((N + B - 1) / B);
+    int32_t *len = nullptr;
+    FV_CUDA_TRY(cudaMalloc(&m->row_ptr, sizeof(int32_t) * (N + 1)));
+    FV_CUDA_TRY(cudaMallocAsync(&len, sizeof(int32_t) * (N + 1), st));
+    FV_CUDA_TRY(cudaMemsetAsync(len + N, 0, sizeof(int32_t), st));
+    const int mf = m->maxf;
+    if (mf <= 4)
+        k_row_count<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+    else if (mf <= 8)
+        k_row_count<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+    else
+        k_row_count<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+    FV_CUDA_TRY(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, len, m->row_ptr, (int)(N + 1), st);
+    void *tmp = nullptr;
+    FV_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+    FV_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, len, m->row_ptr, (int)(N + 1), st));
+    int32_t nnz = 0;
+    FV_CUDA_TRY(cudaMemcpyAsync(&nnz, m->row_ptr + N, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(tmp, st);
+    cudaFreeAsync(len, st);
+    m->nnz = nnz;
+    FV_CUDA_TRY(cudaMalloc(&m->cols, sizeof(int32_t) * (nnz ? nnz : 1)));
+    if (mf <= 4)
+        k_row_fill<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+    else if (mf <= 8)
+        k_row_fill<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+    else
+        k_row_fill<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const fv_bc_desc *bc, fv_csr **A,
+                                 double *b, void *stream) {
+    if (!m || !terms || !A || !b) return FV_ERR_INVALID;
+    auto okc = [](double c) { return c == -1.0 || c == 0.0 || c == 1.0; };
+    if (!okc(terms->laplacian_coef) || !okc(terms->convection_coef) || !okc(terms->source_coef))
+        return FV_ERR_UNSUPPORTED;
+    if ((terms->laplacian_coef != 0.0 && !terms->diffusivity) || (terms->convection_coef != 0.0 && !terms->flux) ||
+        (terms->source_coef != 0.0 && !terms->source))
+        return FV_ERR_INVALID;
+    if (m->n_bfaces > 0 && (!bc || !bc->bndi || !bc->bnde)) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    if (m->nnz < 0) FV_TRY(build_pattern(m, st));
+    fv_csr *a = *A;
+    if (!a) {
+        a = new fv_csr();
+        a->nrows = a->ncols = m->n_cells;
+        a->nnz = m->nnz;
+        a->row_ptr = m->row_ptr;
+        a->cols = m->cols;
+        a->owns_pattern = false;
+        a->mesh = m;
+        cudaError_t e = cudaMalloc(&a->vals, sizeof(double) * (a->nnz ? a->nnz : 1));
+        if (e != cudaSuccess) {
+            delete a;
+            fv_internal_set_cuda_error(e, "fv_assemble vals");
+            return FV_ERR_ALLOC;
+        }
+        *A = a;
+    } else if (a->mesh != m) {
+        return FV_ERR_INVALID;
+    }
+    AssembleArgs args;
+    args.n = m->n_cells;
+    args.fb0 = m->n_faces - m->n_bfaces;
+    args.cf_ptr = m->cf_ptr;
+    args.cf_face = m->cf_face;
+    args.cf_other = m->cf_other;
+    args.cell = m->cell;
+    args.bfc = m->bface_center;
+    args.area = m->face_area;
+    args.kappa = terms->diffusivity;
+    args.flux = terms->flux;
+    args.src = terms->source;
+    args.bndi = bc ? bc->bndi : nullptr;
+    args.bnde = bc ? bc->bnde : nullptr;
+    args.c_lap = terms->laplacian_coef;
+    args.c_conv = terms->convection_coef;
+    args.c_src = terms->source_coef;
+    args.row_ptr = m->row_ptr;
+    args.vals = a->vals;
+    args.rhs = b;
+    const int mf = m->maxf;
+    if (m->dim == 2) {
+        if (mf <= 4)
+            launch_assemble<2, 4>(args, st);
+        else if (mf <= 8)
+            launch_assemble<2, 8>(args, st);
+        else
+            launch_assemble<2, 16>(args, st);
+    } else {
+        if (mf <= 4)
+            launch_assemble<3, 4>(args, st);
+        else if (mf <= 8)
+            launch_assemble<3, 8>(args, st);
+        else
+            launch_assemble<3, 16>(args, st);
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+extern "C" fv_status fv_assemble_host(fv_mesh *m, const fv_terms_desc *terms, const fv_bc_desc *bc, fv_csr **A,
+                                      double *b_host, void *stream) {
+    if (!m || !terms || !A || !b_host) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    const int64_t N = m->n_cells, F = m->n_faces, Fb = m->n_bfaces;
+    double *buf = nullptr;
+    const size_t tot = (size_t)(2 * F + 2 * N + 2 * Fb);
+    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * tot, st));
+    double *dk = buf, *dfl = buf + F, *ds = buf + 2 * F, *db = buf + 2 * F + N, *dbi = buf + 2 * F + 2 * N,
+           *dbe = dbi + Fb;
+    fv_terms_desc t = *terms;
+    if (terms->diffusivity) {
+        FV_CUDA_TRY(cudaMemcpyAsync(dk, terms->diffusivity, sizeof(double) * F, cudaMemcpyHostToDevice, st));
+        t.diffusivity = dk;
+    }
+    if (terms->flux) {
+        FV_CUDA_TRY(cudaMemcpyAsync(dfl, terms->flux, sizeof(double) * F, cudaMemcpyHostToDevice, st));
+        t.flux = dfl;
+    }
+    if (terms->source) {
+        FV_CUDA_TRY(cudaMemcpyAsync(ds, terms->source, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+        t.source = ds;
+    }
+    fv_bc_desc bd = {nullptr, nullptr};
+    if (bc && Fb > 0) {
+        FV_CUDA_TRY(cudaMemcpyAsync(dbi, bc->bndi, sizeof(double) * Fb, cudaMemcpyHostToDevice, st));
+        FV_CUDA_TRY(cudaMemcpyAsync(dbe, bc->bnde, sizeof(double) * Fb, cudaMemcpyHostToDevice, st));
+        bd.bndi = dbi;
+        bd.bnde = dbe;
+    }
+    fv_status s = fv_assemble(m, &t, bc ? &bd : nullptr, A, db, stream);
+    if (s == FV_OK) {
+        FV_CUDA_TRY(cudaMemcpyAsync(b_host, db, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    }
+    cudaFreeAsync(buf, st);
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    return s;
+}

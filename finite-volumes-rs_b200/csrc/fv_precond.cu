@@ -1,0 +1,638 @@
+// IC(0) / ILU(0) factorisation and the triangular sweeps that apply them.
+//
+// Reference: src/linalg/preconditioners/incomplete_cholesky.rs (build :148-202,
+// compute :87-145, precondition :217-255) and incomplete_lower_upper.rs
+// (build_and_compute_row_by_row :200-261 with the drop rule of
+// src/linalg/sparse_array.rs:48-50, precondition :287-329).
+//
+// Design.  Both the numeric factorisation and the sweeps are dependency
+// graphs over rows (row i needs the rows j of its strict lower part forward,
+// of its strict upper part backward).  Rows are processed in level order
+// (a stable sort by level of the DAG), handed out 32 at a time to warps via an
+// atomic ticket, one row per lane.  A row waits only for the rows it depends
+// on, through the produced values themselves (sweeps: a slot holds the
+// all-ones sentinel until written) or through per-row done flags
+// (factorisation).  Because tickets are taken in order by running warps, the
+// oldest unfinished row always belongs to a running warp whose inputs are
+// ready: the scheme cannot deadlock whatever the grid size or the other work
+// on the GPU, and every wait is bounded in time anyway.
+//
+// Each row is computed in the reference's own order (ascending column, same
+// reciprocal-then-multiply, no FMA), so the factors and the sweep results are
+// the reference's bits.  ILU entries dropped by the 1e-6 rule are stored as
+// exact zeros in place: subtracting lik*0 or l_ij*0 leaves every later value
+// unchanged, which is what skipping them does in the reference.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fv_internal.cuh"
+
+struct fv_symbolic {
+    int64_t n = 0, nnz_l = 0, nnz_u = 0;
+    int32_t *l_ptr = nullptr, *l_col = nullptr;  // strict lower part of the pattern
+    int32_t *u_ptr = nullptr, *u_col = nullptr;  // strict upper part
+    int32_t *fwd_order = nullptr, *bwd_order = nullptr;
+    int32_t *l_tpos = nullptr;                   // L entry (i,j) -> slot of (j,i) in U (IC only)
+    int32_t n_fwd_levels = 0, n_bwd_levels = 0;
+    int32_t max_row = 0;                         // longest row of the pattern
+    bool symmetric_pattern = false;
+    std::vector<int32_t> h_fwd_level, h_bwd_level;
+};
+
+void fv_symbolic_free(fv_symbolic *s) {
+    if (!s) return;
+    cudaFree(s->l_ptr);
+    cudaFree(s->l_col);
+    cudaFree(s->u_ptr);
+    cudaFree(s->u_col);
+    cudaFree(s->fwd_order);
+    cudaFree(s->bwd_order);
+    cudaFree(s->l_tpos);
+    delete s;
+}
+
+struct fv_precond {
+    int kind = 0;  // 1 = IC(0), 2 = ILU(0)
+    int64_t n = 0;
+    const fv_csr *A = nullptr;
+    fv_symbolic *sym = nullptr;  // owned by A
+    double *l_val = nullptr, *u_val = nullptr, *diag = nullptr, *dinv = nullptr;
+    double *tmp = nullptr;        // forward-sweep output, kept at sentinel between applies
+    unsigned *done = nullptr;     // factorisation flags
+    unsigned epoch = 0;
+    unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
+    int *err = nullptr;
+    int64_t n_dropped = 0;
+};
+
+// ------------------------------------------------------------------ symbolic
+static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **out) {
+    const int64_t n = A->nrows, nnz = A->nnz;
+    std::vector<int32_t> ptr((size_t)n + 1), col((size_t)(nnz ? nnz : 1));
+    FV_CUDA_TRY(cudaMemcpyAsync(ptr.data(), A->row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    if (nnz) FV_CUDA_TRY(cudaMemcpyAsync(col.data(), A->cols, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    fv_symbolic *s = new fv_symbolic();
+    s->n = n;
+    std::vector<int32_t> lp((size_t)n + 1), up((size_t)n + 1);
+    int64_t nl = 0, nu = 0;
+    int32_t maxrow = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        lp[i] = (int32_t)nl;
+        up[i] = (int32_t)nu;
+        bool has_diag = false;
+        maxrow = std::max(maxrow, ptr[i + 1] - ptr[i]);
+        for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+            if (k > ptr[i] && col[k] <= col[k - 1]) {
+                delete s;
+                return FV_ERR_INVALID;  // columns must be sorted and unique
+            }
+            if (col[k] < i)
+                ++nl;
+            else if (col[k] > i)
+                ++nu;
+            else
+                has_diag = true;
+        }
+        if (!has_diag) {  // the reference indexes [[i,i]] and panics
+            delete s;
+            return FV_ERR_INVALID;
+        }
+    }
+    lp[n] = (int32_t)nl;
+    up[n] = (int32_t)nu;
+    s->nnz_l = nl;
+    s->nnz_u = nu;
+    s->max_row = maxrow;
+    std::vector<int32_t> lc((size_t)(nl ? nl : 1)), uc((size_t)(nu ? nu : 1));
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t a = lp[i], b = up[i];
+        for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+            if (col[k] < i) lc[a++] = col[k];
+            if (col[k] > i) uc[b++] = col[k];
+        }
+    }
+    // level schedules (stable: rows of a level keep ascending order)
+    auto schedule = [&](bool upper, std::vector<int32_t> &level, std::vector<int32_t> &order) -> int32_t {
+        level.assign((size_t)n, 0);
+        int32_t nlev = 0;
+        if (!upper) {
+            for (int64_t i = 0; i < n; ++i) {
+                int32_t l = 0;
+                for (int32_t k = lp[i]; k < lp[i + 1]; ++k) l = std::max(l, level[lc[k]] + 1);
+                level[i] = l;
+                nlev = std::max(nlev, l + 1);
+            }
+        } else {
+            for (int64_t i = n - 1; i >= 0; --i) {
+                int32_t l = 0;
+                for (int32_t k = up[i]; k < up[i + 1]; ++k) l = std::max(l, level[uc[k]] + 1);
+                level[i] = l;
+                nlev = std::max(nlev, l + 1);
+            }
+        }
+        std::vector<int64_t> start((size_t)nlev + 1, 0);
+        for (int64_t i = 0; i < n; ++i) start[level[i] + 1]++;
+        for (int32_t l = 0; l < nlev; ++l) start[l + 1] += start[l];
+        order.assign((size_t)n, 0);
+        for (int64_t i = 0; i < n; ++i) order[start[level[i]]++] = (int32_t)i;
+        return nlev;
+    };
+    std::vector<int32_t> fo, bo;
+    s->n_fwd_levels = schedule(false, s->h_fwd_level, fo);
+    s->n_bwd_levels = schedule(true, s->h_bwd_level, bo);
+    // transpose map L(i,j) -> U(j,i); also tells whether the pattern is symmetric
+    std::vector<int32_t> tpos((size_t)(nl ? nl : 1)), cur(up.begin(), up.end() - 1);
+    bool sym = (nl == nu);
+    for (int64_t i = 0; i < n && sym; ++i)
+        for (int32_t k = lp[i]; k < lp[i + 1]; ++k) {
+            int32_t j = lc[k];
+            int32_t p = cur[j]++;
+            if (p >= up[j + 1] || uc[p] != i) {
+                sym = false;
+                break;
+            }
+            tpos[k] = p;
+        }
+    s->symmetric_pattern = sym;
+    cudaError_t e = cudaSuccess;
+    auto up_load = [&](int32_t **d, const std::vector<int32_t> &h, size_t cnt) {
+        if (e != cudaSuccess) return;
+        e = cudaMalloc(d, sizeof(int32_t) * (cnt ? cnt : 1));
+        if (e == cudaSuccess && cnt) e = cudaMemcpyAsync(*d, h.data(), sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, st);
+    };
+    up_load(&s->l_ptr, lp, (size_t)n + 1);
+    up_load(&s->u_ptr, up, (size_t)n + 1);
+    up_load(&s->l_col, lc, (size_t)nl);
+    up_load(&s->u_col, uc, (size_t)nu);
+    up_load(&s->fwd_order, fo, (size_t)n);
+    up_load(&s->bwd_order, bo, (size_t)n);
+    if (sym) up_load(&s->l_tpos, tpos, (size_t)nl);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "symbolic upload");
+        fv_symbolic_free(s);
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    *out = s;
+    return FV_OK;
+}
+
+fv_status fv_get_symbolic(fv_csr *A, cudaStream_t st, fv_symbolic **out) {
+    if (!A->sym) FV_TRY(build_symbolic(A, st, &A->sym));
+    *out = A->sym;
+    return FV_OK;
+}
+
+// ------------------------------------------------------------------ kernels
+namespace {
+
+__device__ __forceinline__ bool take_chunk(unsigned *ticket, int64_t nchunks, int64_t &chunk) {
+    unsigned c = 0;
+    if ((threadIdx.x & 31) == 0) c = atomicAdd(ticket, 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    chunk = c;
+    return (int64_t)c < nchunks;
+}
+
+__device__ __forceinline__ void leave(unsigned *ticket, unsigned *exits) {
+    if ((threadIdx.x & 31) == 0) {
+        unsigned total = gridDim.x * (blockDim.x >> 5);
+        if (atomicAdd(exits, 1u) == total - 1) {
+            *ticket = 0;
+            *exits = 0;
+        }
+    }
+}
+
+// ILU(0) numeric, one row per lane (incomplete_lower_upper.rs:207-261).
+template <int MAXR>
+__global__ void __launch_bounds__(128) k_ilu0(int64_t n, const int32_t *__restrict__ order,
+                                              const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
+                                              const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
+                                              const int32_t *__restrict__ u_ptr, const int32_t *__restrict__ u_col,
+                                              double *l_val, double *u_val, double *diag, double *dinv,
+                                              unsigned *done, unsigned epoch, unsigned *ctrl, int *err) {
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int i = order[idx];
+        const int l0 = l_ptr[i], nl = l_ptr[i + 1] - l0;
+        const int u0 = u_ptr[i], nu = u_ptr[i + 1] - u0;
+        const int m = nl + 1 + nu;
+        const int a0 = a_ptr[i];
+        int c[MAXR];
+        double v[MAXR];
+        for (int q = 0; q < m; ++q) {
+            v[q] = a_val[a0 + q];
+            c[q] = q < nl ? l_col[l0 + q] : (q == nl ? i : u_col[u0 + q - nl - 1]);
+        }
+        for (int q = 0; q < nl; ++q) {
+            const int k = c[q];
+            fv_wait_flag(&done[k], epoch, err);
+            const double lukk = __ldcg(&diag[k]);
+            if (fabs(lukk) < 1e-16) atomicOr(err, FV_DEV_SINGULAR);
+            const double lukkinv = 1.0 / lukk;
+            v[q] = lukkinv * v[q];
+            const double lik = v[q];
+            int p = q + 1;
+            for (int s = u_ptr[k]; s < u_ptr[k + 1]; ++s) {
+                const int j = u_col[s];
+                const double term = lik * __ldcg(&u_val[s]);
+                while (p < m && c[p] < j) ++p;
+                if (p < m && c[p] == j) v[p] -= term;
+            }
+        }
+        const double tol = fabs(v[nl]) * 1e-6;
+        for (int q = 0; q < m; ++q)
+            if (q != nl && !(fabs(v[q]) > tol)) v[q] = 0.0;
+        for (int q = 0; q < nl; ++q) l_val[l0 + q] = v[q];
+        for (int q = 0; q < nu; ++q) u_val[u0 + q] = v[nl + 1 + q];
+        diag[i] = v[nl];
+        dinv[i] = 1.0 / v[nl];
+        __threadfence();
+        fv_st_release_u32(&done[i], epoch);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+// IC(0) numeric, up-looking form of the reference's right-looking loop
+// (incomplete_cholesky.rs:87-135): every l_ij receives the same updates
+// l_ik*l_jk in ascending k and the same final scaling by 1/l_jj.
+template <int MAXR>
+__global__ void __launch_bounds__(128) k_ic0(int64_t n, const int32_t *__restrict__ order,
+                                             const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
+                                             const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
+                                             const int32_t *__restrict__ l_tpos, double *l_val, double *u_val,
+                                             double *diag, double *dinv, unsigned *done, unsigned epoch,
+                                             unsigned *ctrl, int *err) {
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int i = order[idx];
+        const int l0 = l_ptr[i], nl = l_ptr[i + 1] - l0;
+        const int a0 = a_ptr[i];
+        int c[MAXR];
+        double v[MAXR];
+        for (int q = 0; q < nl; ++q) {
+            c[q] = l_col[l0 + q];
+            v[q] = a_val[a0 + q];
+        }
+        double vd = a_val[a0 + nl];
+        for (int q = 0; q < nl; ++q) {
+            const int j = c[q];
+            fv_wait_flag(&done[j], epoch, err);
+            // merge row i (k < j) with row j's strict lower part
+            int p = 0;
+            const int s1 = l_ptr[j + 1];
+            for (int s = l_ptr[j]; s < s1 && p < q; ++s) {
+                const int k = l_col[s];
+                while (p < q && c[p] < k) ++p;
+                if (p < q && c[p] == k) v[q] -= v[p] * __ldcg(&l_val[s]);
+            }
+            v[q] = __ldcg(&dinv[j]) * v[q];
+        }
+        for (int q = 0; q < nl; ++q) vd -= v[q] * v[q];
+        const double lii = sqrt(vd);
+        for (int q = 0; q < nl; ++q) {
+            l_val[l0 + q] = v[q];
+            u_val[l_tpos[l0 + q]] = v[q];
+        }
+        diag[i] = lii;
+        dinv[i] = 1.0 / lii;
+        __threadfence();
+        fv_st_release_u32(&done[i], epoch);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+// |a_ij - a_ji| < 1e-14 for every stored pair (is_symmetric, dmatrix.rs:76-88)
+__global__ void k_check_symmetric(int64_t n, const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
+                                  const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
+                                  const int32_t *__restrict__ u_ptr, const int32_t *__restrict__ l_tpos, int *bad) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int l0 = l_ptr[i], nl = l_ptr[i + 1] - l0, a0 = a_ptr[i];
+    for (int q = 0; q < nl; ++q) {
+        // the transposed entry (j,i) sits in U slot p of row j, i.e. at A position
+        // a_ptr[j] + (number of strict-lower entries of row j) + 1 + (p - u_ptr[j])
+        const int j = l_col[l0 + q];
+        const int p = l_tpos[l0 + q];
+        const double aji = a_val[a_ptr[j] + (l_ptr[j + 1] - l_ptr[j]) + 1 + (p - u_ptr[j])];
+        const double aij = a_val[a0 + q];
+        if (!(fabs(aij - aji) < 1e-14)) atomicOr(bad, 1);
+    }
+}
+
+__global__ void k_count_dropped(int64_t nl, const double *__restrict__ l_val, int64_t nu,
+                                const double *__restrict__ u_val, unsigned long long *cnt) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned c = 0;
+    for (int64_t k = t; k < nl; k += (int64_t)gridDim.x * blockDim.x) c += (l_val[k] == 0.0);
+    for (int64_t k = t; k < nu; k += (int64_t)gridDim.x * blockDim.x) c += (u_val[k] == 0.0);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, (unsigned long long)c);
+}
+
+}  // namespace
+
+// Triangular sweep (one row per lane, level order, values as readiness).
+//   x_i = [dinv_i *] (rhs_i - sum_{j in row} val * x_j), ascending j.
+// After reading rhs_i the lane may reset it to the sentinel (rhs_reset), and
+// it may pre-fill a later sweep's output slot (next_reset) with the sentinel.
+template <typename T, bool UNIT>
+__global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restrict__ order,
+                                               const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                                               const T *__restrict__ val, const T *__restrict__ dinv,
+                                               const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
+                                               int *err, const int *skip) {
+    if (skip && *(volatile const int *)skip) return;  // a converged solve: no warp takes a ticket
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int i = order[idx];
+        T s = rhs[i];
+        if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
+        const int k1 = ptr[i + 1];
+        for (int k = ptr[i]; k < k1; ++k) {
+            const T xj = fv_wait_value(&x[col[k]], err);
+            s = s - val[k] * xj;
+        }
+        const T r = UNIT ? s : dinv[i] * s;
+        fv_publish(&x[i], r);
+        if (next_reset) fv_reset_slot(&next_reset[i]);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+
+static int sweep_grid(int64_t n) {
+    int64_t warps = (n + 31) / 32;
+    int64_t blocks = (warps + 7) / 8;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 8));
+}
+
+// z = M^-1 r.  r must not alias z.  The forward sweep writes P->tmp and
+// pre-fills z with the sentinel; the backward sweep consumes tmp (resetting it
+// to the sentinel for the next apply) and writes z.
+fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaStream_t st, const int *skip) {
+    const fv_symbolic *s = P->sym;
+    const int64_t n = P->n;
+    const int G = sweep_grid(n);
+    if (P->kind == 2) {
+        k_sweep<double, true><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r, P->tmp,
+                                                 nullptr, z, P->ctrl, P->err, skip);
+    } else {
+        k_sweep<double, false><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
+                                                  P->tmp, nullptr, z, P->ctrl, P->err, skip);
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    k_sweep<double, false><<<G, 256, 0, st>>>(n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp, z,
+                                              P->tmp, nullptr, P->ctrl + 2, P->err, skip);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+fv_status fv_precond_check_error(fv_precond *P, cudaStream_t st) {
+    int e = 0;
+    FV_CUDA_TRY(cudaMemcpyAsync(&e, P->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    if (e) {
+        FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+        if (e & FV_DEV_TIMEOUT) return FV_ERR_TIMEOUT;
+        if (e & FV_DEV_SINGULAR) return FV_ERR_SINGULAR_PIVOT;
+        return FV_ERR_BREAKDOWN;
+    }
+    return FV_OK;
+}
+
+int *fv_precond_err_ptr(fv_precond *P) { return P->err; }
+
+extern "C" fv_status fv_precond_destroy(fv_precond *P) {
+    if (!P) return FV_OK;
+    cudaFree(P->l_val);
+    cudaFree(P->u_val);
+    cudaFree(P->diag);
+    cudaFree(P->dinv);
+    cudaFree(P->tmp);
+    cudaFree(P->done);
+    cudaFree(P->ctrl);
+    cudaFree(P->err);
+    delete P;
+    return FV_OK;
+}
+
+static fv_status precond_alloc(fv_precond *P, cudaStream_t st) {
+    const int64_t n = P->n;
+    FV_CUDA_TRY(cudaMalloc(&P->l_val, sizeof(double) * (P->sym->nnz_l ? P->sym->nnz_l : 1)));
+    FV_CUDA_TRY(cudaMalloc(&P->u_val, sizeof(double) * (P->sym->nnz_u ? P->sym->nnz_u : 1)));
+    FV_CUDA_TRY(cudaMalloc(&P->diag, sizeof(double) * n));
+    FV_CUDA_TRY(cudaMalloc(&P->dinv, sizeof(double) * n));
+    FV_CUDA_TRY(cudaMalloc(&P->tmp, sizeof(double) * n));
+    FV_CUDA_TRY(cudaMalloc(&P->done, sizeof(unsigned) * n));
+    FV_CUDA_TRY(cudaMalloc(&P->ctrl, sizeof(unsigned) * 8));
+    FV_CUDA_TRY(cudaMalloc(&P->err, sizeof(int)));
+    FV_CUDA_TRY(cudaMemsetAsync(P->tmp, 0xFF, sizeof(double) * n, st));
+    FV_CUDA_TRY(cudaMemsetAsync(P->done, 0, sizeof(unsigned) * n, st));
+    FV_CUDA_TRY(cudaMemsetAsync(P->ctrl, 0, sizeof(unsigned) * 8, st));
+    FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+    return FV_OK;
+}
+
+static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_precond **out) {
+    if (!Ac || !out) return FV_ERR_INVALID;
+    if (Ac->nrows != Ac->ncols) return FV_ERR_INVALID;
+    fv_csr *A = const_cast<fv_csr *>(Ac);
+    fv_symbolic *sym = nullptr;
+    FV_TRY(fv_get_symbolic(A, st, &sym));
+    if (sym->max_row > 32) return FV_ERR_UNSUPPORTED;
+    if (kind == 1 && !sym->symmetric_pattern) return FV_ERR_NOT_SYMMETRIC;
+    fv_precond *P = *out;
+    const bool fresh = (P == nullptr);
+    if (fresh) {
+        P = new fv_precond();
+        P->kind = kind;
+        P->n = A->nrows;
+        P->A = A;
+        P->sym = sym;
+        fv_status s = precond_alloc(P, st);
+        if (s != FV_OK) {
+            fv_precond_destroy(P);
+            return s;
+        }
+    } else if (P->A != A || P->kind != kind) {
+        return FV_ERR_INVALID;
+    }
+    const int64_t n = P->n;
+    if (kind == 1) {
+        FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+        k_check_symmetric<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, A->row_ptr, A->vals, sym->l_ptr, sym->l_col,
+                                                                      sym->u_ptr, sym->l_tpos, P->err);
+        FV_CUDA_TRY(cudaGetLastError());
+        int bad = 0;
+        FV_CUDA_TRY(cudaMemcpyAsync(&bad, P->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaStreamSynchronize(st));
+        if (bad) {
+            FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+            if (fresh) fv_precond_destroy(P);
+            return FV_ERR_NOT_SYMMETRIC;
+        }
+    }
+    P->epoch += 1;
+    if (P->epoch == 0) {  // wrapped: clear the flags
+        FV_CUDA_TRY(cudaMemsetAsync(P->done, 0, sizeof(unsigned) * n, st));
+        P->epoch = 1;
+    }
+    const int G = sweep_grid(n) * 2;  // 128-thread blocks
+    const int mr = sym->max_row;
+    if (kind == 2) {
+#define FV_ILU(MR)                                                                                          \
+    k_ilu0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->u_ptr, \
+                                  sym->u_col, P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch,        \
+                                  P->ctrl + 4, P->err)
+        if (mr <= 8)
+            FV_ILU(8);
+        else if (mr <= 16)
+            FV_ILU(16);
+        else
+            FV_ILU(32);
+#undef FV_ILU
+    } else {
+#define FV_IC(MR)                                                                                             \
+    k_ic0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->l_tpos, \
+                                 P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch, P->ctrl + 4, P->err)
+        if (mr <= 8)
+            FV_IC(8);
+        else if (mr <= 16)
+            FV_IC(16);
+        else
+            FV_IC(32);
+#undef FV_IC
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    fv_status es = fv_precond_check_error(P, st);
+    if (es != FV_OK) {
+        if (fresh) fv_precond_destroy(P);
+        return es;
+    }
+    if (kind == 2) {
+        unsigned long long *cnt = nullptr;
+        FV_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(unsigned long long), st));
+        FV_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+        k_count_dropped<<<592, 256, 0, st>>>(sym->nnz_l, P->l_val, sym->nnz_u, P->u_val, cnt);
+        unsigned long long h = 0;
+        FV_CUDA_TRY(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaFreeAsync(cnt, st));
+        FV_CUDA_TRY(cudaStreamSynchronize(st));
+        P->n_dropped = (int64_t)h;
+    }
+    *out = P;
+    return FV_OK;
+}
+
+extern "C" fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out) {
+    if (!out) return FV_ERR_INVALID;
+    *out = nullptr;
+    return factor_common(A, 1, fv_stream(stream), out);
+}
+extern "C" fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out) {
+    if (!out) return FV_ERR_INVALID;
+    *out = nullptr;
+    return factor_common(A, 2, fv_stream(stream), out);
+}
+// Value-only refactorisation into an existing preconditioner (same matrix object).
+extern "C" fv_status fv_precond_refactor(fv_precond *P, void *stream) {
+    if (!P) return FV_ERR_INVALID;
+    fv_precond *q = P;
+    return factor_common(P->A, P->kind, fv_stream(stream), &q);
+}
+
+extern "C" fv_status fv_precond_apply(fv_precond *P, const double *r, double *z, void *stream) {
+    if (!P || !r || !z || r == z) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    FV_TRY(fv_precond_apply_dev(P, r, z, st, nullptr));
+    return fv_precond_check_error(P, st);
+}
+
+extern "C" fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, double *z_host, void *stream) {
+    if (!P || !r_host || !z_host) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    double *buf = nullptr;
+    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * 2 * P->n, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(buf, r_host, sizeof(double) * P->n, cudaMemcpyHostToDevice, st));
+    fv_status s = fv_precond_apply_dev(P, buf, buf + P->n, st, nullptr);
+    if (s == FV_OK) s = fv_precond_check_error(P, st);
+    if (s == FV_OK)
+        FV_CUDA_TRY(cudaMemcpyAsync(z_host, buf + P->n, sizeof(double) * P->n, cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(buf, st);
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    return s;
+}
+
+extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr, int32_t *cols,
+                                       double *vals, int32_t *n_dropped, void *stream) {
+    if (!P || !nnz) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    const fv_symbolic *s = P->sym;
+    const int64_t n = P->n;
+    if (n_dropped) *n_dropped = (int32_t)P->n_dropped;
+    // IC: the reference's `l` (lower incl. diagonal); ILU: the reference's `lu` (dropped entries removed)
+    const int64_t total = P->kind == 1 ? s->nnz_l + n : s->nnz_l + s->nnz_u + n - P->n_dropped;
+    if (!row_ptr || !cols || !vals) {
+        *nnz = total;
+        return FV_OK;
+    }
+    std::vector<int32_t> lp(n + 1), lc(s->nnz_l ? s->nnz_l : 1), up(n + 1), uc(s->nnz_u ? s->nnz_u : 1);
+    std::vector<double> lv(s->nnz_l ? s->nnz_l : 1), uv(s->nnz_u ? s->nnz_u : 1), dg(n);
+    FV_CUDA_TRY(cudaMemcpyAsync(lp.data(), s->l_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(up.data(), s->u_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    if (s->nnz_l) {
+        FV_CUDA_TRY(cudaMemcpyAsync(lc.data(), s->l_col, sizeof(int32_t) * s->nnz_l, cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaMemcpyAsync(lv.data(), P->l_val, sizeof(double) * s->nnz_l, cudaMemcpyDeviceToHost, st));
+    }
+    if (s->nnz_u) {
+        FV_CUDA_TRY(cudaMemcpyAsync(uc.data(), s->u_col, sizeof(int32_t) * s->nnz_u, cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaMemcpyAsync(uv.data(), P->u_val, sizeof(double) * s->nnz_u, cudaMemcpyDeviceToHost, st));
+    }
+    FV_CUDA_TRY(cudaMemcpyAsync(dg.data(), P->diag, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    int64_t o = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        row_ptr[i] = (int32_t)o;
+        for (int32_t k = lp[i]; k < lp[i + 1]; ++k) {
+            if (P->kind == 2 && lv[k] == 0.0) continue;
+            cols[o] = lc[k];
+            vals[o++] = lv[k];
+        }
+        cols[o] = (int32_t)i;
+        vals[o++] = dg[i];
+        if (P->kind == 2)
+            for (int32_t k = up[i]; k < up[i + 1]; ++k) {
+                if (uv[k] == 0.0) continue;
+                cols[o] = uc[k];
+                vals[o++] = uv[k];
+            }
+    }
+    row_ptr[n] = (int32_t)o;
+    *nnz = o;
+    return FV_OK;
+}
+
+extern "C" fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,
+                                       int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream) {
+    (void)stream;
+    if (!P) return FV_ERR_INVALID;
+    const fv_symbolic *s = P->sym;
+    if (fwd_level) std::copy(s->h_fwd_level.begin(), s->h_fwd_level.end(), fwd_level);
+    if (bwd_level) std::copy(s->h_bwd_level.begin(), s->h_bwd_level.end(), bwd_level);
+    if (n_fwd_levels) *n_fwd_levels = s->n_fwd_levels;
+    if (n_bwd_levels) *n_bwd_levels = s->n_bwd_levels;
+    return FV_OK;
+}

@@ -1,0 +1,15 @@
+"""fvb200: B200 implementation of the finite-volumes crate's assemble + Krylov
+hot path, behind the C ABI of include/fv_b200.h.
+
+The names mirror the reference crate (fvm::assembly::assemble,
+linalg::{DistributedMatrix, DistributedVector}, preconditioners::{
+IncompleteCholesky, IncompleteLowerUpper}, solvers::{conjugate_gradient,
+bi_conjugate_gradient_stab, LinearSolverOptions, LinearSolverInfo}).
+"""
+from ._lib import FvError, lib  # noqa: F401
+from .linalg import (  # noqa: F401
+    DistributedMatrix, DistributedVector, IdentityPreconditioner, IncompleteCholesky, IncompleteLowerUpper,
+    LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, conjugate_gradient,
+)
+from .mesh import DeviceMesh, Mesh  # noqa: F401
+from .terms import Orthogonal, Upwind, convection, laplacian, source  # noqa: F401

@@ -1,0 +1,145 @@
+"""ctypes binding of libfvb200.so (the C ABI declared in include/fv_b200.h).
+
+Loading never falls back to anything: if the shared library is missing the
+import raises, and every device entry point reports CUDA errors as FvError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libfvb200.so"
+
+FV_STATUS = {
+    0: "FV_OK", 1: "FV_ERR_ALLOC", 2: "FV_ERR_INVALID", 3: "FV_ERR_SINGULAR_PIVOT", 4: "FV_ERR_BREAKDOWN",
+    5: "FV_ERR_TIMEOUT", 6: "FV_ERR_NOT_SYMMETRIC", 7: "FV_ERR_CUDA", 8: "FV_ERR_UNSUPPORTED",
+}
+FV_OK, FV_ERR_ALLOC, FV_ERR_INVALID, FV_ERR_SINGULAR_PIVOT, FV_ERR_BREAKDOWN = 0, 1, 2, 3, 4
+FV_ERR_TIMEOUT, FV_ERR_NOT_SYMMETRIC, FV_ERR_CUDA, FV_ERR_UNSUPPORTED = 5, 6, 7, 8
+
+
+class FvError(RuntimeError):
+    """A status other than FV_OK; the reference panics in the same situations."""
+
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        name = FV_STATUS.get(status, f"status {status}")
+        detail = ""
+        try:
+            detail = lib().fv_last_error().decode()
+        except Exception:  # pragma: no cover - best effort
+            pass
+        super().__init__(f"{what}: {name}" + (f" ({detail})" if detail and status == FV_ERR_CUDA else ""))
+
+
+P = C.POINTER
+dp, ip, i64 = P(C.c_double), P(C.c_int32), C.c_int64
+
+
+class HostMesh_(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("n_nodes", i64), ("n_faces", i64), ("n_cells", i64), ("n_boundary_faces", i64),
+        ("nodes", dp), ("face_node_ptr", ip), ("face_nodes", ip), ("face_patch", ip),
+        ("cell_face_ptr", ip), ("cell_faces", ip), ("face_owner", ip), ("face_neighbor", ip),
+        ("face_area", dp), ("face_normal", dp), ("face_center", dp), ("cell_center", dp), ("cell_volume", dp),
+    ]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("n_cells", i64), ("n_faces", i64), ("n_boundary_faces", i64),
+        ("face_owner", ip), ("face_neighbor", ip), ("face_area", dp), ("face_center", dp),
+        ("cell_center", dp), ("cell_volume", dp),
+    ]
+
+
+class TermsDesc(C.Structure):
+    _fields_ = [
+        ("laplacian_coef", C.c_double), ("convection_coef", C.c_double), ("source_coef", C.c_double),
+        ("diffusivity", C.c_void_p), ("flux", C.c_void_p), ("source", C.c_void_p),
+    ]
+
+
+class BcDesc(C.Structure):
+    _fields_ = [("bndi", C.c_void_p), ("bnde", C.c_void_p)]
+
+
+class SolverOptions(C.Structure):
+    _fields_ = [("relative_tolerance", C.c_double), ("absolute_tolerance", C.c_double),
+                ("max_iterations", i64)]
+
+
+class SolverInfo(C.Structure):
+    _fields_ = [
+        ("iterations", i64), ("initial_residual", C.c_double), ("final_residual", C.c_double),
+        ("status", C.c_int32), ("restarts", C.c_int32), ("history", dp), ("history_cap", i64),
+        ("history_len", i64), ("device_ms", C.c_double),
+    ]
+
+
+vp = C.c_void_p
+_SIGS = {
+    # host mesh
+    "fv_host_mesh_from_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, P(P(HostMesh_))],
+    "fv_host_mesh_generate_square": [C.c_int32, C.c_double, C.c_uint64, P(P(HostMesh_))],
+    "fv_host_mesh_generate_cube": [C.c_int32, C.c_double, C.c_uint64, P(P(HostMesh_))],
+    "fv_host_fields_generate": [P(HostMesh_), C.c_uint64, C.c_double, C.c_double, dp, C.c_double, C.c_int32,
+                                dp, dp, dp],
+    # device objects
+    "fv_mesh_upload": [P(MeshDesc), vp, P(vp)],
+    "fv_mesh_destroy": [vp],
+    "fv_assemble": [vp, P(TermsDesc), P(BcDesc), P(vp), vp, vp],
+    "fv_assemble_host": [vp, P(TermsDesc), P(BcDesc), P(vp), dp, vp],
+    "fv_csr_create_host": [i64, i64, ip, ip, dp, vp, P(vp)],
+    "fv_csr_info": [vp, P(i64), P(i64), P(i64)],
+    "fv_csr_download": [vp, ip, ip, dp, vp],
+    "fv_csr_destroy": [vp],
+    "fv_spmv": [vp, vp, vp, vp],
+    "fv_spmv_host": [vp, dp, dp, vp],
+    "fv_ic0_factor": [vp, vp, P(vp)],
+    "fv_ilu0_factor": [vp, vp, P(vp)],
+    "fv_precond_refactor": [vp, vp],
+    "fv_precond_apply": [vp, vp, vp, vp],
+    "fv_precond_apply_host": [vp, dp, dp, vp],
+    "fv_precond_export": [vp, P(i64), ip, ip, dp, ip, vp],
+    "fv_precond_levels": [vp, ip, ip, ip, ip, vp],
+    "fv_precond_destroy": [vp],
+    "fv_cg": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
+    "fv_bicgstab": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
+    "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
+    "fv_bicgstab_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libfvb200.so (built in-tree by build.py).  Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() (or fvb200/build.py)")
+        L = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.fv_host_mesh_free.argtypes = [P(HostMesh_)]
+        L.fv_host_mesh_free.restype = None
+        L.fv_status_string.argtypes = [C.c_int]
+        L.fv_status_string.restype = C.c_char_p
+        L.fv_last_error.argtypes = []
+        L.fv_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str) -> None:
+    if status != FV_OK:
+        raise FvError(status, what)
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS) + ["fv_host_mesh_free", "fv_status_string"]

@@ -1,0 +1,315 @@
+"""DistributedMatrix / DistributedVector, assemble(), the preconditioners and
+the Krylov solvers, mirroring the reference crate's Rust API on the device.
+
+  assemble ................... src/fvm/assembly.rs:11
+  DistributedMatrix::imul .... src/linalg/dmatrix.rs:136
+  IncompleteCholesky ......... src/linalg/preconditioners/incomplete_cholesky.rs:205
+  IncompleteLowerUpper ....... src/linalg/preconditioners/incomplete_lower_upper.rs:266
+  conjugate_gradient ......... src/linalg/solvers/conjugate_gradient.rs:12
+  bi_conjugate_gradient_stab . src/linalg/solvers/bi_conjugate_gradient_stab.rs:13
+  LinearSolverOptions/Info ... src/linalg/solvers/mod.rs:11-42
+
+Error behaviour: where the reference panics (missing matrix entry, ILU pivot
+below 1e-16, IC on a non-symmetric matrix) these raise FvError; solvers
+return a LinearSolverInfo and never raise for non-convergence.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import BcDesc, FvError, SolverInfo, SolverOptions, TermsDesc, check, lib
+from .streams import stream_handle
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dev_f64(a):
+    """Device float64 tensor for an array-like (numpy / torch / DistributedVector)."""
+    torch = _torch()
+    if isinstance(a, DistributedVector):
+        return a.data
+    if isinstance(a, torch.Tensor):
+        t = a.to(device="cuda", dtype=torch.float64)
+        return t.contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+class DistributedVector:
+    """Dense FP64 vector resident on the GPU (torch tensor)."""
+
+    def __init__(self, data):
+        self.data = _dev_f64(data)
+
+    @classmethod
+    def from_size(cls, n: int) -> "DistributedVector":
+        torch = _torch()
+        return cls(torch.zeros(n, dtype=torch.float64, device="cuda"))
+
+    @classmethod
+    def from_data(cls, data) -> "DistributedVector":
+        return cls(data)
+
+    def __len__(self):
+        return int(self.data.numel())
+
+    def len(self):
+        return len(self)
+
+    def numpy(self) -> np.ndarray:
+        return self.data.detach().cpu().numpy()
+
+    def ptr(self) -> C.c_void_p:
+        return C.c_void_p(self.data.data_ptr())
+
+
+class DistributedMatrix:
+    """CSR matrix on the GPU (fv_csr handle), FP64 values, int32 indices."""
+
+    def __init__(self, handle: C.c_void_p, keepalive=None):
+        self.handle = handle
+        self._keep = keepalive
+
+    @classmethod
+    def from_csr(cls, row_ptr, cols, vals, ncols=None, stream=None) -> "DistributedMatrix":
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        cc = np.ascontiguousarray(cols, dtype=np.int32)
+        vv = np.ascontiguousarray(vals, dtype=np.float64)
+        n = len(rp) - 1
+        h = C.c_void_p()
+        check(lib().fv_csr_create_host(n, n if ncols is None else ncols, rp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       cc.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       vv.ctypes.data_as(C.POINTER(C.c_double)), stream_handle(stream),
+                                       C.byref(h)), "DistributedMatrix.from_csr")
+        return cls(h)
+
+    def shape(self):
+        nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().fv_csr_info(self.handle, C.byref(nr), C.byref(nc), C.byref(nz)), "fv_csr_info")
+        return nr.value, nc.value, nz.value
+
+    def nrows(self):
+        return self.shape()[0]
+
+    def ncols(self):
+        return self.shape()[1]
+
+    def nnz(self):
+        return self.shape()[2]
+
+    def to_csr(self, stream=None):
+        """(row_ptr, cols, vals) as numpy arrays."""
+        n, _, nz = self.shape()
+        rp = np.empty(n + 1, np.int32)
+        cc = np.empty(max(nz, 1), np.int32)
+        vv = np.empty(max(nz, 1), np.float64)
+        check(lib().fv_csr_download(self.handle, rp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    cc.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    vv.ctypes.data_as(C.POINTER(C.c_double)), stream_handle(stream)),
+              "fv_csr_download")
+        return rp, cc[:nz], vv[:nz]
+
+    def imul(self, result: DistributedVector, rhs, stream=None) -> None:
+        """result = self * rhs (dmatrix.rs:136-146), bit-exact per row."""
+        x = _dev_f64(rhs)
+        check(lib().fv_spmv(self.handle, C.c_void_p(x.data_ptr()), result.ptr(), stream_handle(stream)), "fv_spmv")
+
+    def close(self):
+        if self.handle:
+            lib().fv_csr_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None = None, stream=None):
+    """assemble(equation, boundary_condition, mesh) -> (DistributedMatrix, DistributedVector).
+
+    boundary_condition: a callable face_id -> (bndi, bnde) as in the reference
+    (evaluated once per boundary face on the host), or a pair of arrays
+    (bndi, bnde) over the boundary faces.  Passing `lhs` from an earlier call
+    on the same mesh refills its values in place (value-only re-assembly).
+    """
+    torch = _torch()
+    dm = mesh.device(stream)
+    c_lap, c_conv, c_src = equation.coefficients()
+    keep = []
+
+    def dptr(kind):
+        if kind not in equation.data:
+            return None
+        t = _dev_f64(equation.data[kind])
+        keep.append(t)
+        return t.data_ptr()
+
+    t = TermsDesc()
+    t.laplacian_coef, t.convection_coef, t.source_coef = c_lap, c_conv, c_src
+    t.diffusivity = dptr("laplacian")
+    t.flux = dptr("convection")
+    t.source = dptr("source")
+    nb = mesh.n_boundary_faces
+    if callable(boundary_condition):
+        fb0 = mesh.n_faces - nb
+        pairs = [boundary_condition(fb0 + k) for k in range(nb)]
+        bndi = np.array([p[0] for p in pairs], dtype=np.float64)
+        bnde = np.array([p[1] for p in pairs], dtype=np.float64)
+    else:
+        bndi, bnde = boundary_condition
+    bi = _dev_f64(bndi)
+    be = _dev_f64(bnde)
+    keep += [bi, be]
+    bc = BcDesc(bi.data_ptr(), be.data_ptr())
+    rhs = DistributedVector.from_size(mesh.n_cells)
+    h = lhs.handle if lhs is not None else C.c_void_p()
+    check(lib().fv_assemble(dm.handle, C.byref(t), C.byref(bc), C.byref(h), rhs.ptr(), stream_handle(stream)),
+          "assemble")
+    # torch's caching allocator is stream ordered: the temporaries in `keep`
+    # are not reused before the assembly kernel has consumed them
+    del keep
+    if lhs is None:
+        lhs = DistributedMatrix(h, keepalive=dm)
+    return lhs, rhs
+
+
+class Preconditioner:
+    handle = C.c_void_p()
+
+    def precondition(self, solution: DistributedVector, rhs: DistributedVector, comm=None, stream=None) -> None:
+        """solution = M^-1 rhs (Preconditioner::precondition, preconditioners/mod.rs:13-17)."""
+        check(lib().fv_precond_apply(self.handle, rhs.ptr(), solution.ptr(), stream_handle(stream)), "precondition")
+
+    def factors(self, stream=None):
+        """Stored factors as CSR numpy arrays: IC -> the reference's `l`,
+        ILU -> the reference's `lu` (dropped entries removed); and n_dropped."""
+        nz = C.c_int64()
+        nd = C.c_int32()
+        check(lib().fv_precond_export(self.handle, C.byref(nz), None, None, None, C.byref(nd),
+                                      stream_handle(stream)), "factors")
+        n = self.n
+        rp = np.empty(n + 1, np.int32)
+        cc = np.empty(max(nz.value, 1), np.int32)
+        vv = np.empty(max(nz.value, 1), np.float64)
+        check(lib().fv_precond_export(self.handle, C.byref(nz), rp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      cc.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      vv.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nd),
+                                      stream_handle(stream)), "factors")
+        return rp, cc[: nz.value], vv[: nz.value], nd.value
+
+    def levels(self):
+        n = self.n
+        fl = np.empty(n, np.int32)
+        bl = np.empty(n, np.int32)
+        nf, nb = C.c_int32(), C.c_int32()
+        check(lib().fv_precond_levels(self.handle, fl.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      bl.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(nf), C.byref(nb), None),
+              "levels")
+        return fl, bl, nf.value, nb.value
+
+    def refactor(self, stream=None):
+        """Value-only refactorisation after the matrix values changed."""
+        check(lib().fv_precond_refactor(self.handle, stream_handle(stream)), "refactor")
+
+    def close(self):
+        if self.handle:
+            lib().fv_precond_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class IncompleteCholesky(Preconditioner):
+    def __init__(self, handle, n, matrix):
+        self.handle, self.n, self._m = handle, n, matrix
+
+    @classmethod
+    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteCholesky":
+        if level != 0:
+            raise NotImplementedError("IC(k) with k > 0 is not implemented on the device path")
+        h = C.c_void_p()
+        check(lib().fv_ic0_factor(matrix.handle, stream_handle(stream), C.byref(h)), "IncompleteCholesky")
+        return cls(h, matrix.nrows(), matrix)
+
+
+class IncompleteLowerUpper(Preconditioner):
+    def __init__(self, handle, n, matrix):
+        self.handle, self.n, self._m = handle, n, matrix
+
+    @classmethod
+    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteLowerUpper":
+        if level != 0:
+            raise NotImplementedError("ILU(k) with k > 0 is not implemented on the device path")
+        h = C.c_void_p()
+        check(lib().fv_ilu0_factor(matrix.handle, stream_handle(stream), C.byref(h)), "IncompleteLowerUpper")
+        return cls(h, matrix.nrows(), matrix)
+
+
+class IdentityPreconditioner(Preconditioner):
+    handle = C.c_void_p()
+
+
+@dataclass
+class LinearSolverOptions:
+    relative_tolerance: float = 1e-6
+    absolute_tolerance: float = 1e-6
+    max_iterations: int = 1000
+
+    def c(self) -> SolverOptions:
+        return SolverOptions(self.relative_tolerance, self.absolute_tolerance, self.max_iterations)
+
+
+@dataclass
+class LinearSolverInfo:
+    solver_identifier: str
+    iterations: int
+    initial_residual: float
+    final_residual: float
+    history: list = field(default_factory=list)
+    status: int = 0
+    restarts: int = 0
+    device_ms: float = 0.0
+
+    def __str__(self):
+        return (f"(solver={self.solver_identifier}, iterations={self.iterations}, "
+                f"initial_residual={self.initial_residual:.3e}, final_residual={self.final_residual:.3e})")
+
+
+def _solve(fn, name, solution, lhs, rhs, preconditioner, options, stream):
+    options = options or LinearSolverOptions()
+    cap = int(options.max_iterations) + 2
+    hist = np.zeros(cap, np.float64)
+    info = SolverInfo()
+    info.history = hist.ctypes.data_as(C.POINTER(C.c_double))
+    info.history_cap = cap
+    b = _dev_f64(rhs)
+    ph = preconditioner.handle if preconditioner is not None else C.c_void_p()
+    st = fn(lhs.handle, ph, C.c_void_p(b.data_ptr()), solution.ptr(), options.c(), C.byref(info),
+            stream_handle(stream))
+    if st not in (0, 4):  # breakdown is reported in the info, as the reference returns Ok with NaN residuals
+        raise FvError(st, name)
+    return LinearSolverInfo(name, int(info.iterations), float(info.initial_residual), float(info.final_residual),
+                            hist[: min(int(info.history_len), cap)].tolist(), int(info.status), int(info.restarts),
+                            float(info.device_ms))
+
+
+def conjugate_gradient(solution: DistributedVector, lhs: DistributedMatrix, rhs, preconditioner=None, comm=None,
+                       options: LinearSolverOptions | None = None, stream=None) -> LinearSolverInfo:
+    return _solve(lib().fv_cg, "ConjugateGradient", solution, lhs, rhs, preconditioner, options, stream)
+
+
+def bi_conjugate_gradient_stab(solution: DistributedVector, lhs: DistributedMatrix, rhs, preconditioner=None,
+                               comm=None, options: LinearSolverOptions | None = None,
+                               stream=None) -> LinearSolverInfo:
+    return _solve(lib().fv_bicgstab, "BiConjugateGradientStab", solution, lhs, rhs, preconditioner, options, stream)

@@ -1,0 +1,230 @@
+/*
+ * fv_b200.h -- C ABI of the B200 assembly + sparse Krylov path.
+ *
+ * This library replaces, behind a plain C boundary, the hot path of the
+ * finite-volumes crate (x318aVkl/finite-volumes-rs):
+ *
+ *   fvm::assembly::assemble                      src/fvm/assembly.rs:11-78
+ *   DistributedMatrix::imul (CSR SpMV)           src/linalg/dmatrix.rs:136-146
+ *   IncompleteCholesky::from_matrix (IC(0))      src/linalg/preconditioners/incomplete_cholesky.rs:205
+ *   IncompleteLowerUpper::from_matrix (ILU(0))   src/linalg/preconditioners/incomplete_lower_upper.rs:266
+ *   Preconditioner::precondition                 src/linalg/preconditioners/mod.rs:13-17
+ *   solvers::conjugate_gradient                  src/linalg/solvers/conjugate_gradient.rs:12-111
+ *   solvers::bi_conjugate_gradient_stab          src/linalg/solvers/bi_conjugate_gradient_stab.rs:13-178
+ *
+ * Conventions
+ *   - Every call returns an fv_status; nothing aborts the process.  Invariant
+ *     violations that the reference turns into a panic (missing matrix entry,
+ *     ILU pivot below 1e-16, IC on a non-symmetric matrix) are returned as
+ *     FV_ERR_INVALID / FV_ERR_SINGULAR_PIVOT / FV_ERR_NOT_SYMMETRIC.
+ *   - Non-convergence is not an error (as in the reference): check
+ *     fv_solver_info.iterations / final_residual.
+ *   - Handles are opaque, single-stream and not thread-safe (the reference is
+ *     single-threaded per MPI rank).  `stream` is a cudaStream_t passed as
+ *     void*; 0 means the legacy default stream.
+ *   - Device pointers are used for vectors unless the function name ends in
+ *     _host, in which case host memory is read/written and the copies happen
+ *     inside the call.
+ *   - Scalars are FP64 and indices int32, cells/faces numbered as in the
+ *     reference's Mesh.  Arithmetic follows the reference's operation order
+ *     without fused multiply-add, so assembly, SpMV, factorisation and the
+ *     triangular sweeps reproduce the reference bit for bit; only reductions
+ *     (dot products) are summed in a different (fixed, deterministic) order.
+ */
+#ifndef FV_B200_H
+#define FV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Mirrors the panics / Result of the reference (core/error.rs:4-21). */
+typedef enum fv_status {
+    FV_OK = 0,
+    FV_ERR_ALLOC = 1,          /* device or host allocation failed */
+    FV_ERR_INVALID = 2,        /* bad argument, corrupted CSR, missing matrix entry */
+    FV_ERR_SINGULAR_PIVOT = 3, /* ILU |u_kk| < 1e-16 (incomplete_lower_upper.rs:234-235) */
+    FV_ERR_BREAKDOWN = 4,      /* Krylov breakdown: NaN/Inf scalar detected on the device */
+    FV_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
+    FV_ERR_NOT_SYMMETRIC = 6,  /* IC on a matrix failing |a_ij-a_ji|<1e-14 (incomplete_cholesky.rs:153) */
+    FV_ERR_CUDA = 7,           /* a CUDA runtime call failed */
+    FV_ERR_UNSUPPORTED = 8     /* feature outside the implemented scope (e.g. level>0) */
+} fv_status;
+
+/* ------------------------------------------------------------------------ */
+/* Host-side mesh (the stand-in for the reference's Mesh<DIM> after
+ * Mesh::compute).  Produced by the generators below or built from an element
+ * list; numbering and geometry follow core/mesh/io.rs:364-486
+ * (compute_vtk_faces), core/mesh/mod.rs:451-529 (add_face/add_cell) and
+ * core/mesh/compute.rs:12-375 (face/cell geometry, orientation).            */
+typedef struct fv_host_mesh {
+    int32_t dim;              /* 2 or 3 */
+    int64_t n_nodes;
+    int64_t n_faces;          /* interior faces first, boundary faces last */
+    int64_t n_cells;
+    int64_t n_boundary_faces; /* boundary faces are [n_faces-n_boundary_faces, n_faces) */
+    double  *nodes;           /* n_nodes*dim */
+    int32_t *face_node_ptr;   /* n_faces+1 */
+    int32_t *face_nodes;
+    int32_t *face_patch;      /* n_faces; -1 for interior faces, else marker id */
+    int32_t *cell_face_ptr;   /* n_cells+1 */
+    int32_t *cell_faces;      /* faces of each cell in element-local order */
+    int32_t *face_owner;      /* n_faces */
+    int32_t *face_neighbor;   /* n_faces; -1 for boundary faces */
+    double  *face_area;       /* n_faces */
+    double  *face_normal;     /* n_faces*dim (3D: |n| = 1/3 for triangles, as the reference) */
+    double  *face_center;     /* n_faces*dim */
+    double  *cell_center;     /* n_cells*dim */
+    double  *cell_volume;     /* n_cells */
+} fv_host_mesh;
+
+/* Build from an element list, as Mesh::read_su2 does (io.rs:489-533).
+ * elem_kind uses VTK ids: 5 triangle, 9 quad, 10 tetrahedron, 12 hexahedron.
+ * Boundary faces are given as node lists with a marker id (SU2 MARKER_ELEMS). */
+fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, const double *nodes,
+                                     int64_t n_elems, const int32_t *elem_kind,
+                                     const int32_t *elem_node_ptr, const int32_t *elem_nodes,
+                                     int64_t n_bfaces, const int32_t *bface_node_ptr,
+                                     const int32_t *bface_nodes, const int32_t *bface_marker,
+                                     fv_host_mesh **out);
+
+/* Unit square, n x n squares each split into 2 triangles along the (i,j)-(i+1,j+1)
+ * diagonal, interior nodes jittered by U(-jitter*h, jitter*h) per coordinate. */
+fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out);
+
+/* Unit cube, n^3 hexes each split into 6 Kuhn tetrahedra (same orientation in
+ * every hex), interior nodes jittered by U(-jitter*h, jitter*h). */
+fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out);
+
+void fv_host_mesh_free(fv_host_mesh *m);
+
+/* Seeded synthetic fields on a host mesh.
+ *   cell diffusivity kappa_c = kappa0 * exp(sigma * z), z ~ N(0,1)
+ *   face diffusivity: linear interpolation weights of faceinterp/linear.rs:25-42
+ *     (w clamped to [0,1]); boundary faces take the owner value
+ *   flux_f = velocity . normal_f (reference normal)
+ *   source_c = source_const if source_uniform==0, else U(0,1)
+ * Any output pointer may be NULL. */
+fv_status fv_host_fields_generate(const fv_host_mesh *m, uint64_t seed, double kappa0, double sigma,
+                                  const double *velocity, double source_const, int32_t source_uniform,
+                                  double *kappa_face, double *flux_face, double *source_cell);
+
+/* ------------------------------------------------------------------------ */
+/* Device objects                                                            */
+typedef struct fv_mesh fv_mesh;       /* device-resident geometry + cell->face table */
+typedef struct fv_csr fv_csr;         /* device CSR matrix, FP64 values, int32 indices */
+typedef struct fv_precond fv_precond; /* IC(0) / ILU(0) factors + level schedules */
+
+typedef struct fv_mesh_desc {
+    int32_t dim;
+    int64_t n_cells;
+    int64_t n_faces;
+    int64_t n_boundary_faces;     /* boundary faces are the tail of the face list */
+    const int32_t *face_owner;    /* host pointers; copied by fv_mesh_upload */
+    const int32_t *face_neighbor; /* -1 = boundary */
+    const double  *face_area;
+    const double  *face_center;   /* n_faces*dim */
+    const double  *cell_center;   /* n_cells*dim */
+    const double  *cell_volume;
+} fv_mesh_desc;
+
+/* The term expression c_conv*convection(Upwind(F),F) + c_lap*laplacian(Orthogonal,kappa)
+ * + c_src*source(f) of fvm/terms (laplacian.rs:35-45, convection.rs:36-45,
+ * source.rs:34-40, operations.rs:86-199).  Coefficients must be -1, 0 or +1
+ * (the reference's term algebra has +, - and unary - only). */
+typedef struct fv_terms_desc {
+    double laplacian_coef;
+    double convection_coef;
+    double source_coef;
+    const double *diffusivity; /* n_faces, device (fv_assemble) or host (_host) */
+    const double *flux;        /* n_faces */
+    const double *source;      /* n_cells */
+} fv_terms_desc;
+
+/* Boundary closure value_b = bndi*value_i + bnde per boundary face
+ * (assembly.rs:64-73, bcs/mod.rs:33).  Dirichlet g: (0,g); zero gradient: (1,0). */
+typedef struct fv_bc_desc {
+    const double *bndi; /* n_boundary_faces */
+    const double *bnde; /* n_boundary_faces */
+} fv_bc_desc;
+
+/* LinearSolverOptions (solvers/mod.rs:22-35). */
+typedef struct fv_solver_options {
+    double relative_tolerance;
+    double absolute_tolerance;
+    int64_t max_iterations;
+} fv_solver_options;
+
+/* LinearSolverInfo (solvers/mod.rs:11-17) plus device-side status. */
+typedef struct fv_solver_info {
+    int64_t iterations;
+    double initial_residual;
+    double final_residual;
+    int32_t status;        /* fv_status of the solve (BREAKDOWN, TIMEOUT, ...) */
+    int32_t restarts;      /* BiCGStab restarts (bi_conjugate_gradient_stab.rs:155-169) */
+    double *history;       /* optional caller buffer for the per-iteration residual */
+    int64_t history_cap;   /* capacity of history (0 = do not record) */
+    int64_t history_len;   /* entries written */
+    double device_ms;      /* device time of the solve, CUDA events */
+} fv_solver_info;
+
+fv_status fv_mesh_upload(const fv_mesh_desc *desc, void *stream, fv_mesh **out);
+fv_status fv_mesh_destroy(fv_mesh *m);
+
+/* assemble(): builds the CSR pattern of cell_to_cell (dmatrix.rs:38-50) on the
+ * first call (*A == NULL) and refills values into the existing pattern when
+ * *A is a matrix returned by an earlier call on the same mesh.
+ * terms/bc pointers are device pointers; b is a device vector of n_cells. */
+fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const fv_bc_desc *bc,
+                      fv_csr **A, double *b, void *stream);
+fv_status fv_assemble_host(fv_mesh *m, const fv_terms_desc *terms, const fv_bc_desc *bc,
+                           fv_csr **A, double *b_host, void *stream);
+
+/* Generic CSR from host arrays (sorted columns per row required). */
+fv_status fv_csr_create_host(int64_t nrows, int64_t ncols, const int32_t *row_ptr,
+                             const int32_t *cols, const double *vals, void *stream, fv_csr **out);
+fv_status fv_csr_info(const fv_csr *A, int64_t *nrows, int64_t *ncols, int64_t *nnz);
+fv_status fv_csr_download(const fv_csr *A, int32_t *row_ptr, int32_t *cols, double *vals, void *stream);
+fv_status fv_csr_destroy(fv_csr *A);
+
+/* y = A x (DistributedMatrix::imul, dmatrix.rs:136-146); bit-exact per row. */
+fv_status fv_spmv(const fv_csr *A, const double *x, double *y, void *stream);
+fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double *y_host, void *stream);
+
+/* IncompleteCholesky::from_matrix(A, 0) / IncompleteLowerUpper::from_matrix(A, 0). */
+fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out);
+fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out);
+/* z = M^-1 r (Preconditioner::precondition).  r and z must not alias. */
+fv_status fv_precond_apply(fv_precond *P, const double *r, double *z, void *stream);
+fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, double *z_host, void *stream);
+/* Export of the stored factors (ILU: dropped entries removed).  Pass NULL
+ * arrays to query sizes (nnz_lower, nnz_upper).  IC: lower = L incl. diagonal
+ * as the reference's `l`; ILU: lower = strict L, upper = U incl. diagonal,
+ * merged per row exactly as the reference's single `lu` CSR when merged=1. */
+fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr, int32_t *cols,
+                            double *vals, int32_t *n_dropped, void *stream);
+/* Level schedules: level of every row in the forward (lower) and backward (upper) DAG. */
+fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,
+                            int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream);
+fv_status fv_precond_destroy(fv_precond *P);
+
+/* conjugate_gradient / bi_conjugate_gradient_stab.  x is the initial guess on
+ * input and the solution on output (device vectors).  P may be NULL (identity). */
+fv_status fv_cg(const fv_csr *A, fv_precond *P, const double *b, double *x,
+                fv_solver_options opt, fv_solver_info *info, void *stream);
+fv_status fv_bicgstab(const fv_csr *A, fv_precond *P, const double *b, double *x,
+                      fv_solver_options opt, fv_solver_info *info, void *stream);
+fv_status fv_cg_host(const fv_csr *A, fv_precond *P, const double *b_host, double *x_host,
+                     fv_solver_options opt, fv_solver_info *info, void *stream);
+fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const double *b_host, double *x_host,
+                           fv_solver_options opt, fv_solver_info *info, void *stream);
+
+/* Human-readable name of a status. */
+const char *fv_status_string(fv_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FV_B200_H */

@@ -1,0 +1,188 @@
+"""CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of oracle/liboracle.so, the single-threaded FP64 C
+restatement of the finite-volumes crate's assemble / SpMV / IC(0) / ILU(0) /
+CG / BiCGStab (see oracle/oracle.c for the file:line map).  Used only by
+tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, as the
+checker and the timed CPU baseline; the product library never calls it.
+
+Parity status: assembly, factorisation and Krylov results are parity-unpinned
+against the reference itself (the reference has no tests for them and cannot
+be built here); the oracle is cross-checked against SciPy and hand-derived
+coefficients in tests/, and the mesh geometry it consumes is pinned by the
+reference's square.su2 known-answer test.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB, build
+
+_L = None
+P = C.POINTER
+dp, ip, i64, vp = P(C.c_double), P(C.c_int32), C.c_int64, C.c_void_p
+
+
+class OrInfo(C.Structure):
+    _fields_ = [("iterations", i64), ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("history_len", i64), ("restarts", C.c_int32)]
+
+
+def lib():
+    global _L
+    if _L is None:
+        build()
+        L = C.CDLL(str(LIB))
+        sig = {
+            "or_pattern": ([i64, ip, ip, ip, ip, ip, ip, P(i64)], C.c_int),
+            "or_assemble": ([C.c_int32, i64, i64, i64, ip, ip, dp, dp, dp, dp, C.c_double, C.c_double, C.c_double,
+                             dp, dp, dp, dp, dp, ip, ip, dp, dp], C.c_int),
+            "or_spmv": ([i64, ip, ip, dp, dp, dp], None),
+            "or_dot": ([i64, dp, dp], C.c_double),
+            "or_ic0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
+            "or_ilu0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
+            "or_precond_apply": ([vp, dp, dp], None),
+            "or_precond_free": ([vp], None),
+            "or_precond_nnz": ([vp], i64),
+            "or_precond_ndropped": ([vp], i64),
+            "or_precond_export": ([vp, ip, ip, dp, dp], None),
+            "or_levels": ([i64, ip, ip, C.c_int32, ip], C.c_int32),
+            "or_cg": ([i64, ip, ip, dp, vp, dp, dp, C.c_double, C.c_double, i64, dp, i64, P(OrInfo)], C.c_int),
+            "or_bicgstab": ([i64, ip, ip, dp, vp, dp, dp, C.c_double, C.c_double, i64, dp, i64, P(OrInfo)],
+                            C.c_int),
+        }
+        for k, (a, r) in sig.items():
+            f = getattr(L, k)
+            f.argtypes = a
+            f.restype = r
+        _L = L
+    return _L
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _pi(a):
+    return a.ctypes.data_as(ip)
+
+
+def _pd(a):
+    return a.ctypes.data_as(dp)
+
+
+def pattern(mesh):
+    """CSR pattern of cell_to_cell (rows sorted)."""
+    cfp, cf, ow, nb = _i(mesh.cell_face_ptr), _i(mesh.cell_faces), _i(mesh.face_owner), _i(mesh.face_neighbor)
+    nnz = C.c_int64()
+    rc = lib().or_pattern(mesh.n_cells, _pi(cfp), _pi(cf), _pi(ow), _pi(nb), None, None, C.byref(nnz))
+    assert rc == 0
+    ptr = np.empty(mesh.n_cells + 1, np.int32)
+    cols = np.empty(max(nnz.value, 1), np.int32)
+    rc = lib().or_pattern(mesh.n_cells, _pi(cfp), _pi(cf), _pi(ow), _pi(nb), _pi(ptr), _pi(cols), C.byref(nnz))
+    assert rc == 0
+    return ptr, cols[: nnz.value]
+
+
+def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bndi=None, bnde=None):
+    """assemble() restated: returns (row_ptr, cols, vals, rhs)."""
+    ptr, cols = pattern(mesh)
+    F, N, Fb = mesh.n_faces, mesh.n_cells, mesh.n_boundary_faces
+    z = lambda n: np.zeros(max(n, 1))  # noqa: E731
+    kappa = _d(kappa) if kappa is not None else z(F)
+    flux = _d(flux) if flux is not None else z(F)
+    source = _d(source) if source is not None else z(N)
+    bndi = _d(bndi) if bndi is not None else z(Fb)
+    bnde = _d(bnde) if bnde is not None else z(Fb)
+    vals = np.empty(len(cols))
+    rhs = np.empty(N)
+    rc = lib().or_assemble(mesh.dim, N, F, Fb, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
+                           _pd(_d(mesh.face_area)), _pd(_d(mesh.face_center)), _pd(_d(mesh.cell_center)),
+                           _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src, _pd(kappa), _pd(flux), _pd(source),
+                           _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols), _pd(vals), _pd(rhs))
+    if rc != 0:
+        raise RuntimeError(f"oracle assemble failed: {rc}")
+    return ptr, cols, vals, rhs
+
+
+def spmv(ptr, cols, vals, x):
+    ptr, cols, vals, x = _i(ptr), _i(cols), _d(vals), _d(x)
+    y = np.empty(len(ptr) - 1)
+    lib().or_spmv(len(ptr) - 1, _pi(ptr), _pi(cols), _pd(vals), _pd(x), _pd(y))
+    return y
+
+
+def dot(a, b):
+    a, b = _d(a), _d(b)
+    return lib().or_dot(len(a), _pd(a), _pd(b))
+
+
+class Precond:
+    """IncompleteCholesky / IncompleteLowerUpper restated (level 0)."""
+
+    def __init__(self, kind, ptr, cols, vals):
+        self.n = len(ptr) - 1
+        self._keep = (_i(ptr), _i(cols), _d(vals))
+        st = C.c_int()
+        f = lib().or_ic0_create if kind == "ic" else lib().or_ilu0_create
+        self.h = f(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]), C.byref(st))
+        self.status = st.value
+        self.kind = kind
+
+    def ok(self):
+        return bool(self.h)
+
+    def apply(self, r):
+        r = _d(r)
+        z = np.zeros(self.n)
+        lib().or_precond_apply(self.h, _pd(r), _pd(z))
+        return z
+
+    def export(self):
+        nz = lib().or_precond_nnz(self.h)
+        ptr = np.empty(self.n + 1, np.int32)
+        cols = np.empty(max(nz, 1), np.int32)
+        vals = np.empty(max(nz, 1))
+        inv = np.empty(self.n)
+        lib().or_precond_export(self.h, _pi(ptr), _pi(cols), _pd(vals), _pd(inv))
+        return ptr, cols[:nz], vals[:nz], inv, lib().or_precond_ndropped(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_precond_free(self.h)
+            self.h = None
+
+
+def levels(ptr, cols, upper=False):
+    ptr, cols = _i(ptr), _i(cols)
+    lev = np.empty(len(ptr) - 1, np.int32)
+    nl = lib().or_levels(len(ptr) - 1, _pi(ptr), _pi(cols), 1 if upper else 0, _pi(lev))
+    return lev, nl
+
+
+def _solve(fn, ptr, cols, vals, pc, b, x0, rtol, atol, maxit):
+    ptr, cols, vals, b = _i(ptr), _i(cols), _d(vals), _d(b)
+    x = _d(x0).copy() if x0 is not None else np.zeros(len(b))
+    hist = np.zeros(maxit + 3)
+    info = OrInfo()
+    rc = fn(len(b), _pi(ptr), _pi(cols), _pd(vals), pc.h if pc is not None else None, _pd(b), _pd(x), rtol, atol,
+            maxit, _pd(hist), len(hist), C.byref(info))
+    assert rc == 0
+    return x, {"iterations": info.iterations, "initial_residual": info.initial_residual,
+               "final_residual": info.final_residual, "history": hist[: info.history_len].tolist(),
+               "restarts": info.restarts}
+
+
+def cg(ptr, cols, vals, pc, b, x0=None, rtol=1e-6, atol=1e-6, maxit=1000):
+    return _solve(lib().or_cg, ptr, cols, vals, pc, b, x0, rtol, atol, maxit)
+
+
+def bicgstab(ptr, cols, vals, pc, b, x0=None, rtol=1e-6, atol=1e-6, maxit=1000):
+    return _solve(lib().or_bicgstab, ptr, cols, vals, pc, b, x0, rtol, atol, maxit)
