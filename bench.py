@@ -1,0 +1,462 @@
+#!/usr/bin/env python3
+"""Benchmark of the assemble + ILU(0)/IC(0) + Krylov hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+One step = one pass of the hot path over one synthetic problem: value
+assembly into the resident CSR pattern, ILU(0) (IC(0)) factorisation and a
+BiCGStab (CG) solve to rtol = atol = 1e-8, all FP64.  At N GPUs every rank
+solves its own seeded problem (independent replicas, weak scaling, no
+data-path collective); `value` is the solves/s of the whole job, timed on the
+device with CUDA events between barriers and taken as the max over ranks.
+
+`--impl reference` times the CPU arm instead: the reference crate cannot be
+built here (no Rust toolchain, no MPI), so the arm runs the oracle's C
+restatement of the reference's MPI algorithm (block-Jacobi ILU/IC over
+contiguous partitions, one OpenMP thread per rank) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "finite-volumes-rs_b200"))
+
+METRIC = "solves/s and DOF-iters/s vs plain FP64 at rel err <=1e-8; p50/p99 solve latency"
+
+WORKLOADS = {
+    # BASELINE configuration "plain FP64 3D convection-diffusion", 128^3 hexes x 6 tets
+    "cube128_convdiff": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
+    # the CPU-runnable 2D case: 256x256 squares x 2 triangles, lognormal(0,1)
+    "square256_diffusion": dict(kind="2d", n=256, jitter=0.2, sigma=1.0, solver="cg"),
+    # small versions for smoke runs
+    "cube32_convdiff": dict(kind="3d", n=32, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
+}
+RTOL = 1e-8
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_problem(fv, wl, seed):
+    if wl["kind"] == "3d":
+        m = fv.Mesh.cube(wl["n"], wl["jitter"], seed)
+        kappa0 = float(np.linalg.norm(wl["velocity"])) * (1.0 / wl["n"]) / 3.0
+        kf, fl, sc = m.fields(seed, kappa0, wl["sigma"], velocity=wl["velocity"], source_uniform=True)
+        coef = (-1.0, 1.0, -1.0)
+    else:
+        m = fv.Mesh.square(wl["n"], wl["jitter"], seed)
+        kf, _, sc = m.fields(seed, 1.0, wl["sigma"], source_const=1.0)
+        fl = None
+        coef = (-1.0, 0.0, -1.0)
+    nb = m.n_boundary_faces
+    return dict(mesh=m, kappa=kf, flux=fl, source=sc, bndi=np.zeros(nb), bnde=np.zeros(nb), coef=coef)
+
+
+def equation(fv, prob, tensors):
+    lap = fv.laplacian(fv.Orthogonal(), tensors["kappa"])
+    src = fv.source(tensors["source"])
+    if prob["coef"][1] != 0.0:
+        return fv.convection(fv.Upwind(tensors["flux"]), tensors["flux"]) - lap - src
+    return -lap - src
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            out = ROOT / "gpurun_out"
+            out.mkdir(exist_ok=True)
+            self.path = out / f"clocks_rank{self.index}.csv"
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def time_kernel(torch, fn, reps, stream):
+    """Average device time of fn() over reps launches, CUDA events on `stream`."""
+    for _ in range(2):
+        fn()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps / 1e3
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    from fvb200.build import build
+    if rank == 0:
+        build()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    build()
+    import fvb200 as fv
+    from fvb200._lib import lib
+    wl = WORKLOADS[args.workload]
+    t0 = time.time()
+    prob = make_problem(fv, wl, seed=1000 + rank)
+    mesh = prob["mesh"]
+    t_mesh = time.time() - t0
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream()
+    T = {k: torch.as_tensor(prob[k], device=dev) for k in ("kappa", "source", "bndi", "bnde")}
+    T["flux"] = torch.as_tensor(prob["flux"], device=dev) if prob["flux"] is not None else None
+    eq = equation(fv, prob, T)
+    bc = (T["bndi"], T["bnde"])
+    Pcls = fv.IncompleteLowerUpper if wl["solver"] == "bicgstab" else fv.IncompleteCholesky
+    solve = fv.bi_conjugate_gradient_stab if wl["solver"] == "bicgstab" else fv.conjugate_gradient
+    opts = fv.LinearSolverOptions(RTOL, RTOL, 10000)
+    N = mesh.n_cells
+
+    # first pass builds the resident pattern, symbolic analysis and factor storage
+    A, b = fv.assemble(eq, bc, mesh)
+    P = Pcls.from_matrix(A, 0)
+    x = fv.DistributedVector.from_size(N)
+
+    # one step: value assembly (new rhs), refactorisation, solve from x0 = 0
+    def step_b():
+        nonlocal b
+        _, b = fv.assemble(eq, bc, mesh, lhs=A)
+        P.refactor()
+        x.data.zero_()
+        return solve(x, A, b, P, None, opts)
+
+    for _ in range(args.warmup):
+        info = step_b()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clk = Clocks(local_rank)
+    clk.start()
+    torch.cuda.synchronize()
+    L0 = lib().fv_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lat = []
+    iters = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        info = step_b()
+        s1.record(stream)
+        iters.append(info.iterations)
+        lat.append((s0, s1))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib().fv_launch_count() - L0
+    clocks = clk.stop()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    lat_ms = [a.elapsed_time(c) for a, c in lat]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    # correctness of the last step: true residual of the solution
+    r = fv.DistributedVector.from_size(N)
+    A.imul(r, x)
+    relres = float(torch.linalg.norm(r.data - b.data) / torch.linalg.norm(b.data))
+
+    # ---- end to end through the public API with host buffers
+    pin = {k: torch.empty(len(prob[k]), dtype=torch.float64).pin_memory()
+           for k in ("kappa", "source", "bndi", "bnde") + (("flux",) if prob["flux"] is not None else ())}
+    for k, t in pin.items():
+        t.copy_(torch.from_numpy(prob[k]))
+    x_host = torch.empty(N, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * 8 for t in pin.values())
+
+    def e2e_step():
+        for k, t in pin.items():
+            T[k].copy_(t, non_blocking=True)
+        _, bb = fv.assemble(eq, bc, mesh, lhs=A)
+        P.refactor()
+        x.data.zero_()
+        solve(x, A, bb, P, None, opts)
+        x_host.copy_(x.data, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_elapsed = e2.elapsed_time(e3) / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+
+    # ---- per-kernel timing of the hot kernels (roofline)
+    _, _, nnz = A.shape()
+    y = fv.DistributedVector.from_size(N)
+    z = fv.DistributedVector.from_size(N)
+    hbm, peak_kind = peaks()
+    t_spmv = time_kernel(torch, lambda: A.imul(y, x), 20, stream)
+    t_prec = time_kernel(torch, lambda: P.precondition(z, b), 10, stream)
+    t_asm = time_kernel(torch, lambda: fv.assemble(eq, bc, mesh, lhs=A), 10, stream)
+    t_fac = time_kernel(torch, lambda: P.refactor(), 3, stream)
+    F, Fb = mesh.n_faces, mesh.n_boundary_faces
+    bytes_spmv = 12 * nnz + 20 * N
+    bytes_prec = 12 * nnz + 40 * N
+    bytes_asm = 32 * F + 24 * Fb + 40 * N + 8 * (F - Fb) + 8 * nnz + 8 * N
+    it_mean = float(np.mean(iters))
+    per_it_spmv = 2 if wl["solver"] == "bicgstab" else 1
+    # share of a step spent in each kernel class (device time), to pick the dominant one
+    step_s = elapsed / args.steps
+    share = {
+        "precond_apply": t_prec * per_it_spmv * it_mean / step_s,
+        "spmv": t_spmv * per_it_spmv * it_mean / step_s,
+        "assembly": t_asm / step_s,
+        "factor": t_fac / step_s,
+    }
+    kern = {
+        "precond_apply": (bytes_prec, t_prec), "spmv": (bytes_spmv, t_spmv), "assembly": (bytes_asm, t_asm),
+    }
+    dom = max(("precond_apply", "spmv", "assembly"), key=lambda k: share[k])
+    bts, tk = kern[dom]
+    ach = bts / tk / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "traffic": None,
+            "algorithmic_bytes": int(bts), "launch_ms": round(tk * 1e3, 4)}
+    others = {k: {"achieved_gbs": round(kern[k][0] / kern[k][1] / 1e9, 1), "frac": round(kern[k][0] / kern[k][1] / 1e9 / hbm, 4),
+                  "launch_ms": round(kern[k][1] * 1e3, 4), "algorithmic_bytes": int(kern[k][0])} for k in kern}
+    res = dict(
+        elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
+        e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
+        kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
+        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A,
+    )
+    return res
+
+
+def cpu_sample(prob, wl, threads, iters_hint, mpi_like):
+    """Time the oracle on a bounded sample of the workload and scale to solves/s.
+
+    Sample: full assembly + full factorisation of the same problem, then a few
+    Krylov iterations; one solve = assembly + factorisation + `iters_hint`
+    iterations (the GPU's count of the same solve)."""
+    import oracle
+    m = prob["mesh"]
+    c = prob["coef"]
+    t0 = time.perf_counter()
+    ptr, cols, vals, rhs = oracle.assemble(m, c[0], c[1], c[2], kappa=prob["kappa"], flux=prob["flux"],
+                                           source=prob["source"], bndi=prob["bndi"], bnde=prob["bnde"])
+    t_asm = time.perf_counter() - t0
+    kind = "ilu" if wl["solver"] == "bicgstab" else "ic"
+    solver = oracle.bicgstab if wl["solver"] == "bicgstab" else oracle.cg
+    if mpi_like:
+        from oracle import mpi as ompi
+        t0 = time.perf_counter()
+        pc = ompi.BlockJacobi(kind, ptr, cols, vals, threads)
+        t_fac = time.perf_counter() - t0
+        k = 3
+        t0 = time.perf_counter()
+        _, info = ompi.solve(wl["solver"], ptr, cols, vals, pc, rhs, RTOL, RTOL, k, threads)
+        t_it = (time.perf_counter() - t0) / max(info["iterations"], 1)
+        iters = iters_hint
+        sample = (f"{wl['solver']}+block-Jacobi {kind.upper()}(0) over {threads} contiguous partitions "
+                  f"(one OpenMP thread per rank), full assembly + factorisation + {info['iterations']} "
+                  f"iterations timed, scaled to {iters} iterations per solve")
+    else:
+        t0 = time.perf_counter()
+        pc = oracle.Precond(kind, ptr, cols, vals)
+        t_fac = time.perf_counter() - t0
+        k = 3
+        t0 = time.perf_counter()
+        _, info = solver(ptr, cols, vals, pc, rhs, rtol=1e-30, atol=1e-30, maxit=k - 1)
+        t_it = (time.perf_counter() - t0) / max(info["iterations"], 1)
+        iters = iters_hint
+        sample = (f"oracle (1 thread): full assembly + full {kind.upper()}(0) factorisation + "
+                  f"{info['iterations']} {wl['solver']} iterations timed, scaled to {iters} iterations per solve")
+    t_solve = t_asm + t_fac + iters * t_it
+    return dict(t_solve=t_solve, t_asm=t_asm, t_fac=t_fac, t_it=t_it, sample=sample, iters=iters)
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "finite-volumes-rs_b200"))
+    from fvb200.build import build
+    build()
+    import fvb200 as fv
+    import oracle
+    oracle.lib()
+    wl = WORKLOADS[args.workload]
+    prob = make_problem(fv, wl, seed=1000)
+    threads = os.cpu_count() or 1
+    # iteration count of the block-Jacobi solve at this thread count, measured once (bounded)
+    from oracle import mpi as ompi
+    c = prob["coef"]
+    ptr, cols, vals, rhs = oracle.assemble(prob["mesh"], c[0], c[1], c[2], kappa=prob["kappa"], flux=prob["flux"],
+                                           source=prob["source"], bndi=prob["bndi"], bnde=prob["bnde"])
+    kind = "ilu" if wl["solver"] == "bicgstab" else "ic"
+    iters = ompi.iterations_estimate(wl["solver"], kind, ptr, cols, vals, rhs, RTOL, threads, budget_s=60.0)
+    times = []
+    for _ in range(args.warmup):
+        pass
+    res = None
+    for _ in range(max(1, min(args.steps, 2))):
+        res = cpu_sample(prob, wl, threads, iters, mpi_like=True)
+        times.append(res["t_solve"])
+    t = float(np.median(times))
+    value = 1.0 / t
+    N = prob["mesh"].n_cells
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(args, wl, N, None),
+        "dof_iters_per_s": round(N * iters / t, 1),
+        "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": res["sample"]},
+        "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference crate not buildable here (no Rust toolchain, no MPI): C restatement of its MPI "
+                "block-Jacobi algorithm on all host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl, N, nnz):
+    return {"workload": args.workload, "cells": N, "nnz": nnz, "dim": 3 if wl["kind"] == "3d" else 2,
+            "solver": f"{wl['solver']}+{'ilu0' if wl['solver'] == 'bicgstab' else 'ic0'}", "rtol": RTOL,
+            "atol": RTOL, "precision": "fp64", "l2": "inputs larger than L2 (no flush needed)"
+            if N > 1_000_000 else "working set fits L2; reported as effective bandwidth",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="cube128_convdiff", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    res = gpu_arm(args, rank, world, local_rank)
+    wl = WORKLOADS[args.workload]
+    K = args.steps
+    solves = K * world
+    value = solves / res["elapsed"]
+    it_mean = float(np.mean(res["iters"]))
+    N = res["N"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cs = cpu_sample(res["prob"], wl, 1, int(round(it_mean)), mpi_like=False)
+            cpu = {"value": round(1.0 / cs["t_solve"], 6), "unit": "solves/s", "cores": 1, "kind": "port",
+                   "sample": cs["sample"]}
+        except Exception as e:  # pragma: no cover - reported, not fatal
+            cpu = {"value": None, "unit": "solves/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+    lat = sorted(res["lat_ms"])
+    line = {
+        "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(res["elapsed"] / K * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(args, wl, N, res["nnz"]),
+        "dof_iters_per_s": round(N * it_mean * solves / res["elapsed"], 1),
+        "iterations": res["iters"], "p50_ms": round(float(np.percentile(lat, 50)), 3),
+        "p99_ms": round(float(np.percentile(lat, 99)), 3), "true_rel_residual": res["relres"],
+        "roofline": res["roofline"], "kernels": res["kernels"], "time_share": res["share"],
+        "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]),
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(solves / res["e2e_elapsed"], 6), "unit": "solves/s",
+                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+        "gpu_launches": int(res["launches"]),
+        "clocks": res["clocks"],
+        "mesh_build_s": round(res["t_mesh"], 2),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -195,10 +195,15 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
 template <int DIM, int MAXF>
 void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const int B = 128;
-    k_assemble<DIM, MAXF><<<(unsigned)((a.n + B - 1) / B), B, 0, st>>>(a);
+    fv_note_launch(), k_assemble<DIM, MAXF><<<(unsigned)((a.n + B - 1) / B), B, 0, st>>>(a);
 }
 
 }  // namespace
+
+#include <atomic>
+static std::atomic<unsigned long long> g_launches{0};
+void fv_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t fv_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 static thread_local char g_last_error[256];
 void fv_internal_set_cuda_error(cudaError_t e, const char *what) {
@@ -333,11 +338,11 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
     FV_CUDA_TRY(cudaMemsetAsync(len + N, 0, sizeof(int32_t), st));
     const int mf = m->maxf;
     if (mf <= 4)
-        k_row_count<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+        fv_note_launch(), k_row_count<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
     else if (mf <= 8)
-        k_row_count<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+        fv_note_launch(), k_row_count<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
     else
-        k_row_count<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
+        fv_note_launch(), k_row_count<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, len);
     FV_CUDA_TRY(cudaGetLastError());
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, len, m->row_ptr, (int)(N + 1), st);
@@ -352,11 +357,11 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
     m->nnz = nnz;
     FV_CUDA_TRY(cudaMalloc(&m->cols, sizeof(int32_t) * (nnz ? nnz : 1)));
     if (mf <= 4)
-        k_row_fill<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+        fv_note_launch(), k_row_fill<4><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
     else if (mf <= 8)
-        k_row_fill<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+        fv_note_launch(), k_row_fill<8><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
     else
-        k_row_fill<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
+        fv_note_launch(), k_row_fill<16><<<G, B, 0, st>>>(N, m->cf_ptr, m->cf_other, m->row_ptr, m->cols);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }

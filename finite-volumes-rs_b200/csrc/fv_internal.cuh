@@ -26,6 +26,8 @@
     } while (0)
 
 void fv_internal_set_cuda_error(cudaError_t e, const char *what);
+// Counts kernel launches made by this library (fv_launch_count).
+void fv_note_launch();
 
 static inline cudaStream_t fv_stream(void *s) { return (cudaStream_t)s; }
 

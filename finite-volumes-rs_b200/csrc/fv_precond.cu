@@ -387,14 +387,14 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const int64_t n = P->n;
     const int G = sweep_grid(n);
     if (P->kind == 2) {
-        k_sweep<double, true><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r, P->tmp,
+        fv_note_launch(), k_sweep<double, true><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r, P->tmp,
                                                  nullptr, z, P->ctrl, P->err, skip);
     } else {
-        k_sweep<double, false><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
+        fv_note_launch(), k_sweep<double, false><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
                                                   P->tmp, nullptr, z, P->ctrl, P->err, skip);
     }
     FV_CUDA_TRY(cudaGetLastError());
-    k_sweep<double, false><<<G, 256, 0, st>>>(n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp, z,
+    fv_note_launch(), k_sweep<double, false><<<G, 256, 0, st>>>(n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp, z,
                                               P->tmp, nullptr, P->ctrl + 2, P->err, skip);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
@@ -473,7 +473,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
     const int64_t n = P->n;
     if (kind == 1) {
         FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
-        k_check_symmetric<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, A->row_ptr, A->vals, sym->l_ptr, sym->l_col,
+        fv_note_launch(), k_check_symmetric<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, A->row_ptr, A->vals, sym->l_ptr, sym->l_col,
                                                                       sym->u_ptr, sym->l_tpos, P->err);
         FV_CUDA_TRY(cudaGetLastError());
         int bad = 0;
@@ -494,7 +494,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
     const int mr = sym->max_row;
     if (kind == 2) {
 #define FV_ILU(MR)                                                                                          \
-    k_ilu0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->u_ptr, \
+    fv_note_launch(), k_ilu0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->u_ptr, \
                                   sym->u_col, P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch,        \
                                   P->ctrl + 4, P->err)
         if (mr <= 8)
@@ -506,7 +506,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
 #undef FV_ILU
     } else {
 #define FV_IC(MR)                                                                                             \
-    k_ic0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->l_tpos, \
+    fv_note_launch(), k_ic0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->l_tpos, \
                                  P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch, P->ctrl + 4, P->err)
         if (mr <= 8)
             FV_IC(8);
@@ -526,7 +526,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
         unsigned long long *cnt = nullptr;
         FV_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(unsigned long long), st));
         FV_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
-        k_count_dropped<<<592, 256, 0, st>>>(sym->nnz_l, P->l_val, sym->nnz_u, P->u_val, cnt);
+        fv_note_launch(), k_count_dropped<<<592, 256, 0, st>>>(sym->nnz_l, P->l_val, sym->nnz_u, P->u_val, cnt);
         unsigned long long h = 0;
         FV_CUDA_TRY(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
         FV_CUDA_TRY(cudaFreeAsync(cnt, st));

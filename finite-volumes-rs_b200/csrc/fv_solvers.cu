@@ -439,7 +439,7 @@ extern "C" fv_status fv_spmv(const fv_csr *A, const double *x, double *y, void *
     if (!A || !x || !y || x == y) return FV_ERR_INVALID;
     if (A->nrows == 0) return FV_OK;
     const int G = (int)std::min<int64_t>((A->nrows + 255) / 256, 148 * 16);
-    k_spmv<<<G, 256, 0, fv_stream(stream)>>>(A->nrows, A->row_ptr, A->cols, A->vals, x, y);
+    fv_note_launch(), k_spmv<<<G, 256, 0, fv_stream(stream)>>>(A->nrows, A->row_ptr, A->cols, A->vals, x, y);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -517,7 +517,7 @@ fv_status fill_info(bool bicg, const SolverState &h, fv_solver_info *info, fv_pr
 fv_status apply_or_copy(fv_precond *P, const double *r, double *z, int64_t n, int G, const SolverState *S,
                         cudaStream_t st) {
     if (P) return fv_precond_apply_dev(P, r, z, st, &S->done);
-    k_copy_if_active<<<G, RB, 0, st>>>(n, r, z, S);  // IdentityPreconditioner
+    fv_note_launch(), k_copy_if_active<<<G, RB, 0, st>>>(n, r, z, S);  // IdentityPreconditioner
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -540,21 +540,21 @@ extern "C" fv_status fv_cg(const fv_csr *A, fv_precond *P, const double *b, doub
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
-    k_dot_self<<<G, RB, 0, st>>>(n, b, S);
-    k_zero_if<<<G, RB, 0, st>>>(n, x, S);
-    k_residual<false><<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, x, b, r, nullptr, nullptr, S);
+    fv_note_launch(), k_dot_self<<<G, RB, 0, st>>>(n, b, S);
+    fv_note_launch(), k_zero_if<<<G, RB, 0, st>>>(n, x, S);
+    fv_note_launch(), k_residual<false><<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, x, b, r, nullptr, nullptr, S);
     fv_status s = apply_or_copy(P, r, z, n, G, S, st);
-    k_cg_init_p<<<G, RB, 0, st>>>(n, r, z, p, S);
+    fv_note_launch(), k_cg_init_p<<<G, RB, 0, st>>>(n, r, z, p, S);
     FV_CUDA_TRY(cudaGetLastError());
     SolverState h{};
     const int B = batch_size(n);
     for (int64_t it = 0; s == FV_OK;) {
         for (int q = 0; q < B && s == FV_OK; ++q, ++it) {
-            k_cg_spmv<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, p, ap, S);
-            k_cg_update<<<G, RB, 0, st>>>(n, x, r, p, ap, S);
+            fv_note_launch(), k_cg_spmv<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, p, ap, S);
+            fv_note_launch(), k_cg_update<<<G, RB, 0, st>>>(n, x, r, p, ap, S);
             s = apply_or_copy(P, r, z, n, G, S, st);
-            k_cg_rz<<<G, RB, 0, st>>>(n, r, z, S);
-            k_cg_p<<<G, RB, 0, st>>>(n, z, p, S);
+            fv_note_launch(), k_cg_rz<<<G, RB, 0, st>>>(n, r, z, S);
+            fv_note_launch(), k_cg_p<<<G, RB, 0, st>>>(n, z, p, S);
         }
         FV_CUDA_TRY(cudaGetLastError());
         if (s != FV_OK) break;
@@ -587,9 +587,9 @@ extern "C" fv_status fv_bicgstab(const fv_csr *A, fv_precond *P, const double *b
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
-    k_dot_self<<<G, RB, 0, st>>>(n, b, S);
-    k_zero_if<<<G, RB, 0, st>>>(n, x, S);
-    k_residual<true><<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, x, b, r, rh, p, S);
+    fv_note_launch(), k_dot_self<<<G, RB, 0, st>>>(n, b, S);
+    fv_note_launch(), k_zero_if<<<G, RB, 0, st>>>(n, x, S);
+    fv_note_launch(), k_residual<true><<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, x, b, r, rh, p, S);
     FV_CUDA_TRY(cudaGetLastError());
     fv_status s = FV_OK;
     SolverState h{};
@@ -597,19 +597,19 @@ extern "C" fv_status fv_bicgstab(const fv_csr *A, fv_precond *P, const double *b
     for (int64_t it = 0; s == FV_OK;) {
         for (int q = 0; q < B && s == FV_OK; ++q, ++it) {
             s = apply_or_copy(P, p, y, n, G, S, st);
-            k_bi_spmv1<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, y, v, rh, S);
-            k_bi_s<<<G, RB, 0, st>>>(n, r, v, s_, S);
+            fv_note_launch(), k_bi_spmv1<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, y, v, rh, S);
+            fv_note_launch(), k_bi_s<<<G, RB, 0, st>>>(n, r, v, s_, S);
             if (s == FV_OK) s = apply_or_copy(P, s_, z, n, G, S, st);
-            k_bi_spmv2<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, z, t, s_, S);
-            k_bi_update<<<G, RB, 0, st>>>(n, x, r, y, z, s_, t, rh, S);
-            k_bi_p<<<G, RB, 0, st>>>(n, r, v, p, rh, S);
+            fv_note_launch(), k_bi_spmv2<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, z, t, s_, S);
+            fv_note_launch(), k_bi_update<<<G, RB, 0, st>>>(n, x, r, y, z, s_, t, rh, S);
+            fv_note_launch(), k_bi_p<<<G, RB, 0, st>>>(n, r, v, p, rh, S);
         }
         FV_CUDA_TRY(cudaGetLastError());
         if (s != FV_OK) break;
         FV_TRY(read_state(w, h, st));
         if (h.done) break;
     }
-    k_bi_finish<<<G, RB, 0, st>>>(n, x, y, S);
+    fv_note_launch(), k_bi_finish<<<G, RB, 0, st>>>(n, x, y, S);
     cudaEventRecord(e1, st);
     if (s == FV_OK) s = read_state(w, h, st);
     float ms = 0.f;

@@ -132,6 +132,8 @@ def lib() -> C.CDLL:
         L.fv_status_string.restype = C.c_char_p
         L.fv_last_error.argtypes = []
         L.fv_last_error.restype = C.c_char_p
+        L.fv_launch_count.argtypes = []
+        L.fv_launch_count.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -142,4 +144,4 @@ def check(status: int, what: str) -> None:
 
 
 def exported_symbols() -> list[str]:
-    return list(_SIGS) + ["fv_host_mesh_free", "fv_status_string"]
+    return list(_SIGS) + ["fv_host_mesh_free", "fv_status_string", "fv_last_error", "fv_launch_count"]

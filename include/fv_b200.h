@@ -196,6 +196,10 @@ fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double *y_host, vo
 /* IncompleteCholesky::from_matrix(A, 0) / IncompleteLowerUpper::from_matrix(A, 0). */
 fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out);
 fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out);
+/* Value-only refactorisation of P after the values of the matrix it was built
+ * from changed (same pattern, same fv_csr object); reuses the symbolic
+ * analysis (triangular split, level schedules) and the factor storage. */
+fv_status fv_precond_refactor(fv_precond *P, void *stream);
 /* z = M^-1 r (Preconditioner::precondition).  r and z must not alias. */
 fv_status fv_precond_apply(fv_precond *P, const double *r, double *z, void *stream);
 fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, double *z_host, void *stream);
@@ -223,6 +227,10 @@ fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const double *b_host,
 
 /* Human-readable name of a status. */
 const char *fv_status_string(fv_status s);
+/* Text of the last CUDA error recorded by this thread (after FV_ERR_CUDA). */
+const char *fv_last_error(void);
+/* Number of kernels this library has launched in this process (diagnostics). */
+uint64_t fv_launch_count(void);
 
 #ifdef __cplusplus
 }
