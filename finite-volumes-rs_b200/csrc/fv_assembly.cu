@@ -210,6 +210,8 @@ void fv_internal_set_cuda_error(cudaError_t e, const char *what) {
     snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(e));
 }
 
+void fv_internal_set_error_text(const char *what) { snprintf(g_last_error, sizeof(g_last_error), "%s", what); }
+
 extern "C" const char *fv_last_error(void) { return g_last_error; }
 
 extern "C" const char *fv_status_string(fv_status s) {

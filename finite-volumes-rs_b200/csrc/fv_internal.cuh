@@ -26,6 +26,7 @@
     } while (0)
 
 void fv_internal_set_cuda_error(cudaError_t e, const char *what);
+void fv_internal_set_error_text(const char *what);
 // Counts kernel launches made by this library (fv_launch_count).
 void fv_note_launch();
 

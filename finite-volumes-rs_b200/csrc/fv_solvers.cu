@@ -646,3 +646,106 @@ extern "C" fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const doub
                                       fv_solver_options opt, fv_solver_info *info, void *stream) {
     return solve_host(true, A, P, b_host, x_host, opt, info, stream);
 }
+
+// ------------------------------------------------------------------ fv_cg_noalloc
+// Allocation-free conjugate gradient.  fv_cg takes its Krylov workspace from
+// cudaMallocAsync on every call; this variant takes it from one statically
+// sized device array that the CUDA module reserves when the library is loaded
+// on a GPU.  It launches the same kernels in the same order as fv_cg, so its
+// results are the same bits.
+namespace {
+constexpr int64_t kNoAllocMaxRows = FV_NOALLOC_MAX_ROWS;
+constexpr int64_t kNoAllocMaxHist = FV_NOALLOC_MAX_ITERATIONS + 3;
+constexpr size_t kNoAllocState = (sizeof(SolverState) + 255) / 256 * 256;
+constexpr size_t kNoAllocPartial = 1184 * 4 * sizeof(double);  // fv_reduce_grid never exceeds 1184 blocks
+constexpr size_t kNoAllocBytes =
+    kNoAllocState + kNoAllocPartial + kNoAllocMaxHist * sizeof(double) + 4 * kNoAllocMaxRows * sizeof(double);
+}  // namespace
+
+// The workspace: solver state, block partials, residual history, r/z/p/Ap.
+// In host code this name is only a handle for cudaGetSymbolAddress, never a
+// device address.
+static __device__ __align__(256) unsigned char g_cg_noalloc_scratch[kNoAllocBytes];
+
+#include <mutex>
+static std::mutex g_cg_noalloc_mu;
+static void *g_cg_noalloc_addr[256];
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current) and cached.
+static fv_status cg_noalloc_scratch(void **out) {
+    int dev = -1;
+    FV_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return FV_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_cg_noalloc_mu);
+    if (!g_cg_noalloc_addr[dev]) {
+        void *p = nullptr;
+        FV_CUDA_TRY(cudaGetSymbolAddress(&p, g_cg_noalloc_scratch));
+        g_cg_noalloc_addr[dev] = p;
+    }
+    *out = g_cg_noalloc_addr[dev];
+    return FV_OK;
+}
+
+extern "C" fv_status fv_cg_noalloc(const fv_csr *A, fv_precond *P, const double *b, double *x,
+                                   fv_solver_options opt, fv_solver_info *info, void *stream) {
+    if (!A || !b || !x || A->nrows != A->ncols || opt.max_iterations < 0) return FV_ERR_INVALID;
+    const int64_t n = A->nrows;
+    if (n > kNoAllocMaxRows) {
+        fv_internal_set_error_text("fv_cg_noalloc: the matrix has more than FV_NOALLOC_MAX_ROWS rows");
+        return FV_ERR_INVALID;
+    }
+    if (opt.max_iterations > FV_NOALLOC_MAX_ITERATIONS) {
+        fv_internal_set_error_text("fv_cg_noalloc: max_iterations exceeds FV_NOALLOC_MAX_ITERATIONS");
+        return FV_ERR_INVALID;
+    }
+    cudaStream_t st = fv_stream(stream);
+    const int G = fv_reduce_grid(n, RB);
+    void *base = nullptr;
+    FV_TRY(cg_noalloc_scratch(&base));
+    unsigned char *mem = (unsigned char *)base;
+    Workspace w;
+    w.S = (SolverState *)mem;
+    double *partial = (double *)(mem + kNoAllocState);
+    double *hist = partial + 1184 * 4;
+    w.vec = hist + kNoAllocMaxHist;
+    w.nvec = 4;
+    // The array keeps whatever the previous call left: the state (including
+    // the reduction ticket and the done flag) is rewritten in full here, and
+    // r, z, p, Ap, the partials and the history are written before they are read.
+    SolverState hs{};
+    hs.tol = opt.absolute_tolerance;
+    hs.rtol = opt.relative_tolerance;
+    hs.max_it = opt.max_iterations;
+    hs.error = 1.0;
+    hs.partial = partial;
+    hs.hist = hist;
+    FV_CUDA_TRY(cudaMemcpyAsync(w.S, &hs, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+    double *r = w.vec, *z = w.vec + n, *p = w.vec + 2 * n, *ap = w.vec + 3 * n;
+    SolverState *S = w.S;
+    fv_note_launch(), k_dot_self<<<G, RB, 0, st>>>(n, b, S);
+    fv_note_launch(), k_zero_if<<<G, RB, 0, st>>>(n, x, S);
+    fv_note_launch(), k_residual<false><<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, x, b, r, nullptr, nullptr, S);
+    fv_status s = apply_or_copy(P, r, z, n, G, S, st);
+    fv_note_launch(), k_cg_init_p<<<G, RB, 0, st>>>(n, r, z, p, S);
+    FV_CUDA_TRY(cudaGetLastError());
+    SolverState h{};
+    const int B = batch_size(n);
+    for (int64_t it = 0; s == FV_OK;) {
+        for (int q = 0; q < B && s == FV_OK; ++q, ++it) {
+            fv_note_launch(), k_cg_spmv<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, p, ap, S);
+            fv_note_launch(), k_cg_update<<<G, RB, 0, st>>>(n, x, r, p, ap, S);
+            s = apply_or_copy(P, r, z, n, G, S, st);
+            fv_note_launch(), k_cg_rz<<<G, RB, 0, st>>>(n, r, z, S);
+            fv_note_launch(), k_cg_p<<<G, RB, 0, st>>>(n, z, p, S);
+        }
+        FV_CUDA_TRY(cudaGetLastError());
+        if (s != FV_OK) break;
+        FV_TRY(read_state(w, h, st));
+        if (h.done) break;
+    }
+    if (s == FV_OK) s = read_state(w, h, st);
+    if (info) info->device_ms = 0.0;
+    if (s == FV_OK) s = fill_info(false, h, info, P, st);
+    return s;
+}

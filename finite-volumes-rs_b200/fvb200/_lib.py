@@ -110,6 +110,7 @@ _SIGS = {
     "fv_bicgstab": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
     "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
     "fv_bicgstab_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
+    "fv_cg_noalloc": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
 }
 
 _lib = None

@@ -225,6 +225,33 @@ fv_status fv_cg_host(const fv_csr *A, fv_precond *P, const double *b_host, doubl
 fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const double *b_host, double *x_host,
                            fv_solver_options opt, fv_solver_info *info, void *stream);
 
+/* Allocation-free conjugate gradient.  No counterpart in the reference crate.
+ *
+ * Same contract and same results as fv_cg, for callers that must not allocate
+ * device memory inside the solve: fv_cg obtains its Krylov workspace with
+ * cudaMallocAsync on every call, which an application cannot allow when
+ * another runtime owns the device memory budget (all memory reserved up front,
+ * a fixed-size pool, a memory-capped process) or when the solve runs in a
+ * phase where allocation is forbidden.  This entry point takes the workspace
+ * from a statically sized device array instead and calls no cudaMalloc,
+ * cudaMallocAsync, cudaFree or allocating library routine.
+ *
+ * Limits: at most FV_NOALLOC_MAX_ROWS rows and FV_NOALLOC_MAX_ITERATIONS
+ * iterations; larger requests return FV_ERR_INVALID (fv_last_error() names
+ * the limit).  The array (about 8.6 MB) is reserved on every GPU that loads
+ * the library and held until the process exits.
+ * The first call on each device looks up the array's device address with
+ * cudaGetSymbolAddress (that device must be current); make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  info->device_ms is left at 0.  A and P are
+ * created beforehand by the allocating calls (fv_assemble / fv_csr_create_host,
+ * fv_ic0_factor). */
+#define FV_NOALLOC_MAX_ROWS 262144
+#define FV_NOALLOC_MAX_ITERATIONS 4093
+fv_status fv_cg_noalloc(const fv_csr *A, fv_precond *P, const double *b, double *x,
+                        fv_solver_options opt, fv_solver_info *info, void *stream);
+
 /* Human-readable name of a status. */
 const char *fv_status_string(fv_status s);
 /* Text of the last CUDA error recorded by this thread (after FV_ERR_CUDA). */
