@@ -36,6 +36,7 @@ struct fv_symbolic {
     int32_t *l_tpos = nullptr;                   // L entry (i,j) -> slot of (j,i) in U (IC only)
     int32_t n_fwd_levels = 0, n_bwd_levels = 0;
     int32_t max_row = 0;                         // longest row of the pattern
+    int32_t max_lower = 0, max_upper = 0;        // longest strict-lower / strict-upper row
     bool symmetric_pattern = false;
     std::vector<int32_t> h_fwd_level, h_bwd_level;
 };
@@ -64,6 +65,8 @@ struct fv_precond {
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
+    // FP32 copies of the factors for mixed-precision inner solves
+    float *l32 = nullptr, *u32 = nullptr, *dinv32 = nullptr, *tmp32 = nullptr;
 };
 
 // ------------------------------------------------------------------ symbolic
@@ -102,6 +105,10 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     }
     lp[n] = (int32_t)nl;
     up[n] = (int32_t)nu;
+    for (int64_t i = 0; i < n; ++i) {
+        s->max_lower = std::max(s->max_lower, lp[i + 1] - lp[i]);
+        s->max_upper = std::max(s->max_upper, up[i + 1] - up[i]);
+    }
     s->nnz_l = nl;
     s->nnz_u = nu;
     s->max_row = maxrow;
@@ -345,7 +352,29 @@ __global__ void k_count_dropped(int64_t nl, const double *__restrict__ l_val, in
 //   x_i = [dinv_i *] (rhs_i - sum_{j in row} val * x_j), ascending j.
 // After reading rhs_i the lane may reset it to the sentinel (rhs_reset), and
 // it may pre-fill a later sweep's output slot (next_reset) with the sentinel.
-template <typename T, bool UNIT>
+//
+// Everything a row needs apart from its dependencies' values (its position in
+// the level order, row bounds, columns, coefficients, rhs, 1/diagonal) is
+// loaded before the first wait, and all dependencies are polled together, so
+// the critical path from one level to the next is one store plus one L2 read.
+// MAXL bounds the off-diagonal count of a row on the swept side; rows are
+// held in registers.
+template <typename T>
+__device__ __forceinline__ bool fv_slot_ready(const T *p, T &v);
+template <>
+__device__ __forceinline__ bool fv_slot_ready<double>(const double *p, double &v) {
+    unsigned long long b = fv_ld_relaxed_u64(p);
+    v = __longlong_as_double((long long)b);
+    return b != FV_SENTINEL_U64;
+}
+template <>
+__device__ __forceinline__ bool fv_slot_ready<float>(const float *p, float &v) {
+    unsigned b = fv_ld_relaxed_u32(p);
+    v = __uint_as_float(b);
+    return b != FV_SENTINEL_U32;
+}
+
+template <typename T, bool UNIT, int MAXL>
 __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restrict__ order,
                                                const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                const T *__restrict__ val, const T *__restrict__ dinv,
@@ -357,9 +386,69 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
     while (take_chunk(&ctrl[0], nchunks, chunk)) {
         const int64_t idx = chunk * 32 + (threadIdx.x & 31);
         if (idx >= n) continue;
+        const int i = __ldg(&order[idx]);
+        const int k0 = __ldg(&ptr[i]);
+        const int m = __ldg(&ptr[i + 1]) - k0;
+        int c[MAXL];
+        T v[MAXL], xv[MAXL];
+#pragma unroll
+        for (int q = 0; q < MAXL; ++q)
+            if (q < m) {
+                c[q] = __ldg(&col[k0 + q]);
+                v[q] = __ldg(&val[k0 + q]);
+            }
+        T s = rhs[i];
+        const T d = UNIT ? T(1) : __ldg(&dinv[i]);
+        if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
+        if (next_reset) fv_reset_slot(&next_reset[i]);
+        unsigned pending = 0;
+#pragma unroll
+        for (int q = 0; q < MAXL; ++q)
+            if (q < m && !fv_slot_ready(&x[c[q]], xv[q])) pending |= 1u << q;
+        if (pending) {
+            const unsigned long long t0 = fv_globaltimer();
+            for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                for (int q = 0; q < MAXL; ++q)
+                    if ((pending >> q) & 1u)
+                        if (fv_slot_ready(&x[c[q]], xv[q])) pending &= ~(1u << q);
+                if (pending && (it & 255u) == 0) {
+                    if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
+                        if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+#pragma unroll
+                        for (int q = 0; q < MAXL; ++q)
+                            if ((pending >> q) & 1u) xv[q] = T(NAN);
+                        pending = 0;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < MAXL; ++q)
+            if (q < m) s = s - v[q] * xv[q];
+        const T r = UNIT ? s : d * s;
+        fv_publish(&x[i], r);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+// Rows longer than 32 entries on the swept side: one dependency at a time.
+template <typename T, bool UNIT>
+__global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__restrict__ order,
+                                                    const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                                                    const T *__restrict__ val, const T *__restrict__ dinv,
+                                                    const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
+                                                    int *err, const int *skip) {
+    if (skip && *(volatile const int *)skip) return;
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
         const int i = order[idx];
         T s = rhs[i];
         if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
+        if (next_reset) fv_reset_slot(&next_reset[i]);
         const int k1 = ptr[i + 1];
         for (int k = ptr[i]; k < k1; ++k) {
             const T xj = fv_wait_value(&x[col[k]], err);
@@ -367,11 +456,30 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
         }
         const T r = UNIT ? s : dinv[i] * s;
         fv_publish(&x[i], r);
-        if (next_reset) fv_reset_slot(&next_reset[i]);
     }
     leave(&ctrl[0], &ctrl[1]);
 }
 
+template <typename T, bool UNIT>
+static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
+                         const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
+                         T *next_reset, unsigned *ctrl, int *err, const int *skip) {
+    if (maxl <= 4)
+        fv_note_launch(), k_sweep<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                next_reset, ctrl, err, skip);
+    else if (maxl <= 8)
+        fv_note_launch(), k_sweep<T, UNIT, 8><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                next_reset, ctrl, err, skip);
+    else if (maxl <= 16)
+        fv_note_launch(), k_sweep<T, UNIT, 16><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                 next_reset, ctrl, err, skip);
+    else if (maxl <= 32)
+        fv_note_launch(), k_sweep<T, UNIT, 32><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                 next_reset, ctrl, err, skip);
+    else
+        fv_note_launch(), k_sweep_long<T, UNIT><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                  next_reset, ctrl, err, skip);
+}
 
 static int sweep_grid(int64_t n) {
     int64_t warps = (n + 31) / 32;
@@ -386,16 +494,15 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
     const int G = sweep_grid(n);
-    if (P->kind == 2) {
-        fv_note_launch(), k_sweep<double, true><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r, P->tmp,
-                                                 nullptr, z, P->ctrl, P->err, skip);
-    } else {
-        fv_note_launch(), k_sweep<double, false><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
-                                                  P->tmp, nullptr, z, P->ctrl, P->err, skip);
-    }
+    if (P->kind == 2)
+        launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
+                                   P->tmp, nullptr, z, P->ctrl, P->err, skip);
+    else
+        launch_sweep<double, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
+                                    P->tmp, nullptr, z, P->ctrl, P->err, skip);
     FV_CUDA_TRY(cudaGetLastError());
-    fv_note_launch(), k_sweep<double, false><<<G, 256, 0, st>>>(n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp, z,
-                                              P->tmp, nullptr, P->ctrl + 2, P->err, skip);
+    launch_sweep<double, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp,
+                                z, P->tmp, nullptr, P->ctrl + 2, P->err, skip);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -415,6 +522,51 @@ fv_status fv_precond_check_error(fv_precond *P, cudaStream_t st) {
 
 int *fv_precond_err_ptr(fv_precond *P) { return P->err; }
 
+namespace {
+__global__ void k_to_f32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+}  // namespace
+
+// FP32 copies of the current factors (rounded from the FP64 factorisation).
+fv_status fv_precond_make_f32(fv_precond *P, cudaStream_t st) {
+    const fv_symbolic *s = P->sym;
+    const int64_t n = P->n;
+    if (!P->l32) {
+        FV_CUDA_TRY(cudaMalloc(&P->l32, sizeof(float) * (s->nnz_l ? s->nnz_l : 1)));
+        FV_CUDA_TRY(cudaMalloc(&P->u32, sizeof(float) * (s->nnz_u ? s->nnz_u : 1)));
+        FV_CUDA_TRY(cudaMalloc(&P->dinv32, sizeof(float) * n));
+        FV_CUDA_TRY(cudaMalloc(&P->tmp32, sizeof(float) * n));
+        FV_CUDA_TRY(cudaMemsetAsync(P->tmp32, 0xFF, sizeof(float) * n, st));
+    }
+    const int G = 148 * 8;
+    if (s->nnz_l) fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(s->nnz_l, P->l_val, P->l32);
+    if (s->nnz_u) fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(s->nnz_u, P->u_val, P->u32);
+    fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(n, P->dinv, P->dinv32);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+// z = M^-1 r in FP32 with the FP32 factor copies (fv_precond_make_f32 first).
+fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cudaStream_t st, const int *skip) {
+    const fv_symbolic *s = P->sym;
+    const int64_t n = P->n;
+    if (!P->l32) return FV_ERR_INVALID;
+    const int G = sweep_grid(n);
+    if (P->kind == 2)
+        launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
+                                  P->tmp32, nullptr, z, P->ctrl, P->err, skip);
+    else
+        launch_sweep<float, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, P->dinv32, r,
+                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip);
+    FV_CUDA_TRY(cudaGetLastError());
+    launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
+                               P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
 extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     if (!P) return FV_OK;
     cudaFree(P->l_val);
@@ -425,6 +577,10 @@ extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     cudaFree(P->done);
     cudaFree(P->ctrl);
     cudaFree(P->err);
+    cudaFree(P->l32);
+    cudaFree(P->u32);
+    cudaFree(P->dinv32);
+    cudaFree(P->tmp32);
     delete P;
     return FV_OK;
 }
