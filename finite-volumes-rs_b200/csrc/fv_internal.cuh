@@ -55,6 +55,14 @@ struct fv_mesh {
 
 struct fv_symbolic;  // triangular split + level schedules of a pattern (fv_precond.cu)
 
+// Rows a sweep may skip: row i is skipped when done[group[i] * stride] != 0
+// (rows of the problems of a batch that have converged).
+struct fv_row_skip {
+    const int32_t *group;
+    const int *done;
+    int stride;
+};
+
 struct fv_csr {
     int64_t nrows = 0, ncols = 0, nnz = 0;
     int32_t *row_ptr = nullptr;   // device

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
                                                const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                const T *__restrict__ val, const T *__restrict__ dinv,
                                                const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
-                                               int *err, const int *skip) {
+                                               int *err, const int *skip, fv_row_skip rs) {
     if (skip && *(volatile const int *)skip) return;  // a converged solve: no warp takes a ticket
     const int64_t nchunks = (n + 31) / 32;
     int64_t chunk;
@@ -387,6 +387,8 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
         const int64_t idx = chunk * 32 + (threadIdx.x & 31);
         if (idx >= n) continue;
         const int i = __ldg(&order[idx]);
+        // a converged problem's rows (and all their dependencies) are skipped together
+        if (rs.group && rs.done[(int64_t)__ldg(&rs.group[i]) * rs.stride]) continue;
         const int k0 = __ldg(&ptr[i]);
         const int m = __ldg(&ptr[i + 1]) - k0;
         int c[MAXL];
@@ -399,8 +401,6 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
             }
         T s = rhs[i];
         const T d = UNIT ? T(1) : __ldg(&dinv[i]);
-        if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
-        if (next_reset) fv_reset_slot(&next_reset[i]);
         unsigned pending = 0;
 #pragma unroll
         for (int q = 0; q < MAXL; ++q)
@@ -428,6 +428,10 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
             if (q < m) s = s - v[q] * xv[q];
         const T r = UNIT ? s : d * s;
         fv_publish(&x[i], r);
+        // sentinel resets come after the publish: a store to the slot just
+        // read would otherwise sit on the row's critical path
+        if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
+        if (next_reset) fv_reset_slot(&next_reset[i]);
     }
     leave(&ctrl[0], &ctrl[1]);
 }
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
                                                     const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                     const T *__restrict__ val, const T *__restrict__ dinv,
                                                     const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
-                                                    int *err, const int *skip) {
+                                                    int *err, const int *skip, fv_row_skip rs) {
     if (skip && *(volatile const int *)skip) return;
     const int64_t nchunks = (n + 31) / 32;
     int64_t chunk;
@@ -446,6 +450,7 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
         const int64_t idx = chunk * 32 + (threadIdx.x & 31);
         if (idx >= n) continue;
         const int i = order[idx];
+        if (rs.group && rs.done[(int64_t)rs.group[i] * rs.stride]) continue;
         T s = rhs[i];
         if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
         if (next_reset) fv_reset_slot(&next_reset[i]);
@@ -463,22 +468,22 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
 template <typename T, bool UNIT>
 static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
                          const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
-                         T *next_reset, unsigned *ctrl, int *err, const int *skip) {
+                         T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs = {}) {
     if (maxl <= 4)
         fv_note_launch(), k_sweep<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                next_reset, ctrl, err, skip);
+                                                                next_reset, ctrl, err, skip, rs);
     else if (maxl <= 8)
         fv_note_launch(), k_sweep<T, UNIT, 8><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                next_reset, ctrl, err, skip);
+                                                                next_reset, ctrl, err, skip, rs);
     else if (maxl <= 16)
         fv_note_launch(), k_sweep<T, UNIT, 16><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                 next_reset, ctrl, err, skip);
+                                                                 next_reset, ctrl, err, skip, rs);
     else if (maxl <= 32)
         fv_note_launch(), k_sweep<T, UNIT, 32><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                 next_reset, ctrl, err, skip);
+                                                                 next_reset, ctrl, err, skip, rs);
     else
         fv_note_launch(), k_sweep_long<T, UNIT><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                  next_reset, ctrl, err, skip);
+                                                                  next_reset, ctrl, err, skip, rs);
 }
 
 static int sweep_grid(int64_t n) {
@@ -490,19 +495,21 @@ static int sweep_grid(int64_t n) {
 // z = M^-1 r.  r must not alias z.  The forward sweep writes P->tmp and
 // pre-fills z with the sentinel; the backward sweep consumes tmp (resetting it
 // to the sentinel for the next apply) and writes z.
-fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaStream_t st, const int *skip) {
+fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaStream_t st, const int *skip,
+                               const fv_row_skip *rskip) {
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
     const int G = sweep_grid(n);
+    const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (P->kind == 2)
         launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
-                                   P->tmp, nullptr, z, P->ctrl, P->err, skip);
+                                   P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
     else
         launch_sweep<double, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
-                                    P->tmp, nullptr, z, P->ctrl, P->err, skip);
+                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
     FV_CUDA_TRY(cudaGetLastError());
     launch_sweep<double, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp,
-                                z, P->tmp, nullptr, P->ctrl + 2, P->err, skip);
+                                z, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -549,20 +556,22 @@ fv_status fv_precond_make_f32(fv_precond *P, cudaStream_t st) {
 }
 
 // z = M^-1 r in FP32 with the FP32 factor copies (fv_precond_make_f32 first).
-fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cudaStream_t st, const int *skip) {
+fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cudaStream_t st, const int *skip,
+                                   const fv_row_skip *rskip) {
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
     if (!P->l32) return FV_ERR_INVALID;
     const int G = sweep_grid(n);
+    const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (P->kind == 2)
         launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
-                                  P->tmp32, nullptr, z, P->ctrl, P->err, skip);
+                                  P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
     else
         launch_sweep<float, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, P->dinv32, r,
-                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip);
+                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
     FV_CUDA_TRY(cudaGetLastError());
     launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
-                               P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip);
+                               P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -713,7 +722,7 @@ extern "C" fv_status fv_precond_refactor(fv_precond *P, void *stream) {
 extern "C" fv_status fv_precond_apply(fv_precond *P, const double *r, double *z, void *stream) {
     if (!P || !r || !z || r == z) return FV_ERR_INVALID;
     cudaStream_t st = fv_stream(stream);
-    FV_TRY(fv_precond_apply_dev(P, r, z, st, nullptr));
+    FV_TRY(fv_precond_apply_dev(P, r, z, st, nullptr, nullptr));
     return fv_precond_check_error(P, st);
 }
 
@@ -723,7 +732,7 @@ extern "C" fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, 
     double *buf = nullptr;
     FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * 2 * P->n, st));
     FV_CUDA_TRY(cudaMemcpyAsync(buf, r_host, sizeof(double) * P->n, cudaMemcpyHostToDevice, st));
-    fv_status s = fv_precond_apply_dev(P, buf, buf + P->n, st, nullptr);
+    fv_status s = fv_precond_apply_dev(P, buf, buf + P->n, st, nullptr, nullptr);
     if (s == FV_OK) s = fv_precond_check_error(P, st);
     if (s == FV_OK)
         FV_CUDA_TRY(cudaMemcpyAsync(z_host, buf + P->n, sizeof(double) * P->n, cudaMemcpyDeviceToHost, st));

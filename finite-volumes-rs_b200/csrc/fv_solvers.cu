@@ -23,7 +23,8 @@
 
 struct fv_symbolic;
 struct fv_precond;
-fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaStream_t st, const int *skip);
+fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaStream_t st, const int *skip,
+                               const fv_row_skip *rskip);
 fv_status fv_precond_check_error(fv_precond *P, cudaStream_t st);
 void fv_symbolic_free(fv_symbolic *s);
 
@@ -516,7 +517,7 @@ fv_status fill_info(bool bicg, const SolverState &h, fv_solver_info *info, fv_pr
 
 fv_status apply_or_copy(fv_precond *P, const double *r, double *z, int64_t n, int G, const SolverState *S,
                         cudaStream_t st) {
-    if (P) return fv_precond_apply_dev(P, r, z, st, &S->done);
+    if (P) return fv_precond_apply_dev(P, r, z, st, &S->done, nullptr);
     fv_note_launch(), k_copy_if_active<<<G, RB, 0, st>>>(n, r, z, S);  // IdentityPreconditioner
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;

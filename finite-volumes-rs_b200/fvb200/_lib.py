@@ -79,6 +79,17 @@ class SolverInfo(C.Structure):
     ]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("relative_tolerance", C.c_double), ("absolute_tolerance", C.c_double),
+                ("max_iterations", i64), ("inner_relative_tolerance", C.c_double), ("outer_tolerance", C.c_double),
+                ("max_outer", C.c_int32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("device_ms", C.c_double), ("launched_iterations", i64), ("iterations", P(i64)),
+                ("outer_steps", ip), ("final_residual", dp), ("status", ip), ("fp64_fallback", ip)]
+
+
 vp = C.c_void_p
 _SIGS = {
     # host mesh
@@ -111,6 +122,10 @@ _SIGS = {
     "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
     "fv_bicgstab_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
     "fv_cg_noalloc": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
+    "fv_batch_create": [vp, C.c_int32, P(i64), C.c_int32, vp, P(vp)],
+    "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
+    "fv_batch_bicgstab": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
+    "fv_batch_destroy": [vp],
 }
 
 _lib = None

@@ -1,0 +1,145 @@
+"""Batched solves: many independent meshes as one block-diagonal system.
+
+MeshBatch concatenates host meshes into one mesh whose faces are ordered
+interior faces of every problem first, then the boundary faces of every
+problem (each problem keeps its own relative face order, so every cell sees
+its faces in the same order as alone).  assemble() on a MeshBatch therefore
+yields exactly the per-problem matrices on the diagonal, IC(0) of the union is
+the per-problem IC(0), and BatchCG solves all problems at once with
+per-problem scalars (fv_batch_cg).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from ._lib import BatchInfo, BatchOptions, check, lib
+from .streams import stream_handle
+
+FV_BATCH_FP64, FV_BATCH_MIXED = 0, 1
+
+
+class MeshBatch:
+    def __init__(self, meshes):
+        assert meshes and len({m.dim for m in meshes}) == 1
+        self.meshes = list(meshes)
+        self.dim = meshes[0].dim
+        self.n_problems = len(meshes)
+        nc = np.array([m.n_cells for m in meshes], np.int64)
+        fi = np.array([m.n_faces - m.n_boundary_faces for m in meshes], np.int64)
+        fb = np.array([m.n_boundary_faces for m in meshes], np.int64)
+        self.cell_offsets = np.concatenate([[0], np.cumsum(nc)])
+        self.int_offsets = np.concatenate([[0], np.cumsum(fi)])
+        self.bnd_offsets = np.concatenate([[0], np.cumsum(fb)])
+        self.n_cells = int(self.cell_offsets[-1])
+        self.n_boundary_faces = int(self.bnd_offsets[-1])
+        self.n_faces = int(self.int_offsets[-1]) + self.n_boundary_faces
+        co = self.cell_offsets
+        own_i = [m.face_owner[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
+        own_b = [m.face_owner[fi[p]:].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
+        nb_i = [m.face_neighbor[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
+        self.face_owner = np.concatenate(own_i + own_b).astype(np.int32)
+        self.face_neighbor = np.concatenate(nb_i + [np.full(fb[p], -1, np.int64) for p in range(len(meshes))]).astype(
+            np.int32)
+        self.face_area = self.face_field([m.face_area for m in meshes])
+        self.face_center = self.face_field([m.face_center for m in meshes])
+        self.cell_center = np.ascontiguousarray(np.concatenate([m.cell_center for m in meshes]))
+        self.cell_volume = np.ascontiguousarray(np.concatenate([m.cell_volume for m in meshes]))
+        self._device = {}
+
+    def face_field(self, per_problem):
+        """Concatenate per-problem face arrays into the union face order."""
+        fi = [m.n_faces - m.n_boundary_faces for m in self.meshes]
+        parts = [a[: fi[p]] for p, a in enumerate(per_problem)] + [a[fi[p]:] for p, a in enumerate(per_problem)]
+        return np.ascontiguousarray(np.concatenate(parts))
+
+    def boundary_field(self, per_problem):
+        """Concatenate per-problem boundary-face arrays (bndi, bnde)."""
+        return np.ascontiguousarray(np.concatenate(per_problem))
+
+    def cell_field(self, per_problem):
+        return np.ascontiguousarray(np.concatenate(per_problem))
+
+    def device(self, stream=None):
+        import torch
+
+        from .mesh import DeviceMesh
+        dev = torch.cuda.current_device()
+        if dev not in self._device:
+            self._device[dev] = DeviceMesh(self, stream)
+        return self._device[dev]
+
+    def __del__(self):
+        try:
+            for dm in self._device.values():
+                dm.close()
+        except Exception:
+            pass
+
+
+class BatchCG:
+    """fv_batch handle over a block-diagonal matrix with row_offsets per problem
+    (solve(..., solver="cg"|"bicgstab"))."""
+
+    def __init__(self, A, row_offsets, tile_rows: int = 0, stream=None):
+        self.A = A
+        self.row_offsets = np.ascontiguousarray(row_offsets, dtype=np.int64)
+        self.n_problems = len(self.row_offsets) - 1
+        self.tile_rows = tile_rows
+        self.handle = C.c_void_p()
+        check(lib().fv_batch_create(A.handle, self.n_problems, self.row_offsets.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    tile_rows, stream_handle(stream), C.byref(self.handle)), "fv_batch_create")
+
+    def solve(self, P, b, x, precision: str = "mixed", relative_tolerance=1e-8, absolute_tolerance=1e-8,
+              max_iterations=10000, inner_relative_tolerance=1e-2, outer_tolerance=1e-10, max_outer=30,
+              stream=None, solver: str = "cg"):
+        o = BatchOptions(FV_BATCH_MIXED if precision == "mixed" else FV_BATCH_FP64, relative_tolerance,
+                         absolute_tolerance, max_iterations, inner_relative_tolerance, outer_tolerance, max_outer)
+        n = self.n_problems
+        its = np.zeros(n, np.int64)
+        outer = np.zeros(n, np.int32)
+        res = np.zeros(n)
+        stat = np.zeros(n, np.int32)
+        fb = np.zeros(n, np.int32)
+        info = BatchInfo(0.0, 0, its.ctypes.data_as(C.POINTER(C.c_int64)), outer.ctypes.data_as(C.POINTER(C.c_int32)),
+                         res.ctypes.data_as(C.POINTER(C.c_double)), stat.ctypes.data_as(C.POINTER(C.c_int32)),
+                         fb.ctypes.data_as(C.POINTER(C.c_int32)))
+        fn = lib().fv_batch_bicgstab if solver == "bicgstab" else lib().fv_batch_cg
+        check(fn(self.handle, P.handle, C.c_void_p(b.data.data_ptr()), C.c_void_p(x.data.data_ptr()), C.byref(o),
+                 C.byref(info), stream_handle(stream)), "fv_batch_" + solver)
+        return dict(iterations=its, outer_steps=outer, final_residual=res, status=stat, device_ms=info.device_ms,
+                    launched_iterations=info.launched_iterations, fp64_fallback=fb)
+
+    def close(self):
+        if self.handle:
+            lib().fv_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_tile(A, row_offsets, P, b, x, candidates=(256, 512, 1024, 2048), iters=10):
+    """Pick the tile size (rows per problem-aligned reduction tile) that runs a
+    fixed number of FP64 CG iterations fastest on this batch."""
+    import torch
+    best, best_t = None, float("inf")
+    timings = {}
+    for tile in candidates:
+        bc = BatchCG(A, row_offsets, tile)
+        bc.solve(P, b, x, precision="fp64", relative_tolerance=0.0, absolute_tolerance=0.0, max_iterations=2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bc.solve(P, b, x, precision="fp64", relative_tolerance=0.0, absolute_tolerance=0.0, max_iterations=iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        timings[tile] = dt
+        bc.close()
+        if dt < best_t:
+            best, best_t = tile, dt
+    return best, timings

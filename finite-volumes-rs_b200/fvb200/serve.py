@@ -1,0 +1,264 @@
+"""Request server: continuous batching of independent solves on one GPU.
+
+Requests (a mesh size, a seed, a tolerance) arrive as a Poisson stream.  An
+arrived request is admitted when its estimated device memory fits the free
+budget; admitted requests of one kind (2D diffusion -> CG + IC(0), 3D
+convection-diffusion -> BiCGStab + ILU(0)) are packed into a wave, a
+block-diagonal batch solved with per-problem scalars in mixed precision
+(fvb200.batch).  Several waves are in flight at once, each on its own CUDA
+stream driven by its own host thread, so work of requests that arrived while
+others were running overlaps on the device; a worker that finishes a wave
+immediately takes the next admitted requests (slots are refilled as they
+free up).  Per-problem reductions never mix problems, so a request's result
+is the same alone and in any wave.
+
+Meshes are built on the host per (kind, size) and cached; the request's seed
+drives its diffusivity and source fields.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import threading
+import time
+
+import numpy as np
+
+from .batch import BatchCG, MeshBatch
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival: float         # seconds from the start of the stream
+    kind: str              # "2d" or "3d"
+    side: int              # 2D: squares per side; 3D: hexes per side
+    seed: int
+    rtol: float = 1e-8
+    cells: int = 0
+    # filled by the server
+    start: float = -1.0
+    finish: float = -1.0
+    wave: int = -1
+    iterations: int = 0
+    residual: float = float("nan")
+    solution: np.ndarray | None = None
+
+
+def request_stream(rate: float, duration: float, seed: int, mix_3d: float = 0.5, lo: float = 1e4,
+                   hi: float = 2e6) -> list[Request]:
+    """Poisson arrivals; cells lognormal with 1st/99th percentiles lo/hi,
+    clipped to [lo, hi]; 2D side = round(sqrt(cells/2)), 3D n = round((cells/6)^(1/3))."""
+    rng = np.random.default_rng(seed)
+    mu = 0.5 * (np.log(lo) + np.log(hi))
+    sigma = (np.log(hi) - mu) / 2.3263478740408408
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        cells = float(np.clip(np.exp(rng.normal(mu, sigma)), lo, hi))
+        if rng.random() < mix_3d:
+            n = max(2, int(round((cells / 6.0) ** (1.0 / 3.0))))
+            out.append(Request(len(out), t, "3d", n, int(rng.integers(1 << 30)), cells=6 * n ** 3))
+        else:
+            s = max(2, int(round(np.sqrt(cells / 2.0))))
+            out.append(Request(len(out), t, "2d", s, int(rng.integers(1 << 30)), cells=2 * s * s))
+    return out
+
+
+class MeshCache:
+    """Host meshes per (kind, side); geometry jitter seeded by the size."""
+
+    def __init__(self, fv, capacity_cells: int = 60_000_000):
+        self.fv = fv
+        self.cap = capacity_cells
+        self.d = collections.OrderedDict()
+        self.cells = 0
+        self.lock = threading.Lock()
+
+    def get(self, kind, side):
+        key = (kind, side)
+        with self.lock:
+            if key in self.d:
+                self.d.move_to_end(key)
+                return self.d[key]
+        m = self.fv.Mesh.square(side, 0.2, 17 + side) if kind == "2d" else self.fv.Mesh.cube(side, 0.15, 17 + side)
+        with self.lock:
+            self.d[key] = m
+            self.cells += m.n_cells
+            while self.cells > self.cap and len(self.d) > 1:
+                _, old = self.d.popitem(last=False)
+                self.cells -= old.n_cells
+        return m
+
+
+def request_fields(m, req: Request):
+    if req.kind == "2d":
+        kf, _, sc = m.fields(req.seed, 1.0, 1.0, source_const=1.0)
+        return kf, None, sc
+    v = (1.0, 0.5, 0.25)
+    kappa0 = float(np.linalg.norm(v)) / req.side / 3.0
+    return m.fields(req.seed, kappa0, 0.5, velocity=v, source_uniform=True)
+
+
+BYTES_PER_CELL = {"2d": 700, "3d": 1100}   # resident estimate: mesh, CSR, factors, FP32 copies, vectors
+
+
+def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol=1e-10, keep_solution=False):
+    """Pack requests of one kind into one batch and solve it on `stream`."""
+    import torch
+    kind = reqs[0].kind
+    with torch.cuda.stream(stream):
+        meshes, kfs, fls, scs = [], [], [], []
+        for r in reqs:
+            m = cache.get(r.kind, r.side)
+            kf, fl, sc = request_fields(m, r)
+            meshes.append(m)
+            kfs.append(kf)
+            fls.append(fl)
+            scs.append(sc)
+        mb = MeshBatch(meshes)
+        kf = mb.face_field(kfs)
+        sc = mb.cell_field(scs)
+        nb = mb.n_boundary_faces
+        bc = (np.zeros(nb), np.zeros(nb))
+        if kind == "2d":
+            eq = -fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+        else:
+            fl = mb.face_field(fls)
+            eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+        A, b = fv.assemble(eq, bc, mb, stream=stream)
+        P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(A, 0, stream=stream)
+        x = fv.DistributedVector.from_size(mb.n_cells)
+        solver = BatchCG(A, mb.cell_offsets, tile_rows, stream=stream)
+        out = solver.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-4,
+                           max_outer=30, max_iterations=20000, stream=stream,
+                           solver="cg" if kind == "2d" else "bicgstab")
+        xs = x.data.cpu().numpy() if keep_solution else None
+        stream.synchronize()
+        for k, r in enumerate(reqs):
+            r.iterations = int(out["iterations"][k])
+            r.residual = float(out["final_residual"][k])
+            if keep_solution:
+                r.solution = xs[mb.cell_offsets[k]:mb.cell_offsets[k + 1]].copy()
+        # release device objects in this thread (frees are stream ordered per object)
+        solver.close()
+        P.close()
+        A.close()
+        del mb
+    return out
+
+
+class Server:
+    def __init__(self, fv, workers: int = 3, budget_bytes: int | None = None, max_wave_cells: int = 16_000_000,
+                 max_wave_requests: int = 256):
+        import torch
+        self.fv = fv
+        self.cache = MeshCache(fv)
+        self.workers = workers
+        free, total = torch.cuda.mem_get_info()
+        self.budget = budget_bytes if budget_bytes is not None else int(free * 0.7)
+        self.max_wave_cells = max_wave_cells
+        self.max_wave_requests = max_wave_requests
+        self.lock = threading.Condition()
+        self.reserved = 0
+        self.admitted = collections.deque()
+        self.done = []
+        self.waves = 0
+
+    def _cost(self, r: Request) -> int:
+        return BYTES_PER_CELL[r.kind] * r.cells
+
+    def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True) -> dict:
+        """Serve `requests` (arrival times relative to now).  Returns latency and
+        throughput statistics over the completed requests."""
+        import torch
+        if warm:  # one small wave of each kind compiles nothing but brings the driver up
+            for kind, side in (("2d", 8), ("3d", 3)):
+                solve_wave(self.fv, self.cache, [Request(-1, 0.0, kind, side, 1, cells=1)],
+                           torch.cuda.Stream())
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        t0 = time.perf_counter()
+        stop = threading.Event()
+
+        def admit_loop():
+            while not stop.is_set():
+                now = time.perf_counter() - t0
+                with self.lock:
+                    while pending and pending[0].arrival <= now:
+                        r = pending[0]
+                        c = self._cost(r)
+                        if self.reserved + c > self.budget and self.reserved > 0:
+                            break  # admission by free device memory
+                        pending.popleft()
+                        self.reserved += c
+                        self.admitted.append(r)
+                        self.lock.notify_all()
+                    if not pending and not self.admitted:
+                        pass
+                time.sleep(0.0005)
+
+        def worker():
+            stream = torch.cuda.Stream()
+            while True:
+                with self.lock:
+                    while not self.admitted and not stop.is_set():
+                        self.lock.wait(0.01)
+                    if stop.is_set() and not self.admitted:
+                        return
+                    kind = self.admitted[0].kind
+                    wave, cells = [], 0
+                    rest = collections.deque()
+                    while self.admitted and len(wave) < self.max_wave_requests:
+                        r = self.admitted.popleft()
+                        if r.kind == kind and (cells + r.cells <= self.max_wave_cells or not wave):
+                            wave.append(r)
+                            cells += r.cells
+                        else:
+                            rest.append(r)
+                    rest.extend(self.admitted)
+                    self.admitted = rest
+                    wid = self.waves
+                    self.waves += 1
+                start = time.perf_counter() - t0
+                for r in wave:
+                    r.start = start
+                    r.wave = wid
+                solve_wave(self.fv, self.cache, wave, stream)
+                fin = time.perf_counter() - t0
+                with self.lock:
+                    for r in wave:
+                        r.finish = fin
+                        self.reserved -= self._cost(r)
+                    self.done.extend(wave)
+                    self.lock.notify_all()
+
+        adm = threading.Thread(target=admit_loop, daemon=True)
+        ws = [threading.Thread(target=worker, daemon=True) for _ in range(self.workers)]
+        adm.start()
+        for w in ws:
+            w.start()
+        deadline = t0 + time_limit
+        while time.perf_counter() < deadline:
+            with self.lock:
+                if len(self.done) == len(requests):
+                    break
+            time.sleep(0.01)
+        stop.set()
+        with self.lock:
+            self.lock.notify_all()
+        for w in ws:
+            w.join(timeout=max(1.0, deadline - time.perf_counter() + 600))
+        wall = time.perf_counter() - t0
+        fin = [r for r in self.done if r.finish >= 0]
+        lat = np.array([r.finish - r.arrival for r in fin]) if fin else np.zeros(0)
+        span = (max(r.finish for r in fin) - min(r.arrival for r in fin)) if fin else 0.0
+        return {
+            "completed": len(fin), "offered": len(requests), "waves": self.waves, "wall_s": wall,
+            "solves_per_s": len(fin) / span if span > 0 else 0.0,
+            "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
+            "max_residual": float(max((r.residual for r in fin), default=float("nan"))),
+            "cells_per_s": float(sum(r.cells for r in fin) / span) if span > 0 else 0.0,
+        }

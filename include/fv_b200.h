@@ -225,6 +225,54 @@ fv_status fv_cg_host(const fv_csr *A, fv_precond *P, const double *b_host, doubl
 fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const double *b_host, double *x_host,
                            fv_solver_options opt, fv_solver_info *info, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched solves (no single counterpart in the reference: every problem is
+ * solved as conjugate_gradient.rs:12-111 would solve it alone).  A is the
+ * block-diagonal union of independent problems (e.g. assembled on a mesh made
+ * by concatenating meshes); row_offsets[p]..row_offsets[p+1] are problem p's
+ * rows.  Per-problem reductions never mix problems, so each result is the same
+ * whether the problem is solved alone or in any batch. */
+typedef struct fv_batch fv_batch;
+
+#define FV_BATCH_FP64 0  /* Krylov in FP64, reference semantics per problem */
+#define FV_BATCH_MIXED 1 /* FP32 Krylov + FP32 factors with FP64 reliable updates: whenever the
+                            FP32 residual estimate fell by inner_relative_tolerance (or reached the
+                            target), x64 += d32 and the residual is recomputed as b - A x64 in FP64
+                            and replaces the FP32 one; the solve stops when that FP64 residual
+                            |b - A x| / |b| <= outer_tolerance. */
+
+typedef struct fv_batch_options {
+    int32_t precision;               /* FV_BATCH_FP64 or FV_BATCH_MIXED */
+    double relative_tolerance;       /* FP64 mode: the CG rtol / atol of LinearSolverOptions */
+    double absolute_tolerance;
+    int64_t max_iterations;          /* per inner solve */
+    double inner_relative_tolerance; /* mixed: residual reduction that triggers a replacement (e.g. 1e-2) */
+    double outer_tolerance;          /* mixed: stop when |b - A x| / |b| <= this (FP64) */
+    int32_t max_outer;               /* unused (kept for ABI stability) */
+} fv_batch_options;
+
+typedef struct fv_batch_info {
+    double device_ms;
+    int64_t launched_iterations;     /* CG iterations enqueued for the whole batch */
+    int64_t *iterations;             /* per problem (optional): Krylov iterations */
+    int32_t *outer_steps;            /* per problem (optional): FP64 residual replacements (mixed) */
+    double *final_residual;          /* per problem (optional): FP64 mode |r|/|b| as LinearSolverInfo;
+                                        mixed: the true FP64 |b - A x| / |b| */
+    int32_t *status;                 /* per problem (optional) */
+    int32_t *fp64_fallback;          /* per problem (optional, mixed): 1 when the FP32 run stagnated
+                                        (no FP64 progress over two replacements; kappa * eps32 >> 1) and
+                                        an FP64 batched pass over the stagnated problems finished it */
+} fv_batch_info;
+
+fv_status fv_batch_create(const fv_csr *A, int32_t n_problems, const int64_t *row_offsets, int32_t tile_rows,
+                          void *stream, fv_batch **out);
+/* x0 = 0 for every problem; P is the IC(0) (CG) or ILU(0) (BiCGStab) of A. */
+fv_status fv_batch_cg(fv_batch *B, fv_precond *P, const double *b, double *x, const fv_batch_options *opt,
+                      fv_batch_info *info, void *stream);
+fv_status fv_batch_bicgstab(fv_batch *B, fv_precond *P, const double *b, double *x, const fv_batch_options *opt,
+                            fv_batch_info *info, void *stream);
+fv_status fv_batch_destroy(fv_batch *B);
+
 /* Allocation-free conjugate gradient.  No counterpart in the reference crate.
  *
  * Same contract and same results as fv_cg, for callers that must not allocate

@@ -1,0 +1,167 @@
+"""Batched solves (block-diagonal union of independent meshes) on the GPU.
+
+- the union's assembly and IC(0) are the per-problem ones, bit for bit
+- FP64 batched CG matches the oracle per problem (<=1e-10, iterations +-2)
+- each problem's result is identical alone and in a mix (per-problem reductions)
+- mixed precision (FP32 CG inside FP64 refinement) reaches the FP64 tolerance and
+  an error <= 1e-8 against a tight FP64 oracle solve
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(fv, sides, seed0=100):
+    out = []
+    for k, s in enumerate(sides):
+        m = fv.Mesh.square(s, 0.2, seed0 + k)
+        sigma = 0.5 + 1.5 * ((k * 0.37) % 1.0)
+        kf, _, sc = m.fields(seed0 + k, 1.0, sigma, source_const=1.0)
+        out.append((m, kf, sc))
+    return out
+
+
+def _union_system(fv, probs):
+    from fvb200.batch import MeshBatch
+    mb = MeshBatch([p[0] for p in probs])
+    kf = mb.face_field([p[1] for p in probs])
+    sc = mb.cell_field([p[2] for p in probs])
+    nb = mb.n_boundary_faces
+    eq = -fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+    A, b = fv.assemble(eq, (np.zeros(nb), np.zeros(nb)), mb)
+    return mb, A, b
+
+
+def test_union_assembly_and_ic0_are_per_problem(fv, orc):
+    probs = _problems(fv, [6, 9, 4])
+    mb, A, b = _union_system(fv, probs)
+    gp, gc, gv = A.to_csr()
+    P = fv.IncompleteCholesky.from_matrix(A, 0)
+    fp, fc, fvv, _ = P.factors()
+    bb = b.numpy()
+    for k, (m, kf, sc) in enumerate(probs):
+        r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+        nb = m.n_boundary_faces
+        ptr, cols, vals, rhs = orc.assemble(m, -1.0, 0.0, -1.0, kappa=kf, source=sc, bndi=np.zeros(nb),
+                                            bnde=np.zeros(nb))
+        a0, a1 = gp[r0], gp[r1]
+        assert np.array_equal(gp[r0:r1 + 1] - a0, ptr)
+        assert np.array_equal(gc[a0:a1] - r0, cols)
+        assert np.array_equal(gv[a0:a1], vals)
+        assert np.array_equal(bb[r0:r1], rhs)
+        op, oc, ov, _, _ = orc.Precond("ic", ptr, cols, vals).export()
+        f0, f1 = fp[r0], fp[r1]
+        assert np.array_equal(fc[f0:f1] - r0, oc) and np.array_equal(fvv[f0:f1], ov)
+
+
+def test_batch_fp64_matches_oracle(fv, orc):
+    from fvb200.batch import BatchCG
+    probs = _problems(fv, [12, 20, 7, 16])
+    mb, A, b = _union_system(fv, probs)
+    P = fv.IncompleteCholesky.from_matrix(A, 0)
+    x = fv.DistributedVector.from_size(mb.n_cells)
+    bc = BatchCG(A, mb.cell_offsets, 256)
+    out = bc.solve(P, b, x, precision="fp64", relative_tolerance=1e-12, absolute_tolerance=1e-12, max_iterations=3000)
+    xs = x.numpy()
+    for k, (m, kf, sc) in enumerate(probs):
+        nb = m.n_boundary_faces
+        ptr, cols, vals, rhs = orc.assemble(m, -1.0, 0.0, -1.0, kappa=kf, source=sc, bndi=np.zeros(nb),
+                                            bnde=np.zeros(nb))
+        xo, io = orc.cg(ptr, cols, vals, orc.Precond("ic", ptr, cols, vals), rhs, rtol=1e-12, atol=1e-12, maxit=3000)
+        r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+        assert abs(int(out["iterations"][k]) - io["iterations"]) <= 2
+        assert np.linalg.norm(xs[r0:r1] - xo) <= 1e-10 * np.linalg.norm(xo)
+        assert out["status"][k] == 0
+
+
+def test_batch_result_same_alone_and_in_mix(fv):
+    from fvb200.batch import BatchCG
+    probs = _problems(fv, [10, 15, 6, 13, 8], seed0=300)
+    target = 3
+    results = {}
+    for name, subset in (("alone", [target]), ("mix", list(range(len(probs))))):
+        sel = [probs[i] for i in subset]
+        mb, A, b = _union_system(fv, sel)
+        P = fv.IncompleteCholesky.from_matrix(A, 0)
+        for precision in ("fp64", "mixed"):
+            x = fv.DistributedVector.from_size(mb.n_cells)
+            out = BatchCG(A, mb.cell_offsets, 512).solve(P, b, x, precision=precision, relative_tolerance=1e-8,
+                                                        absolute_tolerance=1e-8, outer_tolerance=1e-10)
+            k = subset.index(target)
+            r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+            results[(name, precision)] = (x.numpy()[r0:r1].copy(), int(out["iterations"][k]))
+    for precision in ("fp64", "mixed"):
+        xa, ia = results[("alone", precision)]
+        xm, im = results[("mix", precision)]
+        assert ia == im
+        assert np.array_equal(xa, xm)
+
+
+def test_batch_mixed_precision_accuracy(fv, orc):
+    from fvb200.batch import BatchCG
+    probs = _problems(fv, [24, 32, 18], seed0=500)
+    mb, A, b = _union_system(fv, probs)
+    P = fv.IncompleteCholesky.from_matrix(A, 0)
+    x = fv.DistributedVector.from_size(mb.n_cells)
+    out = BatchCG(A, mb.cell_offsets, 1024).solve(P, b, x, precision="mixed", outer_tolerance=1e-10,
+                                                  inner_relative_tolerance=1e-4, max_outer=30)
+    xs = x.numpy()
+    for k, (m, kf, sc) in enumerate(probs):
+        nb = m.n_boundary_faces
+        ptr, cols, vals, rhs = orc.assemble(m, -1.0, 0.0, -1.0, kappa=kf, source=sc, bndi=np.zeros(nb),
+                                            bnde=np.zeros(nb))
+        xo, _ = orc.cg(ptr, cols, vals, orc.Precond("ic", ptr, cols, vals), rhs, rtol=1e-13, atol=1e-13, maxit=5000)
+        r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+        assert out["final_residual"][k] <= 1e-10
+        assert out["outer_steps"][k] >= 1 or out["fp64_fallback"][k] == 1
+        assert np.linalg.norm(xs[r0:r1] - xo) <= 1e-8 * np.linalg.norm(xo)
+        # the true FP64 residual of the returned solution
+        import scipy.sparse as sp
+        Ak = sp.csr_matrix((vals, cols, ptr))
+        assert np.linalg.norm(rhs - Ak @ xs[r0:r1]) <= 1.0001e-10 * np.linalg.norm(rhs)
+
+
+def _cube_problems(fv, sides, seed0=700):
+    out = []
+    for k, n in enumerate(sides):
+        m = fv.Mesh.cube(n, 0.15, seed0 + k)
+        kappa0 = float(np.linalg.norm((1.0, 0.5, 0.25))) / n / 3.0
+        kf, fl, sc = m.fields(seed0 + k, kappa0, 0.5, velocity=(1.0, 0.5, 0.25), source_uniform=True)
+        out.append((m, kf, fl, sc))
+    return out
+
+
+def test_batch_bicgstab_fp64_and_mixed(fv, orc):
+    """Convection-diffusion problems, BiCGStab + ILU(0): FP64 batched matches the
+    oracle per problem; mixed precision (FP32 BiCGStab + FP32 ILU(0) inside FP64
+    refinement) reaches |b-Ax|/|b| <= 1e-10 and error <= 1e-8."""
+    from fvb200.batch import BatchCG, MeshBatch
+    probs = _cube_problems(fv, [5, 7, 4])
+    mb = MeshBatch([p[0] for p in probs])
+    kf = mb.face_field([p[1] for p in probs])
+    fl = mb.face_field([p[2] for p in probs])
+    sc = mb.cell_field([p[3] for p in probs])
+    nb = mb.n_boundary_faces
+    eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+    A, b = fv.assemble(eq, (np.zeros(nb), np.zeros(nb)), mb)
+    P = fv.IncompleteLowerUpper.from_matrix(A, 0)
+    bc = BatchCG(A, mb.cell_offsets, 256)
+    x64 = fv.DistributedVector.from_size(mb.n_cells)
+    o64 = bc.solve(P, b, x64, precision="fp64", relative_tolerance=1e-12, absolute_tolerance=1e-12,
+                   max_iterations=2000, solver="bicgstab")
+    xm = fv.DistributedVector.from_size(mb.n_cells)
+    om = bc.solve(P, b, xm, precision="mixed", outer_tolerance=1e-10, inner_relative_tolerance=1e-4,
+                  max_iterations=2000, solver="bicgstab")
+    a64, am = x64.numpy(), xm.numpy()
+    for k, (m, kfk, flk, sck) in enumerate(probs):
+        nbk = m.n_boundary_faces
+        ptr, cols, vals, rhs = orc.assemble(m, -1.0, 1.0, -1.0, kappa=kfk, flux=flk, source=sck, bndi=np.zeros(nbk),
+                                            bnde=np.zeros(nbk))
+        o = orc.Precond("ilu", ptr, cols, vals)
+        xo, io = orc.bicgstab(ptr, cols, vals, o, rhs, rtol=1e-12, atol=1e-12, maxit=2000)
+        r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+        assert abs(int(o64["iterations"][k]) - io["iterations"]) <= 2
+        assert np.linalg.norm(a64[r0:r1] - xo) <= 1e-10 * np.linalg.norm(xo)
+        assert om["final_residual"][k] <= 1e-10
+        assert np.linalg.norm(am[r0:r1] - xo) <= 1e-8 * np.linalg.norm(xo)
