@@ -40,6 +40,10 @@ WORKLOADS = {
     # the CPU-runnable 2D case: 256x256 squares x 2 triangles, lognormal(0,1)
     "square256_diffusion": dict(kind="2d", n=256, jitter=0.2, sigma=1.0, solver="cg"),
     # smaller versions (profiling captures, smoke runs); cube64 still exceeds L2
+    # BASELINE mixed-precision configuration: the 3D case with FP32 BiCGStab + FP32 ILU(0)
+    # inside FP64 reliable updates, to |b - A x| / |b| <= 1e-10
+    "cube128_convdiff_mixed": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
+                                   solver="bicgstab", precision="mixed"),
     "cube64_convdiff": dict(kind="3d", n=64, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     "cube32_convdiff": dict(kind="3d", n=32, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     # BASELINE batched configuration: 1,024 2D diffusion problems, mixed precision
@@ -180,12 +184,24 @@ def gpu_arm(args, rank, world, local_rank):
     P = Pcls.from_matrix(A, 0)
     x = fv.DistributedVector.from_size(N)
 
+    mixed = wl.get("precision") == "mixed"
+    if mixed:
+        from types import SimpleNamespace
+
+        from fvb200.batch import BatchCG
+        single = BatchCG(A, [0, N], 2048)
+
     # one step: value assembly (new rhs), refactorisation, solve from x0 = 0
     def step_b():
         nonlocal b
         _, b = fv.assemble(eq, bc, mesh, lhs=A)
         P.refactor()
         x.data.zero_()
+        if mixed:
+            o = single.solve(P, b, x, precision="mixed", outer_tolerance=1e-10, inner_relative_tolerance=1e-2,
+                             max_iterations=20000, solver=wl["solver"])
+            return SimpleNamespace(iterations=int(o["iterations"][0]), refinements=int(o["outer_steps"][0]),
+                                   fallback=int(o["fp64_fallback"][0]), final=float(o["final_residual"][0]))
         return solve(x, A, b, P, None, opts)
 
     for _ in range(args.warmup):
@@ -225,6 +241,14 @@ def gpu_arm(args, rank, world, local_rank):
     r = fv.DistributedVector.from_size(N)
     A.imul(r, x)
     relres = float(torch.linalg.norm(r.data - b.data) / torch.linalg.norm(b.data))
+    mixed_info = None
+    if mixed:
+        xt = fv.DistributedVector.from_size(N)
+        solve(xt, A, b, P, None, fv.LinearSolverOptions(1e-13, 1e-13, 20000))
+        err = float(torch.linalg.norm(x.data - xt.data) / torch.linalg.norm(xt.data))
+        mixed_info = {"refinement_steps": info.refinements, "fp64_fallback": info.fallback,
+                      "final_fp64_residual": info.final, "rel_err_vs_fp64_tight": err}
+        del xt
 
     # ---- end to end through the public API with host buffers
     pin = {k: torch.empty(len(prob[k]), dtype=torch.float64).pin_memory()
@@ -237,10 +261,7 @@ def gpu_arm(args, rank, world, local_rank):
     def e2e_step():
         for k, t in pin.items():
             T[k].copy_(t, non_blocking=True)
-        _, bb = fv.assemble(eq, bc, mesh, lhs=A)
-        P.refactor()
-        x.data.zero_()
-        solve(x, A, bb, P, None, opts)
+        step_b()
         x_host.copy_(x.data, non_blocking=True)
 
     e2e_step()
@@ -300,7 +321,7 @@ def gpu_arm(args, rank, world, local_rank):
         elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
         e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
         kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
-        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A,
+        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A, mixed_info=mixed_info,
     )
     return res
 
@@ -711,6 +732,10 @@ def main():
         "clocks": res["clocks"],
         "mesh_build_s": round(res["t_mesh"], 2),
     }
+    if res.get("mixed_info"):
+        line["dtype"] = "f32-inner/f64-refinement"
+        line["config"]["precision"] = "FP32 BiCGStab + FP32 ILU(0), FP64 reliable updates to |b-Ax|/|b| <= 1e-10"
+        line["mixed"] = res["mixed_info"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

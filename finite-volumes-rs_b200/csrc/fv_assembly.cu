@@ -203,6 +203,8 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
 #include <atomic>
 static std::atomic<unsigned long long> g_launches{0};
 void fv_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void fv_note_launches(long long delta) { g_launches.fetch_add((unsigned long long)delta, std::memory_order_relaxed); }
+unsigned long long fv_launches_now() { return g_launches.load(std::memory_order_relaxed); }
 extern "C" uint64_t fv_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 static thread_local char g_last_error[256];

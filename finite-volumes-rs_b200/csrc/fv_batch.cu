@@ -70,10 +70,12 @@ struct BGlobal {
 };
 
 constexpr int TB = 256;  // threads per tile block
+constexpr int kMaxTileSums = 3;  // largest NV of finish_tile (kbm_rep2); sizes the partial-sum buffer
 
 template <int NV, class Epi>
 __device__ __forceinline__ void finish_tile(double (&v)[NV], int p, int64_t t, const int32_t *__restrict__ ptile,
                                             double *partial, BProb *S, BGlobal *G, Epi epi) {
+    static_assert(NV <= kMaxTileSums, "the partial-sum buffer holds kMaxTileSums values per tile");
     __shared__ double sm[NV * 32];
     __shared__ bool last;
     fv_block_reduce<NV>(v, sm);
@@ -698,7 +700,7 @@ extern "C" fv_status fv_batch_create(const fv_csr *A, int32_t n_problems, const 
     up(&B->row_prob, rp);
     if (e == cudaSuccess) e = cudaMalloc(&B->S, sizeof(BProb) * n_problems);
     if (e == cudaSuccess) e = cudaMalloc(&B->G, sizeof(BGlobal));
-    if (e == cudaSuccess) e = cudaMalloc(&B->partial, sizeof(double) * B->ntiles * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&B->partial, sizeof(double) * B->ntiles * kMaxTileSums);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         fv_internal_set_cuda_error(e, "fv_batch_create");

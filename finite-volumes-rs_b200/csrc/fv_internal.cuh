@@ -29,6 +29,8 @@ void fv_internal_set_cuda_error(cudaError_t e, const char *what);
 void fv_internal_set_error_text(const char *what);
 // Counts kernel launches made by this library (fv_launch_count).
 void fv_note_launch();
+void fv_note_launches(long long delta);  // graph replays add, captures (not run) subtract
+unsigned long long fv_launches_now();
 
 static inline cudaStream_t fv_stream(void *s) { return (cudaStream_t)s; }
 

@@ -523,7 +523,65 @@ fv_status apply_or_copy(fv_precond *P, const double *r, double *z, int64_t n, in
     return FV_OK;
 }
 
-int batch_size(int64_t n) { return n >= (1 << 20) ? 2 : 8; }
+int batch_size(int64_t n) { return n >= (1 << 20) ? 4 : 8; }
+
+// Runs body(stream) -- one batch of iterations -- until the device state says
+// done.  The batch is captured once into a CUDA graph on a private stream (the
+// legacy default stream cannot be captured) and replayed, so the GPU runs the
+// iterations back to back and the host only reads one state word per replay.
+// Falls back to plain launches on the caller's stream when capture fails.
+template <class Body>
+fv_status loop_until_done(const Workspace &w, cudaStream_t st, Body body, SolverState &h) {
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    long long per_replay = 0;
+    bool graph_ok = false;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+        cudaEventRecord(ev, st);
+        cudaStreamWaitEvent(cs, ev, 0);
+        const unsigned long long c0 = fv_launches_now();
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const fv_status bs = body(cs);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(cs, &g);
+            if (bs == FV_OK && e == cudaSuccess && g && cudaGraphInstantiate(&gx, g, 0) == cudaSuccess)
+                graph_ok = true;
+            if (g) cudaGraphDestroy(g);
+        }
+        per_replay = (long long)(fv_launches_now() - c0);
+        fv_note_launches(-per_replay);  // captured, not run
+        cudaGetLastError();
+    }
+    fv_status s = FV_OK;
+    if (graph_ok) {
+        while (true) {
+            cudaError_t e = cudaGraphLaunch(gx, cs);
+            if (e != cudaSuccess) {
+                fv_internal_set_cuda_error(e, "cudaGraphLaunch");
+                s = FV_ERR_CUDA;
+                break;
+            }
+            fv_note_launches(per_replay);
+            s = read_state(w, h, cs);
+            if (s != FV_OK || h.done) break;
+        }
+        cudaEventRecord(ev, cs);
+        cudaStreamWaitEvent(st, ev, 0);
+    } else {
+        while (true) {
+            s = body(st);
+            if (s != FV_OK) break;
+            s = read_state(w, h, st);
+            if (s != FV_OK || h.done) break;
+        }
+    }
+    if (gx) cudaGraphExecDestroy(gx);
+    if (ev) cudaEventDestroy(ev);
+    if (cs) cudaStreamDestroy(cs);
+    return s;
+}
 
 }  // namespace
 
@@ -549,19 +607,18 @@ extern "C" fv_status fv_cg(const fv_csr *A, fv_precond *P, const double *b, doub
     FV_CUDA_TRY(cudaGetLastError());
     SolverState h{};
     const int B = batch_size(n);
-    for (int64_t it = 0; s == FV_OK;) {
-        for (int q = 0; q < B && s == FV_OK; ++q, ++it) {
-            fv_note_launch(), k_cg_spmv<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, p, ap, S);
-            fv_note_launch(), k_cg_update<<<G, RB, 0, st>>>(n, x, r, p, ap, S);
-            s = apply_or_copy(P, r, z, n, G, S, st);
-            fv_note_launch(), k_cg_rz<<<G, RB, 0, st>>>(n, r, z, S);
-            fv_note_launch(), k_cg_p<<<G, RB, 0, st>>>(n, z, p, S);
+    auto body = [&](cudaStream_t q_st) -> fv_status {
+        for (int q = 0; q < B; ++q) {
+            fv_note_launch(), k_cg_spmv<<<G, RB, 0, q_st>>>(n, A->row_ptr, A->cols, A->vals, p, ap, S);
+            fv_note_launch(), k_cg_update<<<G, RB, 0, q_st>>>(n, x, r, p, ap, S);
+            FV_TRY(apply_or_copy(P, r, z, n, G, S, q_st));
+            fv_note_launch(), k_cg_rz<<<G, RB, 0, q_st>>>(n, r, z, S);
+            fv_note_launch(), k_cg_p<<<G, RB, 0, q_st>>>(n, z, p, S);
         }
         FV_CUDA_TRY(cudaGetLastError());
-        if (s != FV_OK) break;
-        FV_TRY(read_state(w, h, st));
-        if (h.done) break;
-    }
+        return FV_OK;
+    };
+    if (s == FV_OK) s = loop_until_done(w, st, body, h);
     cudaEventRecord(e1, st);
     if (s == FV_OK) s = read_state(w, h, st);
     float ms = 0.f;
@@ -595,21 +652,20 @@ extern "C" fv_status fv_bicgstab(const fv_csr *A, fv_precond *P, const double *b
     fv_status s = FV_OK;
     SolverState h{};
     const int B = batch_size(n);
-    for (int64_t it = 0; s == FV_OK;) {
-        for (int q = 0; q < B && s == FV_OK; ++q, ++it) {
-            s = apply_or_copy(P, p, y, n, G, S, st);
-            fv_note_launch(), k_bi_spmv1<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, y, v, rh, S);
-            fv_note_launch(), k_bi_s<<<G, RB, 0, st>>>(n, r, v, s_, S);
-            if (s == FV_OK) s = apply_or_copy(P, s_, z, n, G, S, st);
-            fv_note_launch(), k_bi_spmv2<<<G, RB, 0, st>>>(n, A->row_ptr, A->cols, A->vals, z, t, s_, S);
-            fv_note_launch(), k_bi_update<<<G, RB, 0, st>>>(n, x, r, y, z, s_, t, rh, S);
-            fv_note_launch(), k_bi_p<<<G, RB, 0, st>>>(n, r, v, p, rh, S);
+    auto body = [&](cudaStream_t q_st) -> fv_status {
+        for (int q = 0; q < B; ++q) {
+            FV_TRY(apply_or_copy(P, p, y, n, G, S, q_st));
+            fv_note_launch(), k_bi_spmv1<<<G, RB, 0, q_st>>>(n, A->row_ptr, A->cols, A->vals, y, v, rh, S);
+            fv_note_launch(), k_bi_s<<<G, RB, 0, q_st>>>(n, r, v, s_, S);
+            FV_TRY(apply_or_copy(P, s_, z, n, G, S, q_st));
+            fv_note_launch(), k_bi_spmv2<<<G, RB, 0, q_st>>>(n, A->row_ptr, A->cols, A->vals, z, t, s_, S);
+            fv_note_launch(), k_bi_update<<<G, RB, 0, q_st>>>(n, x, r, y, z, s_, t, rh, S);
+            fv_note_launch(), k_bi_p<<<G, RB, 0, q_st>>>(n, r, v, p, rh, S);
         }
         FV_CUDA_TRY(cudaGetLastError());
-        if (s != FV_OK) break;
-        FV_TRY(read_state(w, h, st));
-        if (h.done) break;
-    }
+        return FV_OK;
+    };
+    s = loop_until_done(w, st, body, h);
     fv_note_launch(), k_bi_finish<<<G, RB, 0, st>>>(n, x, y, S);
     cudaEventRecord(e1, st);
     if (s == FV_OK) s = read_state(w, h, st);

@@ -43,6 +43,7 @@ class Request:
     iterations: int = 0
     residual: float = float("nan")
     solution: np.ndarray | None = None
+    error: str | None = None
 
 
 def request_stream(rate: float, duration: float, seed: int, mix_3d: float = 0.5, lo: float = 1e4,
@@ -132,7 +133,7 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
         P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(A, 0, stream=stream)
         x = fv.DistributedVector.from_size(mb.n_cells)
         solver = BatchCG(A, mb.cell_offsets, tile_rows, stream=stream)
-        out = solver.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-4,
+        out = solver.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-2,
                            max_outer=30, max_iterations=20000, stream=stream,
                            solver="cg" if kind == "2d" else "bicgstab")
         xs = x.data.cpu().numpy() if keep_solution else None
@@ -151,14 +152,26 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
 
 
 class Server:
+    """solve_fn(fv, cache, wave, stream) solves a wave in place (default: solve_wave);
+    it is a parameter so the scheduling can be exercised without a GPU."""
+
     def __init__(self, fv, workers: int = 3, budget_bytes: int | None = None, max_wave_cells: int = 16_000_000,
-                 max_wave_requests: int = 256):
-        import torch
+                 max_wave_requests: int = 256, solve_fn=None, make_stream=None):
         self.fv = fv
         self.cache = MeshCache(fv)
         self.workers = workers
-        free, total = torch.cuda.mem_get_info()
-        self.budget = budget_bytes if budget_bytes is not None else int(free * 0.7)
+        self.solve_fn = solve_fn or solve_wave
+        if make_stream is None:
+            import torch
+            make_stream = torch.cuda.Stream
+        self.make_stream = make_stream
+        if budget_bytes is None:
+            import torch
+            free, total = torch.cuda.mem_get_info()
+            budget_bytes = int(free * 0.7)
+        self.budget = budget_bytes
+        self.peak_reserved = 0
+        self.failed = 0
         self.max_wave_cells = max_wave_cells
         self.max_wave_requests = max_wave_requests
         self.lock = threading.Condition()
@@ -173,11 +186,9 @@ class Server:
     def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True) -> dict:
         """Serve `requests` (arrival times relative to now).  Returns latency and
         throughput statistics over the completed requests."""
-        import torch
-        if warm:  # one small wave of each kind compiles nothing but brings the driver up
+        if warm:  # one small wave of each kind brings the driver and the caches up
             for kind, side in (("2d", 8), ("3d", 3)):
-                solve_wave(self.fv, self.cache, [Request(-1, 0.0, kind, side, 1, cells=1)],
-                           torch.cuda.Stream())
+                self.solve_fn(self.fv, self.cache, [Request(-1, 0.0, kind, side, 1, cells=1)], self.make_stream())
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter()
         stop = threading.Event()
@@ -193,6 +204,7 @@ class Server:
                             break  # admission by free device memory
                         pending.popleft()
                         self.reserved += c
+                        self.peak_reserved = max(self.peak_reserved, self.reserved)
                         self.admitted.append(r)
                         self.lock.notify_all()
                     if not pending and not self.admitted:
@@ -200,7 +212,7 @@ class Server:
                 time.sleep(0.0005)
 
         def worker():
-            stream = torch.cuda.Stream()
+            stream = self.make_stream()
             while True:
                 with self.lock:
                     while not self.admitted and not stop.is_set():
@@ -225,7 +237,14 @@ class Server:
                 for r in wave:
                     r.start = start
                     r.wave = wid
-                solve_wave(self.fv, self.cache, wave, stream)
+                try:
+                    self.solve_fn(self.fv, self.cache, wave, stream)
+                except Exception as e:  # a failed wave fails its requests, not the server
+                    for r in wave:
+                        r.error = f"{type(e).__name__}: {e}"
+                        r.residual = float("nan")
+                    with self.lock:
+                        self.failed += len(wave)
                 fin = time.perf_counter() - t0
                 with self.lock:
                     for r in wave:
@@ -251,11 +270,12 @@ class Server:
         for w in ws:
             w.join(timeout=max(1.0, deadline - time.perf_counter() + 600))
         wall = time.perf_counter() - t0
-        fin = [r for r in self.done if r.finish >= 0]
+        fin = [r for r in self.done if r.finish >= 0 and r.error is None]
         lat = np.array([r.finish - r.arrival for r in fin]) if fin else np.zeros(0)
         span = (max(r.finish for r in fin) - min(r.arrival for r in fin)) if fin else 0.0
         return {
-            "completed": len(fin), "offered": len(requests), "waves": self.waves, "wall_s": wall,
+            "completed": len(fin), "offered": len(requests), "failed": self.failed, "waves": self.waves,
+            "wall_s": wall, "peak_reserved_bytes": self.peak_reserved, "budget_bytes": self.budget,
             "solves_per_s": len(fin) / span if span > 0 else 0.0,
             "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
