@@ -560,13 +560,17 @@ __global__ void __launch_bounds__(TB) kbm_rep2(Tiles tl, const int32_t *__restri
             // residual): the FP32 run cannot resolve this problem.  The first
             // time, restart the Krylov space from the true residual; the
             // second time, give up on FP32 (an FP64 pass finishes it).
-            // progress expected: a replacement triggered by a 1/delta drop of the
+            // Progress expected: a replacement triggered by a 1/delta drop of the
             // FP32 estimate must at least halve the FP64 residual; a forced one
-            // must not let it grow
+            // (128 iterations without a trigger) must cut it by 10%.
+            // A progress-triggered replacement also fails when the true
+            // residual is far above the FP32 estimate that triggered it: the
+            // FP32 recursion has decoupled from the FP64 residual.
             bool fresh = false;
-            const double need = s.forced ? 1.0 : 0.5;
+            const double need = s.forced ? 0.9 : 0.5;
+            const bool gap = !s.forced && s.res64 * s.bnorm64 > 100.0 * s.error * s.bnorm;
             s.iter_at_rep = s.iter;
-            if (!isfinite(s.res64) || (s.n_replace > 1 && s.res64 > need * s.prev_res64)) {
+            if (!isfinite(s.res64) || gap || (s.n_replace > 1 && s.res64 > need * s.prev_res64)) {
                 s.strikes += 1;
                 if (s.strikes >= 2 || !isfinite(s.res64)) {
                     s.stagnated = 1;

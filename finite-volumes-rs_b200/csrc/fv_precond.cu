@@ -489,7 +489,9 @@ static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int3
 static int sweep_grid(int64_t n) {
     int64_t warps = (n + 31) / 32;
     int64_t blocks = (warps + 7) / 8;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 8));
+    // 592 blocks of 8 warps: enough chunks in flight to fill the memory system;
+    // more warps only add pollers that compete with the level frontier for L2
+    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 4));
 }
 
 // z = M^-1 r.  r must not alias z.  The forward sweep writes P->tmp and
