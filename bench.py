@@ -92,8 +92,9 @@ class Clocks:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, tag: str = ""):
         self.index = index
+        self.tag = tag
         self.proc = None
         self.path = None
 
@@ -101,7 +102,7 @@ class Clocks:
         try:
             out = ROOT / "gpurun_out"
             out.mkdir(exist_ok=True)
-            self.path = out / f"clocks_rank{self.index}.csv"
+            self.path = out / f"clocks_rank{self.index}{self.tag}.csv"
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
@@ -269,14 +270,24 @@ def gpu_arm(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+    clk2 = Clocks(local_rank, "_e2e")
+    clk2.start()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
+    e2e_lat = []
     e2.record(stream)
     for _ in range(args.steps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
         e2e_step()
+        s1.record(stream)
+        e2e_lat.append((s0, s1))
     e3.record(stream)
     torch.cuda.synchronize()
+    e2e_clocks = clk2.stop()
     e2e_elapsed = e2.elapsed_time(e3) / 1e3
+    e2e_lat_ms = [round(a.elapsed_time(c), 1) for a, c in e2e_lat]
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([e2e_elapsed], device=dev, dtype=torch.float64)
@@ -320,6 +331,7 @@ def gpu_arm(args, rank, world, local_rank):
     res = dict(
         elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
         e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
+        e2e_lat_ms=e2e_lat_ms, e2e_clocks=e2e_clocks,
         kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
         levels=P.levels()[2:], mesh=mesh, prob=prob, A=A, mixed_info=mixed_info,
     )
@@ -727,7 +739,8 @@ def main():
         "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]),
         "cpu_baseline": cpu,
         "e2e": {"value": round(solves / res["e2e_elapsed"], 6), "unit": "solves/s",
-                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+                "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"],
+                "step_ms": res["e2e_lat_ms"], "clocks": res["e2e_clocks"]},
         "gpu_launches": int(res["launches"]),
         "clocks": res["clocks"],
         "mesh_build_s": round(res["t_mesh"], 2),

@@ -192,10 +192,170 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
     a.rhs[i] = rhs;
 }
 
+// The same row arithmetic with every per-face quantity in registers (MAXF is
+// small: 4 for triangles and tetrahedra, 8 up to hexahedra).  All gathers of a
+// cell (incidences, face data, the other cells' centres) are issued before any
+// of them is used, the slot of each neighbour in the sorted row is a count of
+// smaller distinct neighbours instead of a sort, and the block's rows are
+// staged in shared memory so the stores of the values are coalesced.  Each
+// output value receives the same additions in the same order as in k_assemble.
+constexpr int kAsmBlock = 128;
+
+template <int DIM, int MAXF>
+__global__ void __launch_bounds__(kAsmBlock) k_assemble_reg(AssembleArgs a) {
+    extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
+    const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
+    const int64_t i = b0 + threadIdx.x;
+    const int64_t bend = min(b0 + (int64_t)kAsmBlock, a.n);
+    const int base = a.row_ptr[b0];
+    const int top = a.row_ptr[bend];
+    const bool live = i < a.n;
+    int s = 0, deg = 0;
+    if (live) {
+        s = a.cf_ptr[i];
+        deg = a.cf_ptr[i + 1] - s;
+    }
+    int fe[MAXF], jj[MAXF];
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) {
+        fe[k] = 0;
+        jj[k] = -1;
+        if (k < deg) {
+            fe[k] = a.cf_face[s + k];
+            jj[k] = a.cf_other[s + k];
+        }
+    }
+    double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    double srci = 0.0;
+    if (live) {
+        ci4 = a.cell[i];
+        if (a.c_src != 0.0) srci = a.src[i];
+    }
+    double4 oc[MAXF];
+    double ar[MAXF], kp[MAXF], fl[MAXF], bi[MAXF], be[MAXF];
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) {
+        oc[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+        ar[k] = kp[k] = fl[k] = bi[k] = be[k] = 0.0;
+        if (k < deg) {
+            const int f = fe[k] & 0x7fffffff;
+            ar[k] = a.area[f];
+            if (a.c_lap != 0.0) kp[k] = a.kappa[f];
+            if (a.c_conv != 0.0) fl[k] = a.flux[f];
+            if (jj[k] >= 0) {
+                oc[k] = a.cell[jj[k]];
+            } else {
+                oc[k] = a.bfc[f - a.fb0];
+                bi[k] = a.bndi[f - a.fb0];
+                be[k] = a.bnde[f - a.fb0];
+            }
+        }
+    }
+    // distinct neighbours: the first incidence of each other cell carries its slot
+    bool first[MAXF];
+    int ndist = 0, pd = 0;
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) {
+        bool f1 = jj[k] >= 0;
+#pragma unroll
+        for (int q = 0; q < k; ++q) f1 = f1 && (jj[q] != jj[k]);
+        first[k] = f1;
+        ndist += f1 ? 1 : 0;
+        pd += (f1 && jj[k] < (int)i) ? 1 : 0;
+    }
+    const double V = ci4.w;
+    const double lcell = 0.0;
+    const double rcell = a.c_src != 0.0 ? a.c_src * (-srci) : 0.0;
+    double diag = lcell * V;
+    double rhs = rcell * V;
+    double acc[MAXF];
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) acc[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) {
+        if (k < deg) {
+            const bool is_nb = fe[k] < 0;
+            double3 pi, pj;
+            if (jj[k] >= 0 && is_nb) {
+                pi = make_double3(oc[k].x, oc[k].y, oc[k].z);
+                pj = make_double3(ci4.x, ci4.y, ci4.z);
+            } else {
+                pi = make_double3(ci4.x, ci4.y, ci4.z);
+                pj = make_double3(oc[k].x, oc[k].y, oc[k].z);
+            }
+            double d2 = 0.0;
+            {
+                double dd = pj.x - pi.x;
+                d2 += dd * dd;
+                dd = pj.y - pi.y;
+                d2 += dd * dd;
+                if (DIM == 3) {
+                    dd = pj.z - pi.z;
+                    d2 += dd * dd;
+                }
+            }
+            const double t = 1.0 / sqrt(d2);
+            double li, lj;
+            face_terms(t, kp[k], fl[k], a.c_lap, a.c_conv, li, lj);
+            const double A = ar[k];
+            li = li * A;
+            lj = lj * A;
+            const double ra = 0.0 * A;
+            if (jj[k] < 0) {
+                diag += li;
+                diag += lj * bi[k];
+                rhs += ra - lj * be[k];
+            } else {
+                // the value of this neighbour's slot sits in acc[] of its first incidence
+#pragma unroll
+                for (int q = 0; q <= k; ++q) {
+                    if (first[q] && jj[q] == jj[k]) {
+                        if (!is_nb)
+                            acc[q] += lj;
+                        else
+                            acc[q] -= li;
+                    }
+                }
+                if (!is_nb) {
+                    diag += li;
+                    rhs += ra;
+                } else {
+                    diag -= lj;
+                    rhs -= ra;
+                }
+            }
+        }
+    }
+    if (live) {
+        const int r0 = a.row_ptr[i] - base;
+        stage[r0 + pd] = diag;
+#pragma unroll
+        for (int k = 0; k < MAXF; ++k) {
+            if (first[k]) {
+                int pos = jj[k] > (int)i ? 1 : 0;
+#pragma unroll
+                for (int q = 0; q < MAXF; ++q) pos += (first[q] && jj[q] < jj[k]) ? 1 : 0;
+                stage[r0 + pos] = acc[k];
+            }
+        }
+        a.rhs[i] = rhs;
+    }
+    (void)ndist;
+    __syncthreads();
+    double *out = a.vals + base;
+    for (int q = threadIdx.x; q < top - base; q += kAsmBlock) out[q] = stage[q];
+}
+
 template <int DIM, int MAXF>
 void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
-    const int B = 128;
-    fv_note_launch(), k_assemble<DIM, MAXF><<<(unsigned)((a.n + B - 1) / B), B, 0, st>>>(a);
+    const int B = kAsmBlock;
+    const unsigned G = (unsigned)((a.n + B - 1) / B);
+    if constexpr (MAXF <= 8) {
+        const size_t smem = sizeof(double) * B * (MAXF + 1);
+        fv_note_launch(), k_assemble_reg<DIM, MAXF><<<G, B, smem, st>>>(a);
+    } else {
+        fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
+    }
 }
 
 }  // namespace
@@ -227,6 +387,7 @@ extern "C" const char *fv_status_string(fv_status s) {
     case FV_ERR_NOT_SYMMETRIC: return "FV_ERR_NOT_SYMMETRIC";
     case FV_ERR_CUDA: return "FV_ERR_CUDA";
     case FV_ERR_UNSUPPORTED: return "FV_ERR_UNSUPPORTED";
+    case FV_ERR_COMM: return "FV_ERR_COMM";
     }
     return "FV_ERR_UNKNOWN";
 }
@@ -259,7 +420,7 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     std::vector<int32_t> cnt((size_t)N + 1, 0);
     for (int64_t f = 0; f < F; ++f) {
         int32_t o = d->face_owner[f], nb = d->face_neighbor[f];
-        if (o < 0 || o >= N || nb < -1 || nb >= N) return FV_ERR_INVALID;
+        if (o < 0 || o >= N || nb < -1 || nb >= N || nb == o) return FV_ERR_INVALID;
         if ((nb < 0) != (f >= fb0)) return FV_ERR_INVALID;
         cnt[o + 1]++;
         if (nb >= 0) cnt[nb + 1]++;

@@ -530,6 +530,7 @@ fv_status fv_precond_check_error(fv_precond *P, cudaStream_t st) {
 }
 
 int *fv_precond_err_ptr(fv_precond *P) { return P->err; }
+int64_t fv_precond_rows(const fv_precond *P) { return P->n; }
 
 namespace {
 __global__ void k_to_f32(int64_t n, const double *__restrict__ a, float *__restrict__ b) {

@@ -14,10 +14,10 @@ LIB_PATH = _PKG / "libfvb200.so"
 
 FV_STATUS = {
     0: "FV_OK", 1: "FV_ERR_ALLOC", 2: "FV_ERR_INVALID", 3: "FV_ERR_SINGULAR_PIVOT", 4: "FV_ERR_BREAKDOWN",
-    5: "FV_ERR_TIMEOUT", 6: "FV_ERR_NOT_SYMMETRIC", 7: "FV_ERR_CUDA", 8: "FV_ERR_UNSUPPORTED",
+    5: "FV_ERR_TIMEOUT", 6: "FV_ERR_NOT_SYMMETRIC", 7: "FV_ERR_CUDA", 8: "FV_ERR_UNSUPPORTED", 9: "FV_ERR_COMM",
 }
 FV_OK, FV_ERR_ALLOC, FV_ERR_INVALID, FV_ERR_SINGULAR_PIVOT, FV_ERR_BREAKDOWN = 0, 1, 2, 3, 4
-FV_ERR_TIMEOUT, FV_ERR_NOT_SYMMETRIC, FV_ERR_CUDA, FV_ERR_UNSUPPORTED = 5, 6, 7, 8
+FV_ERR_TIMEOUT, FV_ERR_NOT_SYMMETRIC, FV_ERR_CUDA, FV_ERR_UNSUPPORTED, FV_ERR_COMM = 5, 6, 7, 8, 9
 
 
 class FvError(RuntimeError):
@@ -90,6 +90,15 @@ class BatchInfo(C.Structure):
                 ("outer_steps", ip), ("final_residual", dp), ("status", ip), ("fp64_fallback", ip)]
 
 
+# fv_comm: the collect / reduce_add callbacks of a distributed solve
+COLLECT_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
+
+
+class FvComm(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("collect", COLLECT_FN), ("reduce_add", REDUCE_FN)]
+
+
 vp = C.c_void_p
 _SIGS = {
     # host mesh
@@ -126,6 +135,13 @@ _SIGS = {
     "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_bicgstab": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_destroy": [vp],
+    "fv_csr_square_block": [vp, vp, P(vp)],
+    "fv_dist_create": [vp, i64, ip, i64, P(FvComm), P(vp)],
+    "fv_dist_destroy": [vp],
+    "fv_dist_spmv": [vp, vp, vp, vp],
+    "fv_dist_dot": [vp, vp, vp, dp, vp],
+    "fv_dist_cg": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
+    "fv_dist_bicgstab": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
 }
 
 _lib = None

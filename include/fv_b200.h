@@ -50,7 +50,8 @@ typedef enum fv_status {
     FV_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
     FV_ERR_NOT_SYMMETRIC = 6,  /* IC on a matrix failing |a_ij-a_ji|<1e-14 (incomplete_cholesky.rs:153) */
     FV_ERR_CUDA = 7,           /* a CUDA runtime call failed */
-    FV_ERR_UNSUPPORTED = 8     /* feature outside the implemented scope (e.g. level>0) */
+    FV_ERR_UNSUPPORTED = 8,    /* feature outside the implemented scope (e.g. level>0) */
+    FV_ERR_COMM = 9            /* a communicator callback (fv_comm) reported failure */
 } fv_status;
 
 /* ------------------------------------------------------------------------ */
@@ -299,6 +300,51 @@ fv_status fv_batch_destroy(fv_batch *B);
 #define FV_NOALLOC_MAX_ITERATIONS 4093
 fv_status fv_cg_noalloc(const fv_csr *A, fv_precond *P, const double *b, double *x,
                         fv_solver_options opt, fv_solver_info *info, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* One rank of a problem split over several GPUs (the reference's MPI design,
+ * core/communicator.rs, core/mesh/decompose.rs).  The rank's matrix A has
+ * n_own rows (its cells) and n_own + n_ghost columns: its own cells first,
+ * then the ghost cells owned by other ranks (dmatrix.rs:38-50 over the local
+ * cell_to_cell).  The two communication steps are supplied by the caller. */
+typedef struct fv_comm {
+    void *ctx;
+    /* Communicator::collect (core/communicator.rs:226-266): send[0..n_send)
+     * holds this rank's values that other ranks need, packed in the order of
+     * the send_idx given to fv_dist_create; fill ghost[0..n_ghost) with the
+     * ghost values in ghost-column order.  Device pointers; order the transfer
+     * on `stream` (or finish it before returning).  Return 0 on success.
+     * NULL means a single rank with no ghosts. */
+    int (*collect)(void *ctx, const double *send, double *ghost, void *stream);
+    /* Communicator::reduce_add (core/communicator.rs:282-290): replace
+     * buf[0..count) (device) by its sum over all ranks, ordered on `stream`.
+     * Return 0 on success.  NULL means a single rank. */
+    int (*reduce_add)(void *ctx, double *buf, int count, void *stream);
+} fv_comm;
+
+typedef struct fv_dist fv_dist;
+
+/* DistributedMatrix::square_block (dmatrix.rs:214-229): the rows of A with
+ * the columns >= nrows (ghost columns) dropped. */
+fv_status fv_csr_square_block(const fv_csr *A, void *stream, fv_csr **out);
+/* A: this rank's matrix (n_own rows, n_own + n_ghost columns; kept, not
+ * copied).  send_idx (host, n_send entries): the owned rows whose values the
+ * other ranks need, in the order collect() expects them.  comm is copied. */
+fv_status fv_dist_create(const fv_csr *A, int64_t n_ghost, const int32_t *send_idx, int64_t n_send,
+                         const fv_comm *comm, fv_dist **out);
+fv_status fv_dist_destroy(fv_dist *D);
+/* y[0..n_own) = A x after collect() refreshed x[n_own .. n_own + n_ghost). */
+fv_status fv_dist_spmv(fv_dist *D, double *x, double *y, void *stream);
+/* Global dot product (local sum + reduce_add), returned on the host. */
+fv_status fv_dist_dot(fv_dist *D, const double *x, const double *y, double *result, void *stream);
+/* conjugate_gradient / bi_conjugate_gradient_stab on every rank together
+ * (each rank calls with its own D, P, b and x; all ranks take the same number
+ * of iterations).  P: this rank's preconditioner built on fv_csr_square_block(A)
+ * (block Jacobi across ranks), or NULL.  b, x: n_own entries (device). */
+fv_status fv_dist_cg(fv_dist *D, fv_precond *P, const double *b, double *x,
+                     fv_solver_options opt, fv_solver_info *info, void *stream);
+fv_status fv_dist_bicgstab(fv_dist *D, fv_precond *P, const double *b, double *x,
+                           fv_solver_options opt, fv_solver_info *info, void *stream);
 
 /* Human-readable name of a status. */
 const char *fv_status_string(fv_status s);
