@@ -137,6 +137,16 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def sweep_schedule(P):
+    """Which sweep schedule the preconditioner uses, with its box-tile plan."""
+    act, st = P.schedule()
+    if act != 2:
+        return {"kind": "level chunks"}
+    return {"kind": "box tiles", "box_edge_cells": float(st[0]), "boxes": int(st[1]),
+            "lane_use": [round(float(st[2]), 3), round(float(st[3]), 3)],
+            "ring_share": [round(float(st[4]), 3), round(float(st[5]), 3)]}
+
+
 def time_kernel(torch, fn, reps, stream):
     """Average device time of fn() over reps launches, CUDA events on `stream`."""
     for _ in range(2):
@@ -193,10 +203,16 @@ def gpu_arm(args, rank, world, local_rank):
         single = BatchCG(A, [0, N], 2048)
 
     # one step: value assembly (new rhs), refactorisation, solve from x0 = 0
-    def step_b():
+    def step_b(marks=None):
         nonlocal b
         _, b = fv.assemble(eq, bc, mesh, lhs=A)
+        if marks is not None:
+            marks.append(torch.cuda.Event(enable_timing=True))
+            marks[-1].record(stream)
         P.refactor()
+        if marks is not None:
+            marks.append(torch.cuda.Event(enable_timing=True))
+            marks[-1].record(stream)
         x.data.zero_()
         if mixed:
             o = single.solve(P, b, x, precision="mixed", outer_tolerance=1e-10, inner_relative_tolerance=1e-2,
@@ -219,16 +235,22 @@ def gpu_arm(args, rank, world, local_rank):
     lat = []
     iters = []
     e0.record(stream)
+    phases = []
     for _ in range(args.steps):
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(stream)
-        info = step_b()
+        marks = []
+        info = step_b(marks)
         s1.record(stream)
         iters.append(info.iterations)
         lat.append((s0, s1))
+        phases.append((s0, marks, s1))
     e1.record(stream)
     torch.cuda.synchronize()
+    # assembly / refactorisation / solve of every step (ms)
+    phase_ms = [[round(s0.elapsed_time(m[0]), 2), round(m[0].elapsed_time(m[1]), 2), round(m[1].elapsed_time(s1), 2)]
+                for s0, m, s1 in phases]
     launches = lib().fv_launch_count() - L0
     clocks = clk.stop()
     elapsed = e0.elapsed_time(e1) / 1e3
@@ -331,9 +353,9 @@ def gpu_arm(args, rank, world, local_rank):
     res = dict(
         elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
         e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
-        e2e_lat_ms=e2e_lat_ms, e2e_clocks=e2e_clocks,
+        e2e_lat_ms=e2e_lat_ms, e2e_clocks=e2e_clocks, phase_ms=phase_ms,
         kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
-        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A, mixed_info=mixed_info,
+        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A, mixed_info=mixed_info, schedule=sweep_schedule(P),
     )
     return res
 
@@ -558,7 +580,7 @@ def batch_arm(args, rank, world, local_rank):
     return dict(elapsed=elapsed, out=out, launches=launches, clocks=clocks, t_mesh=t_mesh, N=mb.n_cells,
                 t_fp64_batch=t_fp64_batch, it64_max=int(np.max(out64["iterations"])),
                 nnz=A.shape()[2], tile=tile, tile_times=tile_times, errs=errs, plain_solves=plain_solves,
-                sample=len(sample), sides=sides, levels=P.levels()[2:])
+                sample=len(sample), sides=sides, levels=P.levels()[2:], schedule=sweep_schedule(P))
 
 
 BATCH_OUTER_TOL = 1e-10
@@ -669,6 +691,7 @@ def main_batch(args, rank, world, local_rank):
         "outer_steps_max": int(np.max(out["outer_steps"])), "inner_iterations_max": int(np.max(its)),
         "fp64_fallback_problems": int(np.sum(out["fp64_fallback"])),
         "launched_iterations": int(out["launched_iterations"]), "levels_fwd_bwd": list(res["levels"]),
+        "sweep_schedule": res["schedule"],
         "autotune_tile_s": {str(k): round(v, 4) for k, v in res["tile_times"].items()},
         "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "mesh_build_s": round(res["t_mesh"], 2),
     }
@@ -733,10 +756,11 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_of(args, wl, N, res["nnz"]),
         "dof_iters_per_s": round(N * it_mean * solves / res["elapsed"], 1),
-        "iterations": res["iters"], "p50_ms": round(float(np.percentile(lat, 50)), 3),
+        "iterations": res["iters"], "step_phase_ms": res["phase_ms"],
+        "p50_ms": round(float(np.percentile(lat, 50)), 3),
         "p99_ms": round(float(np.percentile(lat, 99)), 3), "true_rel_residual": res["relres"],
         "roofline": res["roofline"], "kernels": res["kernels"], "time_share": res["share"],
-        "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]),
+        "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]), "sweep_schedule": res["schedule"],
         "cpu_baseline": cpu,
         "e2e": {"value": round(solves / res["e2e_elapsed"], 6), "unit": "solves/s",
                 "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"],

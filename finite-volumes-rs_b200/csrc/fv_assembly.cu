@@ -69,6 +69,7 @@ __global__ void k_row_fill(int64_t n, const int32_t *__restrict__ cf_ptr, const 
 struct AssembleArgs {
     int64_t n, fb0;
     const int32_t *cf_ptr, *cf_face, *cf_other;
+    const int2 *cf_pad;
     const double4 *cell, *bfc;
     const double *area, *kappa, *flux, *src, *bndi, *bnde;
     double c_lap, c_conv, c_src;
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
 constexpr int kAsmBlock = 128;
 
 template <int DIM, int MAXF>
-__global__ void __launch_bounds__(kAsmBlock) k_assemble_reg(AssembleArgs a) {
+__global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
     extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
     const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
     const int64_t i = b0 + threadIdx.x;
@@ -210,45 +211,42 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble_reg(AssembleArgs a) {
     const int base = a.row_ptr[b0];
     const int top = a.row_ptr[bend];
     const bool live = i < a.n;
-    int s = 0, deg = 0;
-    if (live) {
-        s = a.cf_ptr[i];
-        deg = a.cf_ptr[i + 1] - s;
-    }
+    // the cell's incidences, padded to MAXF slots: no dependent load of cf_ptr
     int fe[MAXF], jj[MAXF];
 #pragma unroll
-    for (int k = 0; k < MAXF; ++k) {
-        fe[k] = 0;
-        jj[k] = -1;
-        if (k < deg) {
-            fe[k] = a.cf_face[s + k];
-            jj[k] = a.cf_other[s + k];
-        }
+    for (int k = 0; k < MAXF; k += 2) {
+        int4 q = make_int4(0, -2, 0, -2);
+        if (live) q = *reinterpret_cast<const int4 *>(&a.cf_pad[i * MAXF + k]);
+        fe[k] = q.x;
+        jj[k] = q.y;
+        fe[k + 1] = q.z;
+        jj[k + 1] = q.w;
     }
+    int deg = 0;
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k) deg += jj[k] != -2 ? 1 : 0;
+#pragma unroll
+    for (int k = 0; k < MAXF; ++k)
+        if (jj[k] == -2) jj[k] = -1;
     double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
     double srci = 0.0;
     if (live) {
         ci4 = a.cell[i];
         if (a.c_src != 0.0) srci = a.src[i];
     }
-    double4 oc[MAXF];
-    double ar[MAXF], kp[MAXF], fl[MAXF], bi[MAXF], be[MAXF];
+    double3 oc[MAXF];
+    double ar[MAXF], kp[MAXF], fl[MAXF];
 #pragma unroll
     for (int k = 0; k < MAXF; ++k) {
-        oc[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-        ar[k] = kp[k] = fl[k] = bi[k] = be[k] = 0.0;
+        oc[k] = make_double3(0.0, 0.0, 0.0);
+        ar[k] = kp[k] = fl[k] = 0.0;
         if (k < deg) {
             const int f = fe[k] & 0x7fffffff;
             ar[k] = a.area[f];
             if (a.c_lap != 0.0) kp[k] = a.kappa[f];
             if (a.c_conv != 0.0) fl[k] = a.flux[f];
-            if (jj[k] >= 0) {
-                oc[k] = a.cell[jj[k]];
-            } else {
-                oc[k] = a.bfc[f - a.fb0];
-                bi[k] = a.bndi[f - a.fb0];
-                be[k] = a.bnde[f - a.fb0];
-            }
+            const double4 o = jj[k] >= 0 ? a.cell[jj[k]] : a.bfc[f - a.fb0];
+            oc[k] = make_double3(o.x, o.y, o.z);
         }
     }
     // distinct neighbours: the first incidence of each other cell carries its slot
@@ -302,9 +300,11 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble_reg(AssembleArgs a) {
             lj = lj * A;
             const double ra = 0.0 * A;
             if (jj[k] < 0) {
+                const int fb = (fe[k] & 0x7fffffff) - (int)a.fb0;
+                const double bi = a.bndi[fb], be = a.bnde[fb];
                 diag += li;
-                diag += lj * bi[k];
-                rhs += ra - lj * be[k];
+                diag += lj * bi;
+                rhs += ra - lj * be;
             } else {
                 // the value of this neighbour's slot sits in acc[] of its first incidence
 #pragma unroll
@@ -352,7 +352,10 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
-        fv_note_launch(), k_assemble_reg<DIM, MAXF><<<G, B, smem, st>>>(a);
+        if (a.cf_pad)
+            fv_note_launch(), k_assemble_reg<DIM, MAXF><<<G, B, smem, st>>>(a);
+        else
+            fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
     } else {
         fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
     }
@@ -401,6 +404,7 @@ extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
     cudaFree(m->cf_ptr);
     cudaFree(m->cf_face);
     cudaFree(m->cf_other);
+    cudaFree(m->cf_pad);
     cudaFree(m->row_ptr);
     cudaFree(m->cols);
     delete m;
@@ -442,6 +446,11 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     int maxf = 0;
     for (int64_t c = 0; c < N; ++c) maxf = std::max(maxf, cnt[c + 1] - cnt[c]);
     if (maxf > 16) return FV_ERR_UNSUPPORTED;
+    const int padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
+    std::vector<int2> pad((size_t)(padf ? N * padf : 1), make_int2(0, -2));
+    if (padf)
+        for (int64_t c = 0; c < N; ++c)
+            for (int32_t k = cnt[c]; k < cnt[c + 1]; ++k) pad[(size_t)(c * padf + (k - cnt[c]))] = make_int2(cff[k], cfo[k]);
     std::vector<double4> cell((size_t)N);
     for (int64_t c = 0; c < N; ++c) {
         const double *p = d->cell_center + c * dim;
@@ -461,6 +470,7 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     m->n_faces = F;
     m->n_bfaces = Fb;
     m->maxf = maxf;
+    m->padf = padf;
     cudaStream_t st = fv_stream(stream);
     cudaError_t e = cudaSuccess;
     e = cudaMalloc(&m->face_cells, sizeof(int2) * F);
@@ -482,6 +492,9 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
         e = cudaMemcpyAsync(m->cf_face, cff.data(), sizeof(int32_t) * ncf, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && ncf)
         e = cudaMemcpyAsync(m->cf_other, cfo.data(), sizeof(int32_t) * ncf, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && padf) e = cudaMalloc(&m->cf_pad, sizeof(int2) * N * padf);
+    if (e == cudaSuccess && padf)
+        e = cudaMemcpyAsync(m->cf_pad, pad.data(), sizeof(int2) * N * padf, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging vectors go out of scope
     if (e != cudaSuccess) {
         fv_internal_set_cuda_error(e, "fv_mesh_upload");
@@ -568,6 +581,7 @@ extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const f
     args.cf_ptr = m->cf_ptr;
     args.cf_face = m->cf_face;
     args.cf_other = m->cf_other;
+    args.cf_pad = m->cf_pad;
     args.cell = m->cell;
     args.bfc = m->bface_center;
     args.area = m->face_area;

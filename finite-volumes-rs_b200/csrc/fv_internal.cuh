@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fv_b200.h"
 
 #define FV_CUDA_TRY(expr)                                  \
@@ -49,6 +51,8 @@ struct fv_mesh {
     int32_t *cf_ptr = nullptr;         // cell -> faces CSR, faces ascending
     int32_t *cf_face = nullptr;        // face id, bit 31 set when the cell is the face's neighbour
     int32_t *cf_other = nullptr;       // the other cell, -1 for boundary faces
+    int2 *cf_pad = nullptr;            // (cf_face, cf_other) at cell * padf + slot, padded with (0, -2)
+    int padf = 0;                      // 4 or 8 (0: no padded copy, cells with more than 8 faces)
     // CSR pattern of cell_to_cell (built on the first assemble)
     int32_t *row_ptr = nullptr;
     int32_t *cols = nullptr;
@@ -56,6 +60,23 @@ struct fv_mesh {
 };
 
 struct fv_symbolic;  // triangular split + level schedules of a pattern (fv_precond.cu)
+
+// Box tiling of one sweep direction (fv_tiles.cu): boxes in dispatch order,
+// each a run of steps (rows of one level, at most 32); trow lists the rows in
+// that order; dsrc[k] (aligned with the swept side's entries) is the column j
+// when the dependency is read from the vector, or -(slot + 1) when it comes
+// from the warp's shared-memory ring of its last `ring` steps.
+struct fv_tile_plan {
+    std::vector<int32_t> box_step, sptr, trow, dsrc;
+    int32_t nb = 0, nsteps = 0;
+    double lane_use = 0.0, ring_share = 0.0, edge = 0.0;
+    double est = 0.0;  // estimated critical path of both sweeps / that of the level schedule
+};
+bool fv_build_tile_plans(int64_t n, int dim, const double *cell, const int32_t *lp, const int32_t *lc,
+                         const int32_t *up, const int32_t *uc, const int32_t *fwd_level, const int32_t *bwd_level,
+                         const int32_t *fwd_order, const int32_t *bwd_order, int ring, fv_tile_plan &fwd,
+                         fv_tile_plan &bwd);
+#define FV_TILE_RING 8
 
 // Rows a sweep may skip: row i is skipped when done[group[i] * stride] != 0
 // (rows of the problems of a batch that have converged).

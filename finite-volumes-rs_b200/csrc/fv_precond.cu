@@ -39,6 +39,14 @@ struct fv_symbolic {
     int32_t max_lower = 0, max_upper = 0;        // longest strict-lower / strict-upper row
     bool symmetric_pattern = false;
     std::vector<int32_t> h_fwd_level, h_bwd_level;
+    // box tiling of the two sweeps ([0] forward over L, [1] backward over U);
+    // absent (tiled = false) for matrices without mesh geometry or without an
+    // acyclic box order
+    bool tiled = false;
+    int32_t t_nb[2] = {0, 0};
+    int32_t *t_box_step[2] = {nullptr, nullptr}, *t_sptr[2] = {nullptr, nullptr};
+    int32_t *t_trow[2] = {nullptr, nullptr}, *t_dsrc[2] = {nullptr, nullptr};
+    double t_lane_use[2] = {0, 0}, t_ring_share[2] = {0, 0}, t_edge = 0;
 };
 
 void fv_symbolic_free(fv_symbolic *s) {
@@ -50,6 +58,12 @@ void fv_symbolic_free(fv_symbolic *s) {
     cudaFree(s->fwd_order);
     cudaFree(s->bwd_order);
     cudaFree(s->l_tpos);
+    for (int d = 0; d < 2; ++d) {
+        cudaFree(s->t_box_step[d]);
+        cudaFree(s->t_sptr[d]);
+        cudaFree(s->t_trow[d]);
+        cudaFree(s->t_dsrc[d]);
+    }
     delete s;
 }
 
@@ -62,6 +76,7 @@ struct fv_precond {
     double *tmp = nullptr;        // forward-sweep output, kept at sentinel between applies
     unsigned *done = nullptr;     // factorisation flags
     unsigned epoch = 0;
+    int schedule = 0;             // 0: box tiles when planned, else level chunks; 1: level chunks
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
@@ -176,6 +191,29 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     up_load(&s->fwd_order, fo, (size_t)n);
     up_load(&s->bwd_order, bo, (size_t)n);
     if (sym) up_load(&s->l_tpos, tpos, (size_t)nl);
+    // box tiles when the matrix was assembled on a mesh (cell centres known)
+    if (e == cudaSuccess && A->mesh && A->mesh->n_cells == n && n > 0) {
+        std::vector<double4> cells((size_t)n);
+        e = cudaMemcpyAsync(cells.data(), A->mesh->cell, sizeof(double4) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        fv_tile_plan tp[2];
+        if (e == cudaSuccess &&
+            fv_build_tile_plans(n, A->mesh->dim, (const double *)cells.data(), lp.data(), lc.data(), up.data(),
+                                uc.data(), s->h_fwd_level.data(), s->h_bwd_level.data(), fo.data(), bo.data(),
+                                FV_TILE_RING, tp[0], tp[1])) {
+            for (int d = 0; d < 2; ++d) {
+                up_load(&s->t_box_step[d], tp[d].box_step, tp[d].box_step.size());
+                up_load(&s->t_sptr[d], tp[d].sptr, tp[d].sptr.size());
+                up_load(&s->t_trow[d], tp[d].trow, tp[d].trow.size());
+                up_load(&s->t_dsrc[d], tp[d].dsrc, tp[d].dsrc.size());
+                s->t_nb[d] = tp[d].nb;
+                s->t_lane_use[d] = tp[d].lane_use;
+                s->t_ring_share[d] = tp[d].ring_share;
+            }
+            s->t_edge = tp[0].edge;
+            s->tiled = e == cudaSuccess;
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         fv_internal_set_cuda_error(e, "symbolic upload");
@@ -465,6 +503,112 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
     leave(&ctrl[0], &ctrl[1]);
 }
 
+// The same sweep over box tiles (fv_tiles.cu): one warp takes a box (tickets
+// in the boxes' dispatch order) and runs its steps in level order.  A lane's
+// dependency comes either from the warp's shared-memory ring (a row of one of
+// the box's last FV_TILE_RING steps) or from the vector (polled like k_sweep).
+// The next step's row data and first polls are issued before the current step
+// waits, so a chain of rows inside a box costs shared-memory latency per level
+// instead of an L2 round trip.
+template <typename T, int MAXL>
+struct TileRow {
+    int i;  // row, or -1 for an idle lane
+    int m;
+    int ds[MAXL];
+    T v[MAXL], xv[MAXL];
+    unsigned pending;
+    T s, d;
+};
+
+template <typename T, bool UNIT, int MAXL>
+__device__ __forceinline__ void tile_load(TileRow<T, MAXL> &R, int step, const int32_t *__restrict__ sptr,
+                                          const int32_t *__restrict__ trow, const int32_t *__restrict__ ptr,
+                                          const int32_t *__restrict__ dsrc, const T *__restrict__ val,
+                                          const T *__restrict__ dinv, const T *rhs, const T *x,
+                                          const fv_row_skip &rs) {
+    const int lane = threadIdx.x & 31;
+    const int r0 = __ldg(&sptr[step]);
+    R.i = -1;
+    R.m = 0;
+    R.pending = 0;
+    if (lane >= __ldg(&sptr[step + 1]) - r0) return;
+    const int i = __ldg(&trow[r0 + lane]);
+    if (rs.group && rs.done[(int64_t)__ldg(&rs.group[i]) * rs.stride]) return;
+    R.i = i;
+    const int k0 = __ldg(&ptr[i]);
+    R.m = __ldg(&ptr[i + 1]) - k0;
+#pragma unroll
+    for (int q = 0; q < MAXL; ++q)
+        if (q < R.m) {
+            R.ds[q] = __ldg(&dsrc[k0 + q]);
+            R.v[q] = __ldg(&val[k0 + q]);
+        }
+    R.s = rhs[i];
+    R.d = UNIT ? T(1) : __ldg(&dinv[i]);
+#pragma unroll
+    for (int q = 0; q < MAXL; ++q)
+        if (q < R.m && R.ds[q] >= 0 && !fv_slot_ready(&x[R.ds[q]], R.xv[q])) R.pending |= 1u << q;
+}
+
+template <typename T, bool UNIT, int MAXL>
+__global__ void __launch_bounds__(256) k_sweep_tiled(int64_t nb, const int32_t *__restrict__ box_step,
+                                                     const int32_t *__restrict__ sptr,
+                                                     const int32_t *__restrict__ trow,
+                                                     const int32_t *__restrict__ ptr,
+                                                     const int32_t *__restrict__ dsrc, const T *__restrict__ val,
+                                                     const T *__restrict__ dinv, const T *rhs, T *x, T *rhs_reset,
+                                                     T *next_reset, unsigned *ctrl, int *err, const int *skip,
+                                                     fv_row_skip rs) {
+    __shared__ T ring_all[8][FV_TILE_RING * 32];
+    if (skip && *(volatile const int *)skip) return;
+    T *ring = ring_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    int64_t b;
+    while (take_chunk(&ctrl[0], nb, b)) {
+        const int s0 = __ldg(&box_step[b]), s1 = __ldg(&box_step[b + 1]);
+        TileRow<T, MAXL> cur, nxt;
+        nxt.i = -1;
+        nxt.m = 0;
+        nxt.pending = 0;
+        tile_load<T, UNIT, MAXL>(cur, s0, sptr, trow, ptr, dsrc, val, dinv, rhs, x, rs);
+        for (int st = s0; st < s1; ++st) {
+            if (st + 1 < s1) tile_load<T, UNIT, MAXL>(nxt, st + 1, sptr, trow, ptr, dsrc, val, dinv, rhs, x, rs);
+            if (cur.i >= 0) {
+                if (cur.pending) {
+                    const unsigned long long t0 = fv_globaltimer();
+                    for (unsigned it = 1; cur.pending; ++it) {
+#pragma unroll
+                        for (int q = 0; q < MAXL; ++q)
+                            if ((cur.pending >> q) & 1u)
+                                if (fv_slot_ready(&x[cur.ds[q]], cur.xv[q])) cur.pending &= ~(1u << q);
+                        if (cur.pending && (it & 255u) == 0) {
+                            if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
+                                if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+#pragma unroll
+                                for (int q = 0; q < MAXL; ++q)
+                                    if ((cur.pending >> q) & 1u) cur.xv[q] = T(NAN);
+                                cur.pending = 0;
+                            }
+                        }
+                    }
+                }
+                T s = cur.s;
+#pragma unroll
+                for (int q = 0; q < MAXL; ++q)
+                    if (q < cur.m) s = s - cur.v[q] * (cur.ds[q] < 0 ? ring[-cur.ds[q] - 1] : cur.xv[q]);
+                const T r = UNIT ? s : cur.d * s;
+                ring[((st - s0) % FV_TILE_RING) * 32 + lane] = r;
+                fv_publish(&x[cur.i], r);
+                if (rhs_reset) fv_reset_slot(&rhs_reset[cur.i]);
+                if (next_reset) fv_reset_slot(&next_reset[cur.i]);
+            }
+            __syncwarp();
+            cur = nxt;
+        }
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
 template <typename T, bool UNIT>
 static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
                          const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
@@ -486,6 +630,28 @@ static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int3
                                                                   next_reset, ctrl, err, skip, rs);
 }
 
+// Tiled sweep of direction d (0 forward over L, 1 backward over U).
+template <typename T, bool UNIT>
+static void launch_tiled(const fv_symbolic *s, int d, int maxl, cudaStream_t st, const int32_t *ptr, const T *val,
+                         const T *dinv, const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl, int *err,
+                         const int *skip, fv_row_skip rs) {
+    const int64_t nb = s->t_nb[d];
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>((nb + 7) / 8, 148 * 4));
+    if (maxl <= 4)
+        fv_note_launch(), k_sweep_tiled<T, UNIT, 4><<<G, 256, 0, st>>>(
+                              nb, s->t_box_step[d], s->t_sptr[d], s->t_trow[d], ptr, s->t_dsrc[d], val, dinv, rhs,
+                              x, rhs_reset, next_reset, ctrl, err, skip, rs);
+    else
+        fv_note_launch(), k_sweep_tiled<T, UNIT, 8><<<G, 256, 0, st>>>(
+                              nb, s->t_box_step[d], s->t_sptr[d], s->t_trow[d], ptr, s->t_dsrc[d], val, dinv, rhs,
+                              x, rhs_reset, next_reset, ctrl, err, skip, rs);
+}
+
+static bool use_tiles(const fv_precond *P) {
+    const fv_symbolic *s = P->sym;
+    return P->schedule == 0 && s->tiled && s->max_lower <= 8 && s->max_upper <= 8;
+}
+
 static int sweep_grid(int64_t n) {
     int64_t warps = (n + 31) / 32;
     int64_t blocks = (warps + 7) / 8;
@@ -503,6 +669,19 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const int64_t n = P->n;
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
+    if (use_tiles(P)) {
+        if (P->kind == 2)
+            launch_tiled<double, true>(s, 0, s->max_lower, st, s->l_ptr, P->l_val, nullptr, r, P->tmp, nullptr, z,
+                                       P->ctrl, P->err, skip, rs);
+        else
+            launch_tiled<double, false>(s, 0, s->max_lower, st, s->l_ptr, P->l_val, P->dinv, r, P->tmp, nullptr, z,
+                                        P->ctrl, P->err, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_tiled<double, false>(s, 1, s->max_upper, st, s->u_ptr, P->u_val, P->dinv, P->tmp, z, P->tmp, nullptr,
+                                    P->ctrl + 2, P->err, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (P->kind == 2)
         launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -566,6 +745,19 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
     if (!P->l32) return FV_ERR_INVALID;
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
+    if (use_tiles(P)) {
+        if (P->kind == 2)
+            launch_tiled<float, true>(s, 0, s->max_lower, st, s->l_ptr, P->l32, nullptr, r, P->tmp32, nullptr, z,
+                                      P->ctrl, P->err, skip, rs);
+        else
+            launch_tiled<float, false>(s, 0, s->max_lower, st, s->l_ptr, P->l32, P->dinv32, r, P->tmp32, nullptr, z,
+                                       P->ctrl, P->err, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_tiled<float, false>(s, 1, s->max_upper, st, s->u_ptr, P->u32, P->dinv32, P->tmp32, z, P->tmp32,
+                                   nullptr, P->ctrl + 2, P->err, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (P->kind == 2)
         launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -576,6 +768,23 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
     launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
                                P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs);
     FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
+    if (!P || request < -1 || request > 2) return FV_ERR_INVALID;
+    const fv_symbolic *s = P->sym;
+    if (request == 2 && !(s->tiled && s->max_lower <= 8 && s->max_upper <= 8)) return FV_ERR_UNSUPPORTED;
+    if (request >= 0) P->schedule = request == 1 ? 1 : 0;
+    if (active) *active = use_tiles(P) ? 2 : 1;
+    if (stats) {
+        stats[0] = s->t_edge;
+        stats[1] = s->t_nb[0];
+        stats[2] = s->t_lane_use[0];
+        stats[3] = s->t_lane_use[1];
+        stats[4] = s->t_ring_share[0];
+        stats[5] = s->t_ring_share[1];
+    }
     return FV_OK;
 }
 

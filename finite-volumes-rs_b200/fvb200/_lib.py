@@ -126,6 +126,8 @@ _SIGS = {
     "fv_precond_export": [vp, P(i64), ip, ip, dp, ip, vp],
     "fv_precond_levels": [vp, ip, ip, ip, ip, vp],
     "fv_precond_destroy": [vp],
+    "fv_precond_schedule": [vp, C.c_int32, P(C.c_int32), dp],
+    "fv_tile_plan_host": [i64, C.c_int32, dp, ip, ip, C.c_int32, P(i64), ip, ip, ip, ip, dp],
     "fv_cg": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
     "fv_bicgstab": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
     "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],

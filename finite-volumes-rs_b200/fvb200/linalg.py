@@ -214,6 +214,17 @@ class Preconditioner:
               "levels")
         return fl, bl, nf.value, nb.value
 
+    def schedule(self, request: int = -1):
+        """Sweep schedule: request -1 = query, 0 = automatic (box tiles when
+        planned), 1 = level chunks, 2 = box tiles.  Returns (active, stats)
+        with active 1 (level chunks) or 2 (box tiles) and stats = (box edge in
+        cell sizes, boxes, lane use fwd/bwd, ring share fwd/bwd)."""
+        act = C.c_int32()
+        st = np.zeros(6)
+        check(lib().fv_precond_schedule(self.handle, int(request), C.byref(act),
+                                        st.ctypes.data_as(C.POINTER(C.c_double))), "schedule")
+        return act.value, st
+
     def refactor(self, stream=None):
         """Value-only refactorisation after the matrix values changed."""
         check(lib().fv_precond_refactor(self.handle, stream_handle(stream)), "refactor")

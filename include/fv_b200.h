@@ -213,7 +213,28 @@ fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr,
 /* Level schedules: level of every row in the forward (lower) and backward (upper) DAG. */
 fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,
                             int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream);
+/* Sweep schedule of P.  request: -1 query only; 0 automatic (box tiles when
+ * the matrix was assembled on a mesh whose box order exists, else level
+ * chunks); 1 level chunks; 2 box tiles (FV_ERR_UNSUPPORTED when there is no
+ * tiling).  *active receives 1 (level chunks) or 2 (box tiles).  stats
+ * (optional, 6 doubles): box edge in mean cell sizes, number of boxes, lane
+ * use of the forward / backward steps, share of dependencies read from
+ * shared memory forward / backward.  Both schedules give the same bits. */
+fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats);
 fv_status fv_precond_destroy(fv_precond *P);
+/* The box-tile plan fv_ic0_factor / fv_ilu0_factor make for a matrix
+ * assembled on a mesh, computed from host arrays (cell: n x 4 doubles, the
+ * centre in the first dim entries): direction 0 = forward over the strict
+ * lower part, 1 = backward over the strict upper part.  sizes receives
+ * (boxes, steps, swept-side entries); pass NULL arrays to query sizes.
+ * box_step: boxes+1 entries; sptr: steps+1; trow: n; dsrc: swept-side
+ * entries in row order (column j, or -(ring slot + 1)); stats (4 doubles):
+ * box edge in mean cell sizes, lane use, share of ring reads, estimated
+ * critical path of both sweeps relative to the level schedule.  FV_ERR_UNSUPPORTED when
+ * no box order exists (the sweeps then use level chunks). */
+fv_status fv_tile_plan_host(int64_t n, int32_t dim, const double *cell, const int32_t *row_ptr,
+                            const int32_t *cols, int32_t direction, int64_t *sizes, int32_t *box_step,
+                            int32_t *sptr, int32_t *trow, int32_t *dsrc, double *stats);
 
 /* conjugate_gradient / bi_conjugate_gradient_stab.  x is the initial guess on
  * input and the solution on output (device vectors).  P may be NULL (identity). */
