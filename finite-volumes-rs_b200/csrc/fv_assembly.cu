@@ -364,7 +364,26 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
 }  // namespace
 
 #include <atomic>
+#include <mutex>
 static std::atomic<unsigned long long> g_launches{0};
+
+cudaError_t fv_malloc_async_raw(void **p, size_t bytes, cudaStream_t st) {
+    static std::atomic<bool> configured[64];
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !configured[dev].load()) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!configured[dev].load()) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            configured[dev].store(true);
+        }
+    }
+    return cudaMallocAsync(p, bytes, st);
+}
 void fv_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void fv_note_launches(long long delta) { g_launches.fetch_add((unsigned long long)delta, std::memory_order_relaxed); }
 unsigned long long fv_launches_now() { return g_launches.load(std::memory_order_relaxed); }
@@ -512,7 +531,7 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
     const unsigned G = (unsigned)((N + B - 1) / B);
     int32_t *len = nullptr;
     FV_CUDA_TRY(cudaMalloc(&m->row_ptr, sizeof(int32_t) * (N + 1)));
-    FV_CUDA_TRY(cudaMallocAsync(&len, sizeof(int32_t) * (N + 1), st));
+    FV_CUDA_TRY(fv_malloc_async(&len, sizeof(int32_t) * (N + 1), st));
     FV_CUDA_TRY(cudaMemsetAsync(len + N, 0, sizeof(int32_t), st));
     const int mf = m->maxf;
     if (mf <= 4)
@@ -525,7 +544,7 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, len, m->row_ptr, (int)(N + 1), st);
     void *tmp = nullptr;
-    FV_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+    FV_CUDA_TRY(fv_malloc_async(&tmp, tmp_bytes, st));
     FV_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, len, m->row_ptr, (int)(N + 1), st));
     int32_t nnz = 0;
     FV_CUDA_TRY(cudaMemcpyAsync(&nnz, m->row_ptr + N, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -623,7 +642,7 @@ extern "C" fv_status fv_assemble_host(fv_mesh *m, const fv_terms_desc *terms, co
     const int64_t N = m->n_cells, F = m->n_faces, Fb = m->n_bfaces;
     double *buf = nullptr;
     const size_t tot = (size_t)(2 * F + 2 * N + 2 * Fb);
-    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * tot, st));
+    FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * tot, st));
     double *dk = buf, *dfl = buf + F, *ds = buf + 2 * F, *db = buf + 2 * F + N, *dbi = buf + 2 * F + 2 * N,
            *dbe = dbi + Fb;
     fv_terms_desc t = *terms;

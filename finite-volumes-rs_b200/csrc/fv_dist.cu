@@ -263,7 +263,7 @@ fv_status precond(fv_precond *P, const double *r, double *z, int64_t n, cudaStre
 struct Vecs {
     double *base = nullptr;
     fv_status alloc(int64_t total, cudaStream_t st) {
-        FV_CUDA_TRY(cudaMallocAsync(&base, sizeof(double) * (total ? total : 1), st));
+        FV_CUDA_TRY(fv_malloc_async(&base, sizeof(double) * (total ? total : 1), st));
         FV_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(double) * (total ? total : 1), st));
         return FV_OK;
     }
@@ -300,14 +300,14 @@ extern "C" fv_status fv_csr_square_block(const fv_csr *A, void *stream, fv_csr *
     size_t tmp_bytes = 0;
     fv_status rc = FV_OK;
     cudaError_t e = cudaMalloc(&s->row_ptr, sizeof(int32_t) * (n + 1));
-    if (e == cudaSuccess) e = cudaMallocAsync(&cnt, sizeof(int32_t) * (n + 1), st);
+    if (e == cudaSuccess) e = fv_malloc_async(&cnt, sizeof(int32_t) * (n + 1), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st);
     if (e == cudaSuccess && n > 0) {
         fv_note_launch(), kd_square_count<<<vec_grid(n), DB, 0, st>>>(n, A->row_ptr, A->cols, cnt);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, s->row_ptr, (int)(n + 1), st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tmp_bytes ? tmp_bytes : 1, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&tmp, tmp_bytes ? tmp_bytes : 1, st);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, s->row_ptr, (int)(n + 1), st);
     int32_t nnz = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&nnz, s->row_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st);

@@ -30,6 +30,15 @@
 void fv_internal_set_cuda_error(cudaError_t e, const char *what);
 void fv_internal_set_error_text(const char *what);
 // Counts kernel launches made by this library (fv_launch_count).
+// cudaMallocAsync from the device's default pool, which is first told to keep
+// freed memory (release threshold = max): without that the pool hands memory
+// back to the driver at synchronisations and re-maps it on the next request,
+// which showed up as rare ~1 s stalls in repeated solves.
+cudaError_t fv_malloc_async_raw(void **p, size_t bytes, cudaStream_t st);
+template <typename T>
+static inline cudaError_t fv_malloc_async(T **p, size_t bytes, cudaStream_t st) {
+    return fv_malloc_async_raw(reinterpret_cast<void **>(p), bytes, st);
+}
 void fv_note_launch();
 void fv_note_launches(long long delta);  // graph replays add, captures (not run) subtract
 unsigned long long fv_launches_now();

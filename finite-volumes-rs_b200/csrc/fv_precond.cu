@@ -42,7 +42,7 @@ struct fv_symbolic {
     // box tiling of the two sweeps ([0] forward over L, [1] backward over U);
     // absent (tiled = false) for matrices without mesh geometry or without an
     // acyclic box order
-    bool tiled = false;
+    bool tiled = false, tiles_tried = false;
     int32_t t_nb[2] = {0, 0};
     int32_t *t_box_step[2] = {nullptr, nullptr}, *t_sptr[2] = {nullptr, nullptr};
     int32_t *t_trow[2] = {nullptr, nullptr}, *t_dsrc[2] = {nullptr, nullptr};
@@ -76,7 +76,7 @@ struct fv_precond {
     double *tmp = nullptr;        // forward-sweep output, kept at sentinel between applies
     unsigned *done = nullptr;     // factorisation flags
     unsigned epoch = 0;
-    int schedule = 0;             // 0: box tiles when planned, else level chunks; 1: level chunks
+    int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned)
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
@@ -191,29 +191,6 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     up_load(&s->fwd_order, fo, (size_t)n);
     up_load(&s->bwd_order, bo, (size_t)n);
     if (sym) up_load(&s->l_tpos, tpos, (size_t)nl);
-    // box tiles when the matrix was assembled on a mesh (cell centres known)
-    if (e == cudaSuccess && A->mesh && A->mesh->n_cells == n && n > 0) {
-        std::vector<double4> cells((size_t)n);
-        e = cudaMemcpyAsync(cells.data(), A->mesh->cell, sizeof(double4) * n, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        fv_tile_plan tp[2];
-        if (e == cudaSuccess &&
-            fv_build_tile_plans(n, A->mesh->dim, (const double *)cells.data(), lp.data(), lc.data(), up.data(),
-                                uc.data(), s->h_fwd_level.data(), s->h_bwd_level.data(), fo.data(), bo.data(),
-                                FV_TILE_RING, tp[0], tp[1])) {
-            for (int d = 0; d < 2; ++d) {
-                up_load(&s->t_box_step[d], tp[d].box_step, tp[d].box_step.size());
-                up_load(&s->t_sptr[d], tp[d].sptr, tp[d].sptr.size());
-                up_load(&s->t_trow[d], tp[d].trow, tp[d].trow.size());
-                up_load(&s->t_dsrc[d], tp[d].dsrc, tp[d].dsrc.size());
-                s->t_nb[d] = tp[d].nb;
-                s->t_lane_use[d] = tp[d].lane_use;
-                s->t_ring_share[d] = tp[d].ring_share;
-            }
-            s->t_edge = tp[0].edge;
-            s->tiled = e == cudaSuccess;
-        }
-    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         fv_internal_set_cuda_error(e, "symbolic upload");
@@ -221,6 +198,57 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
         return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
     }
     *out = s;
+    return FV_OK;
+}
+
+// Box tiles of the two sweeps, planned on first request when the matrix was
+// assembled on a mesh (cell centres known); s->tiled says whether a plan exists.
+static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
+    if (s->tiles_tried) return FV_OK;
+    s->tiles_tried = true;
+    const int64_t n = s->n;
+    if (!A->mesh || A->mesh->n_cells != n || n <= 0) return FV_OK;
+    std::vector<int32_t> lp((size_t)n + 1), up((size_t)n + 1), lc((size_t)(s->nnz_l ? s->nnz_l : 1)),
+        uc((size_t)(s->nnz_u ? s->nnz_u : 1)), fo((size_t)n), bo((size_t)n);
+    std::vector<double4> cells((size_t)n);
+    FV_CUDA_TRY(cudaMemcpyAsync(lp.data(), s->l_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(up.data(), s->u_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    if (s->nnz_l)
+        FV_CUDA_TRY(cudaMemcpyAsync(lc.data(), s->l_col, sizeof(int32_t) * s->nnz_l, cudaMemcpyDeviceToHost, st));
+    if (s->nnz_u)
+        FV_CUDA_TRY(cudaMemcpyAsync(uc.data(), s->u_col, sizeof(int32_t) * s->nnz_u, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(fo.data(), s->fwd_order, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(bo.data(), s->bwd_order, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(cells.data(), A->mesh->cell, sizeof(double4) * n, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    fv_tile_plan tp[2];
+    if (!fv_build_tile_plans(n, A->mesh->dim, (const double *)cells.data(), lp.data(), lc.data(), up.data(),
+                             uc.data(), s->h_fwd_level.data(), s->h_bwd_level.data(), fo.data(), bo.data(),
+                             FV_TILE_RING, tp[0], tp[1]))
+        return FV_OK;
+    cudaError_t e = cudaSuccess;
+    auto up_load = [&](int32_t **d, const std::vector<int32_t> &h) {
+        if (e != cudaSuccess) return;
+        e = cudaMalloc(d, sizeof(int32_t) * (h.size() ? h.size() : 1));
+        if (e == cudaSuccess && h.size())
+            e = cudaMemcpyAsync(*d, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, st);
+    };
+    for (int d = 0; d < 2; ++d) {
+        up_load(&s->t_box_step[d], tp[d].box_step);
+        up_load(&s->t_sptr[d], tp[d].sptr);
+        up_load(&s->t_trow[d], tp[d].trow);
+        up_load(&s->t_dsrc[d], tp[d].dsrc);
+        s->t_nb[d] = tp[d].nb;
+        s->t_lane_use[d] = tp[d].lane_use;
+        s->t_ring_share[d] = tp[d].ring_share;
+    }
+    s->t_edge = tp[0].edge;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "tile plan upload");
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    s->tiled = true;
     return FV_OK;
 }
 
@@ -649,7 +677,7 @@ static void launch_tiled(const fv_symbolic *s, int d, int maxl, cudaStream_t st,
 
 static bool use_tiles(const fv_precond *P) {
     const fv_symbolic *s = P->sym;
-    return P->schedule == 0 && s->tiled && s->max_lower <= 8 && s->max_upper <= 8;
+    return P->schedule == 2 && s->tiled && s->max_lower <= 8 && s->max_upper <= 8;
 }
 
 static int sweep_grid(int64_t n) {
@@ -773,9 +801,10 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
 
 extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
     if (!P || request < -1 || request > 2) return FV_ERR_INVALID;
-    const fv_symbolic *s = P->sym;
+    fv_symbolic *s = P->sym;
+    if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
     if (request == 2 && !(s->tiled && s->max_lower <= 8 && s->max_upper <= 8)) return FV_ERR_UNSUPPORTED;
-    if (request >= 0) P->schedule = request == 1 ? 1 : 0;
+    if (request >= 0) P->schedule = request == 2 ? 2 : 1;
     if (active) *active = use_tiles(P) ? 2 : 1;
     if (stats) {
         stats[0] = s->t_edge;
@@ -901,7 +930,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
     }
     if (kind == 2) {
         unsigned long long *cnt = nullptr;
-        FV_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(unsigned long long), st));
+        FV_CUDA_TRY(fv_malloc_async(&cnt, sizeof(unsigned long long), st));
         FV_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
         fv_note_launch(), k_count_dropped<<<592, 256, 0, st>>>(sym->nnz_l, P->l_val, sym->nnz_u, P->u_val, cnt);
         unsigned long long h = 0;
@@ -942,7 +971,7 @@ extern "C" fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, 
     if (!P || !r_host || !z_host) return FV_ERR_INVALID;
     cudaStream_t st = fv_stream(stream);
     double *buf = nullptr;
-    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * 2 * P->n, st));
+    FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * 2 * P->n, st));
     FV_CUDA_TRY(cudaMemcpyAsync(buf, r_host, sizeof(double) * P->n, cudaMemcpyHostToDevice, st));
     fv_status s = fv_precond_apply_dev(P, buf, buf + P->n, st, nullptr, nullptr);
     if (s == FV_OK) s = fv_precond_check_error(P, st);

@@ -449,7 +449,7 @@ extern "C" fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double 
     if (!A || !x_host || !y_host) return FV_ERR_INVALID;
     cudaStream_t st = fv_stream(stream);
     double *buf = nullptr;
-    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * (A->ncols + A->nrows + 1), st));
+    FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * (A->ncols + A->nrows + 1), st));
     FV_CUDA_TRY(cudaMemcpyAsync(buf, x_host, sizeof(double) * A->ncols, cudaMemcpyHostToDevice, st));
     fv_status s = fv_spmv(A, buf, buf + A->ncols, stream);
     if (s == FV_OK)
@@ -472,7 +472,7 @@ fv_status ws_alloc(Workspace &w, int64_t n, int nvec, const fv_solver_options &o
     const int64_t hist = opt.max_iterations + 3;
     const size_t bytes = sizeof(SolverState) + sizeof(double) * ((size_t)grid * 4 + (size_t)hist + (size_t)n * nvec);
     char *mem = nullptr;
-    FV_CUDA_TRY(cudaMallocAsync(&mem, bytes, st));
+    FV_CUDA_TRY(fv_malloc_async(&mem, bytes, st));
     w.S = (SolverState *)mem;
     double *d = (double *)(mem + sizeof(SolverState));
     SolverState h{};
@@ -685,7 +685,7 @@ static fv_status solve_host(bool bicg, const fv_csr *A, fv_precond *P, const dou
     cudaStream_t st = fv_stream(stream);
     const int64_t n = A->nrows;
     double *buf = nullptr;
-    FV_CUDA_TRY(cudaMallocAsync(&buf, sizeof(double) * 2 * n, st));
+    FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * 2 * n, st));
     FV_CUDA_TRY(cudaMemcpyAsync(buf, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     FV_CUDA_TRY(cudaMemcpyAsync(buf + n, x_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     fv_status s = bicg ? fv_bicgstab(A, P, buf, buf + n, opt, info, stream) : fv_cg(A, P, buf, buf + n, opt, info, stream);

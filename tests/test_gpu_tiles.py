@@ -21,7 +21,8 @@ def test_tiled_apply_equals_level_apply_and_oracle(fv, orc, kind):
     case = convdiff_3d(fv, 10, seed=4) if kind == "3d" else diffusion_2d(fv, 48, seed=4)
     A, b = _system(fv, case)
     P = (fv.IncompleteLowerUpper if kind == "3d" else fv.IncompleteCholesky).from_matrix(A, 0)
-    act, st = P.schedule()
+    assert P.schedule()[0] == 1  # level chunks by default
+    act, st = P.schedule(2)
     assert act == 2 and st[0] > 0 and st[1] > 1
     r = fv.DistributedVector(np.random.default_rng(5).standard_normal(A.nrows()))
     z_tiles = fv.DistributedVector.from_size(A.nrows())
@@ -35,7 +36,7 @@ def test_tiled_apply_equals_level_apply_and_oracle(fv, orc, kind):
     want = orc.Precond("ilu" if kind == "3d" else "ic", ptr, cols, vals).apply(r.numpy())
     assert np.array_equal(z_tiles.numpy(), want)
     # repeated applies keep the sentinel protocol intact
-    P.schedule(0)
+    P.schedule(2)
     for _ in range(3):
         P.precondition(z_tiles, r)
     assert np.array_equal(z_tiles.numpy(), want)
@@ -47,14 +48,14 @@ def test_tiled_solve_equals_level_solve(fv):
     P = fv.IncompleteLowerUpper.from_matrix(A, 0)
     opts = fv.LinearSolverOptions(1e-10, 1e-10, 2000)
     out = {}
-    for req in (0, 1):
+    for req in (2, 1):
         P.schedule(req)
         x = fv.DistributedVector.from_size(A.nrows())
         info = fv.bi_conjugate_gradient_stab(x, A, b, P, None, opts)
         out[req] = (x.numpy(), info.iterations, info.history)
-    assert out[0][1] == out[1][1]
-    assert np.array_equal(out[0][0], out[1][0])
-    assert out[0][2] == out[1][2]
+    assert out[2][1] == out[1][1]
+    assert np.array_equal(out[2][0], out[1][0])
+    assert out[2][2] == out[1][2]
 
 
 def test_tiled_fp32_batch_equals_level_batch(fv):
@@ -67,12 +68,12 @@ def test_tiled_fp32_batch_equals_level_batch(fv):
     nb = mb.n_boundary_faces
     A, b = fv.assemble(-fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc), (np.zeros(nb), np.zeros(nb)), mb)
     P = fv.IncompleteCholesky.from_matrix(A, 0)
-    assert P.schedule()[0] == 2
+    assert P.schedule(2)[0] == 2
     res = {}
-    for req in (0, 1):
+    for req in (2, 1):
         P.schedule(req)
         x = fv.DistributedVector.from_size(mb.n_cells)
         o = BatchCG(A, mb.cell_offsets, 256).solve(P, b, x, precision="mixed", outer_tolerance=1e-10)
         res[req] = (x.numpy(), list(o["iterations"]))
-    assert res[0][1] == res[1][1]
-    assert np.array_equal(res[0][0], res[1][0])
+    assert res[2][1] == res[1][1]
+    assert np.array_equal(res[2][0], res[1][0])
