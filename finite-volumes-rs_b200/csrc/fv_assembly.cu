@@ -75,6 +75,10 @@ struct AssembleArgs {
     double c_lap, c_conv, c_src;
     const int32_t *row_ptr;
     double *vals, *rhs;
+    // Corrected scheme
+    const double4 *fnorm, *fcen;
+    const double *grad;
+    double red;
 };
 
 // Face coefficients (li, lj) before the area factor, exactly as the
@@ -105,6 +109,175 @@ __device__ __forceinline__ void face_terms(double t, double kappa, double F, dou
         li = c_conv * conv0;
         lj = c_conv * conv1;
     }
+}
+
+// ------------------------------------------------------------ gradients
+// Vector of the face from cell c to the other cell (or to the boundary face
+// centre), as Mesh::compute forms it (compute.rs:165-177).
+template <int DIM>
+__device__ __forceinline__ void grad_dgc(int c, int f, const double4 *__restrict__ cell, const int2 *__restrict__ fc,
+                                         const double4 *__restrict__ fcen, double xc[3], double dgc[3]) {
+    const int2 on = fc[f];
+    double4 p;
+    if (on.y < 0) {
+        p = fcen[f];
+    } else {
+        const int co = on.y == c ? on.x : on.y;
+        p = cell[co];
+    }
+    dgc[0] = p.x - xc[0];
+    dgc[1] = p.y - xc[1];
+    dgc[2] = DIM == 3 ? p.z - xc[2] : 0.0;
+}
+
+// Matrix::inv (core/matrix.rs:320-380): Gauss-Jordan with the reference's
+// pivot rule (a pivot below 1e-14 is swapped with the row whose entry in the
+// pivot row is largest).  Returns false for a singular matrix.
+template <int N>
+__device__ __forceinline__ bool mat_inv(double (&a)[N][N], double (&out)[N][N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) out[i][j] = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < N - 1; ++k) {
+        double piv = a[k][k];
+        if (fabs(piv) < 1e-14) {
+            int maxi = k;
+            double maxp = fabs(piv);
+#pragma unroll
+            for (int j = k + 1; j < N; ++j) {
+                const double pj = fabs(a[k][j]);
+                if (pj > maxp) {
+                    maxi = j;
+                    maxp = pj;
+                }
+            }
+            if (maxi == k) return false;
+#pragma unroll
+            for (int r = k + 1; r < N; ++r)
+                if (r == maxi)
+#pragma unroll
+                    for (int j = 0; j < N; ++j) {
+                        double t = a[k][j];
+                        a[k][j] = a[r][j];
+                        a[r][j] = t;
+                        t = out[k][j];
+                        out[k][j] = out[r][j];
+                        out[r][j] = t;
+                    }
+        }
+        piv = a[k][k];
+#pragma unroll
+        for (int i = k + 1; i < N; ++i) {
+            const double f = (-a[i][k]) / piv;
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                a[i][j] += a[k][j] * f;
+                out[i][j] += out[k][j] * f;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const double piv = a[k][k];
+        if (fabs(piv) < 1e-14) return false;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            a[k][j] /= piv;
+            out[k][j] /= piv;
+        }
+    }
+#pragma unroll
+    for (int k = N - 1; k >= 1; --k) {
+        const double piv = a[k][k];
+#pragma unroll
+        for (int i = 0; i < k; ++i) {
+            const double f = (-a[i][k]) / piv;
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                a[i][j] += a[k][j] * f;
+                out[i][j] += out[k][j] * f;
+            }
+        }
+    }
+    return true;
+}
+
+// Gradient coefficients of Mesh::compute (compute.rs:155-203), one cell per thread.
+template <int DIM>
+__global__ void k_grad_coeffs(int64_t n, const double4 *__restrict__ cell, const int2 *__restrict__ fc,
+                              const double4 *__restrict__ fcen, const int32_t *__restrict__ gptr,
+                              const int32_t *__restrict__ gface, double4 *__restrict__ gcoef,
+                              double4 *__restrict__ gdiag, int *bad) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double4 x4 = cell[c];
+    double xc[3] = {x4.x, x4.y, x4.z};
+    double g[DIM][DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) g[i][j] = 0.0;
+    const int s = gptr[c], e = gptr[c + 1];
+    for (int k = s; k < e; ++k) {
+        double d[3];
+        grad_dgc<DIM>((int)c, gface[k], cell, fc, fcen, xc, d);
+#pragma unroll
+        for (int i = 0; i < DIM; ++i)
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) g[i][j] += d[i] * d[j];
+    }
+    double gi[DIM][DIM];
+    if (!mat_inv<DIM>(g, gi)) {
+        atomicOr(bad, 1);
+        return;
+    }
+    double own[3] = {0.0, 0.0, 0.0};
+    for (int k = s; k < e; ++k) {
+        double d[3], v[3] = {0.0, 0.0, 0.0};
+        grad_dgc<DIM>((int)c, gface[k], cell, fc, fcen, xc, d);
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) {
+            double x = 0.0;
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) x += gi[i][j] * d[j];
+            v[i] = x;
+            own[i] -= x;
+        }
+        gcoef[k] = make_double4(v[0], v[1], v[2], 0.0);
+    }
+    gdiag[c] = make_double4(own[0], own[1], own[2], 0.0);
+}
+
+// compute_gradients (gradients.rs:48-86) for a scalar field, one cell per thread.
+template <int DIM>
+__global__ void k_gradients(int64_t n, int64_t fb0, const double *__restrict__ val, const int2 *__restrict__ fc,
+                            const int32_t *__restrict__ gptr, const int32_t *__restrict__ gface,
+                            const double4 *__restrict__ gcoef, const double4 *__restrict__ gdiag,
+                            const double *__restrict__ bndi, const double *__restrict__ bnde,
+                            double *__restrict__ grad) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double vc = val[c];
+    const double4 o = gdiag[c];
+    double g[3] = {vc * o.x, vc * o.y, DIM == 3 ? vc * o.z : 0.0};
+    for (int k = gptr[c]; k < gptr[c + 1]; ++k) {
+        const int f = gface[k];
+        const int2 on = fc[f];
+        double w;
+        if (on.y >= 0) {
+            w = val[on.y == (int)c ? on.x : on.y];
+        } else {
+            w = bndi[f - fb0] * vc + bnde[f - fb0];
+        }
+        const double4 q = gcoef[k];
+        g[0] += w * q.x;
+        g[1] += w * q.y;
+        if (DIM == 3) g[2] += w * q.z;
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) grad[c * DIM + d] = g[d];
 }
 
 template <int DIM, int MAXF>
@@ -202,7 +375,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
 // output value receives the same additions in the same order as in k_assemble.
 constexpr int kAsmBlock = 128;
 
-template <int DIM, int MAXF>
+template <int DIM, int MAXF, bool CORR>
 __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
     extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
     const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
@@ -281,8 +454,9 @@ __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(A
                 pi = make_double3(ci4.x, ci4.y, ci4.z);
                 pj = make_double3(oc[k].x, oc[k].y, oc[k].z);
             }
-            double d2 = 0.0;
-            {
+            double t, rsch = 0.0;
+            if (!CORR) {  // Orthogonal (orthogonal.rs:26-46): 1/|d|
+                double d2 = 0.0;
                 double dd = pj.x - pi.x;
                 d2 += dd * dd;
                 dd = pj.y - pi.y;
@@ -291,14 +465,57 @@ __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(A
                     dd = pj.z - pi.z;
                     d2 += dd * dd;
                 }
+                t = 1.0 / sqrt(d2);
+            } else {  // Corrected (corrected.rs:36-67): 1/(n.d) and the explicit correction
+                const int f = fe[k] & 0x7fffffff;
+                const double4 n4 = a.fnorm[f];
+                const double d0 = pj.x - pi.x, d1 = pj.y - pi.y, d2 = DIM == 3 ? pj.z - pi.z : 0.0;
+                double nd = 0.0;
+                nd += n4.x * d0;
+                nd += n4.y * d1;
+                if (DIM == 3) nd += n4.z * d2;
+                const double cc = 1.0 / nd;
+                const double v0 = n4.x - cc * d0, v1 = n4.y - cc * d1, v2 = DIM == 3 ? n4.z - cc * d2 : 0.0;
+                const int own = (jj[k] >= 0 && is_nb) ? jj[k] : (int)i;
+                double g0, g1, g2 = 0.0;
+                if (jj[k] >= 0) {
+                    const int nbr = is_nb ? (int)i : jj[k];
+                    const double4 c4 = a.fcen[f];
+                    const double e0 = c4.x - pi.x, e1 = c4.y - pi.y, e2 = DIM == 3 ? c4.z - pi.z : 0.0;
+                    double en = 0.0, dn = 0.0;
+                    en += e0 * n4.x;
+                    en += e1 * n4.y;
+                    if (DIM == 3) en += e2 * n4.z;
+                    dn += d0 * n4.x;
+                    dn += d1 * n4.y;
+                    if (DIM == 3) dn += d2 * n4.z;
+                    const double w = en / dn;
+                    g0 = a.grad[(int64_t)own * DIM] * (1.0 - w) + a.grad[(int64_t)nbr * DIM] * w;
+                    g1 = a.grad[(int64_t)own * DIM + 1] * (1.0 - w) + a.grad[(int64_t)nbr * DIM + 1] * w;
+                    if (DIM == 3) g2 = a.grad[(int64_t)own * DIM + 2] * (1.0 - w) + a.grad[(int64_t)nbr * DIM + 2] * w;
+                } else {
+                    g0 = a.grad[(int64_t)own * DIM];
+                    g1 = a.grad[(int64_t)own * DIM + 1];
+                    if (DIM == 3) g2 = a.grad[(int64_t)own * DIM + 2];
+                }
+                double ex = 0.0;
+                ex += g0 * v0;
+                ex += g1 * v1;
+                if (DIM == 3) ex += g2 * v2;
+                t = cc;
+                rsch = ex * a.red;
             }
-            const double t = 1.0 / sqrt(d2);
             double li, lj;
             face_terms(t, kp[k], fl[k], a.c_lap, a.c_conv, li, lj);
             const double A = ar[k];
             li = li * A;
             lj = lj * A;
-            const double ra = 0.0 * A;
+            double r = 0.0;
+            if (CORR) {  // laplacian rhs -(kappa * explicit), combined like li/lj
+                const double lap_r = -(kp[k] * rsch);
+                r = (a.c_conv != 0.0) ? a.c_conv * 0.0 + a.c_lap * lap_r : a.c_lap * lap_r;
+            }
+            const double ra = r * A;
             if (jj[k] < 0) {
                 const int fb = (fe[k] & 0x7fffffff) - (int)a.fb0;
                 const double bi = a.bndi[fb], be = a.bnde[fb];
@@ -352,8 +569,10 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
-        if (a.cf_pad)
-            fv_note_launch(), k_assemble_reg<DIM, MAXF><<<G, B, smem, st>>>(a);
+        if (a.grad)
+            fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
+        else if (a.cf_pad)
+            fv_note_launch(), k_assemble_reg<DIM, MAXF, false><<<G, B, smem, st>>>(a);
         else
             fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
     } else {
@@ -424,6 +643,12 @@ extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
     cudaFree(m->cf_face);
     cudaFree(m->cf_other);
     cudaFree(m->cf_pad);
+    cudaFree(m->face_normal);
+    cudaFree(m->face_center);
+    cudaFree(m->gcf_ptr);
+    cudaFree(m->gcf_face);
+    cudaFree(m->gcoef);
+    cudaFree(m->gdiag);
     cudaFree(m->row_ptr);
     cudaFree(m->cols);
     delete m;
@@ -465,6 +690,18 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     int maxf = 0;
     for (int64_t c = 0; c < N; ++c) maxf = std::max(maxf, cnt[c + 1] - cnt[c]);
     if (maxf > 16) return FV_ERR_UNSUPPORTED;
+    // optional gradient data: every listed face must touch its cell
+    const bool grad_ok = d->face_normal && d->cell_face_ptr && d->cell_faces && d->face_center;
+    if (grad_ok) {
+        if (d->cell_face_ptr[0] != 0) return FV_ERR_INVALID;
+        for (int64_t c = 0; c < N; ++c) {
+            if (d->cell_face_ptr[c + 1] < d->cell_face_ptr[c]) return FV_ERR_INVALID;
+            for (int32_t k = d->cell_face_ptr[c]; k < d->cell_face_ptr[c + 1]; ++k) {
+                const int32_t f = d->cell_faces[k];
+                if (f < 0 || f >= F || (d->face_owner[f] != c && d->face_neighbor[f] != c)) return FV_ERR_INVALID;
+            }
+        }
+    }
     const int padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
     std::vector<int2> pad((size_t)(padf ? N * padf : 1), make_int2(0, -2));
     if (padf)
@@ -514,13 +751,82 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     if (e == cudaSuccess && padf) e = cudaMalloc(&m->cf_pad, sizeof(int2) * N * padf);
     if (e == cudaSuccess && padf)
         e = cudaMemcpyAsync(m->cf_pad, pad.data(), sizeof(int2) * N * padf, cudaMemcpyHostToDevice, st);
+    // normals, all face centres and the mesh-order cell faces: gradient
+    // coefficients (compute.rs:155-203) for the Corrected scheme
+    std::vector<double4> fn4, fc4;
+    int gbad = 0;
+    int *dbad = nullptr;
+    if (e == cudaSuccess && grad_ok) {
+        fn4.resize((size_t)F);
+        fc4.resize((size_t)F);
+        for (int64_t f = 0; f < F; ++f) {
+            const double *q = d->face_normal + f * dim, *p = d->face_center + f * dim;
+            fn4[f] = make_double4(q[0], q[1], dim == 3 ? q[2] : 0.0, 0.0);
+            fc4[f] = make_double4(p[0], p[1], dim == 3 ? p[2] : 0.0, 0.0);
+        }
+        const int64_t ng = d->cell_face_ptr[N];
+        e = cudaMalloc(&m->face_normal, sizeof(double4) * F);
+        if (e == cudaSuccess) e = cudaMalloc(&m->face_center, sizeof(double4) * F);
+        if (e == cudaSuccess) e = cudaMalloc(&m->gcf_ptr, sizeof(int32_t) * (N + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&m->gcf_face, sizeof(int32_t) * (ng ? ng : 1));
+        if (e == cudaSuccess) e = cudaMalloc(&m->gcoef, sizeof(double4) * (ng ? ng : 1));
+        if (e == cudaSuccess) e = cudaMalloc(&m->gdiag, sizeof(double4) * N);
+        if (e == cudaSuccess) e = cudaMalloc(&dbad, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(dbad, 0, sizeof(int), st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(m->face_normal, fn4.data(), sizeof(double4) * F, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(m->face_center, fc4.data(), sizeof(double4) * F, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(m->gcf_ptr, d->cell_face_ptr, sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && ng)
+            e = cudaMemcpyAsync(m->gcf_face, d->cell_faces, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            const unsigned G = (unsigned)((N + 127) / 128);
+            if (dim == 2)
+                fv_note_launch(), k_grad_coeffs<2><<<G, 128, 0, st>>>(N, m->cell, m->face_cells, m->face_center,
+                                                                       m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag,
+                                                                       dbad);
+            else
+                fv_note_launch(), k_grad_coeffs<3><<<G, 128, 0, st>>>(N, m->cell, m->face_cells, m->face_center,
+                                                                       m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag,
+                                                                       dbad);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&gbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging vectors go out of scope
+    if (dbad) cudaFree(dbad);
     if (e != cudaSuccess) {
         fv_internal_set_cuda_error(e, "fv_mesh_upload");
         fv_mesh_destroy(m);
         return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
     }
+    if (gbad) {  // Mesh::compute returns Error::SingularMatrix
+        fv_internal_set_error_text("fv_mesh_upload: singular gradient matrix of a cell");
+        fv_mesh_destroy(m);
+        return FV_ERR_INVALID;
+    }
     *out = m;
+    return FV_OK;
+}
+
+extern "C" fv_status fv_compute_gradients(fv_mesh *m, const double *values, const fv_bc_desc *bc, double *grad,
+                                          void *stream) {
+    if (!m || !values || !grad) return FV_ERR_INVALID;
+    if (!m->gcoef) return FV_ERR_UNSUPPORTED;
+    if (m->n_bfaces > 0 && (!bc || !bc->bndi || !bc->bnde)) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    const int64_t N = m->n_cells;
+    const unsigned G = (unsigned)((N + 127) / 128);
+    const double *bi = bc ? bc->bndi : nullptr, *be = bc ? bc->bnde : nullptr;
+    if (m->dim == 2)
+        fv_note_launch(), k_gradients<2><<<G, 128, 0, st>>>(N, m->n_faces - m->n_bfaces, values, m->face_cells,
+                                                             m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag, bi, be, grad);
+    else
+        fv_note_launch(), k_gradients<3><<<G, 128, 0, st>>>(N, m->n_faces - m->n_bfaces, values, m->face_cells,
+                                                             m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag, bi, be, grad);
+    FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
 
@@ -615,6 +921,17 @@ extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const f
     args.row_ptr = m->row_ptr;
     args.vals = a->vals;
     args.rhs = b;
+    args.fnorm = m->face_normal;
+    args.fcen = m->face_center;
+    args.grad = nullptr;
+    args.red = terms->corrector_reduction;
+    if (terms->scheme == FV_SCHEME_CORRECTED && terms->laplacian_coef != 0.0) {
+        if (!m->face_normal || !m->cf_pad) return FV_ERR_UNSUPPORTED;
+        if (!terms->gradients) return FV_ERR_INVALID;
+        args.grad = terms->gradients;
+    } else if (terms->scheme != FV_SCHEME_ORTHOGONAL && terms->scheme != FV_SCHEME_CORRECTED) {
+        return FV_ERR_INVALID;
+    }
     const int mf = m->maxf;
     if (m->dim == 2) {
         if (mf <= 4)
@@ -641,11 +958,15 @@ extern "C" fv_status fv_assemble_host(fv_mesh *m, const fv_terms_desc *terms, co
     cudaStream_t st = fv_stream(stream);
     const int64_t N = m->n_cells, F = m->n_faces, Fb = m->n_bfaces;
     double *buf = nullptr;
-    const size_t tot = (size_t)(2 * F + 2 * N + 2 * Fb);
+    const size_t tot = (size_t)(2 * F + 2 * N + 2 * Fb + N * m->dim);
     FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * tot, st));
     double *dk = buf, *dfl = buf + F, *ds = buf + 2 * F, *db = buf + 2 * F + N, *dbi = buf + 2 * F + 2 * N,
-           *dbe = dbi + Fb;
+           *dbe = dbi + Fb, *dg = dbe + Fb;
     fv_terms_desc t = *terms;
+    if (terms->gradients) {
+        FV_CUDA_TRY(cudaMemcpyAsync(dg, terms->gradients, sizeof(double) * N * m->dim, cudaMemcpyHostToDevice, st));
+        t.gradients = dg;
+    }
     if (terms->diffusivity) {
         FV_CUDA_TRY(cudaMemcpyAsync(dk, terms->diffusivity, sizeof(double) * F, cudaMemcpyHostToDevice, st));
         t.diffusivity = dk;

@@ -62,6 +62,13 @@ struct fv_mesh {
     int32_t *cf_other = nullptr;       // the other cell, -1 for boundary faces
     int2 *cf_pad = nullptr;            // (cf_face, cf_other) at cell * padf + slot, padded with (0, -2)
     int padf = 0;                      // 4 or 8 (0: no padded copy, cells with more than 8 faces)
+    // Corrected scheme / gradients (present when uploaded with normals and cell_faces)
+    double4 *face_normal = nullptr;    // per face (x, y, z|0, 0)
+    double4 *face_center = nullptr;    // per face, all faces
+    int32_t *gcf_ptr = nullptr;        // the cells' faces in mesh order (Mesh::cell_faces)
+    int32_t *gcf_face = nullptr;
+    double4 *gcoef = nullptr;          // gradient coefficient of each (cell, face) in that order
+    double4 *gdiag = nullptr;          // gradient coefficient of the cell itself
     // CSR pattern of cell_to_cell (built on the first assemble)
     int32_t *row_ptr = nullptr;
     int32_t *cols = nullptr;

@@ -9,7 +9,8 @@ bi_conjugate_gradient_stab, LinearSolverOptions, LinearSolverInfo}).
 from ._lib import FvError, lib  # noqa: F401
 from .linalg import (  # noqa: F401
     DistributedMatrix, DistributedVector, IdentityPreconditioner, IncompleteCholesky, IncompleteLowerUpper,
-    LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, conjugate_gradient,
+    LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, compute_gradients,
+    conjugate_gradient,
 )
 from .mesh import DeviceMesh, Mesh  # noqa: F401
-from .terms import Orthogonal, Upwind, convection, laplacian, source  # noqa: F401
+from .terms import Corrected, Orthogonal, Upwind, convection, laplacian, source  # noqa: F401

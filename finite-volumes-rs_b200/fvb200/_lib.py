@@ -51,7 +51,7 @@ class MeshDesc(C.Structure):
     _fields_ = [
         ("dim", C.c_int32), ("n_cells", i64), ("n_faces", i64), ("n_boundary_faces", i64),
         ("face_owner", ip), ("face_neighbor", ip), ("face_area", dp), ("face_center", dp),
-        ("cell_center", dp), ("cell_volume", dp),
+        ("cell_center", dp), ("cell_volume", dp), ("face_normal", dp), ("cell_face_ptr", ip), ("cell_faces", ip),
     ]
 
 
@@ -59,6 +59,7 @@ class TermsDesc(C.Structure):
     _fields_ = [
         ("laplacian_coef", C.c_double), ("convection_coef", C.c_double), ("source_coef", C.c_double),
         ("diffusivity", C.c_void_p), ("flux", C.c_void_p), ("source", C.c_void_p),
+        ("scheme", C.c_int32), ("corrector_reduction", C.c_double), ("gradients", C.c_void_p),
     ]
 
 
@@ -110,6 +111,7 @@ _SIGS = {
     # device objects
     "fv_mesh_upload": [P(MeshDesc), vp, P(vp)],
     "fv_mesh_destroy": [vp],
+    "fv_compute_gradients": [vp, vp, P(BcDesc), vp, vp],
     "fv_assemble": [vp, P(TermsDesc), P(BcDesc), P(vp), vp, vp],
     "fv_assemble_host": [vp, P(TermsDesc), P(BcDesc), P(vp), dp, vp],
     "fv_csr_create_host": [i64, i64, ip, ip, dp, vp, P(vp)],

@@ -156,6 +156,16 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
     t.diffusivity = dptr("laplacian")
     t.flux = dptr("convection")
     t.source = dptr("source")
+    sch = equation.data.get("laplacian_scheme")
+    if sch is not None and sch.__class__.__name__ == "Corrected":
+        g = sch.gradients.data if isinstance(sch.gradients, DistributedVector) else _dev_f64(sch.gradients)
+        g = g.reshape(-1).contiguous()
+        if g.numel() != mesh.n_cells * mesh.dim:
+            raise ValueError("Corrected: gradients must hold n_cells * dim values")
+        keep.append(g)
+        t.scheme = 1
+        t.corrector_reduction = sch.corrector_reduction
+        t.gradients = g.data_ptr()
     nb = mesh.n_boundary_faces
     if callable(boundary_condition):
         fb0 = mesh.n_faces - nb
@@ -178,6 +188,30 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
     if lhs is None:
         lhs = DistributedMatrix(h, keepalive=dm)
     return lhs, rhs
+
+
+def compute_gradients(gradients: DistributedVector, values, boundary_condition, mesh, stream=None) -> None:
+    """compute_gradients (fvm/tools/gradients.rs:48-86): least-squares cell
+    gradients of a cell field into `gradients` (n_cells*dim, cell-major).
+    boundary_condition as in assemble (callable face id -> (bndi, bnde), or a
+    pair of arrays over the boundary faces)."""
+    dm = mesh.device(stream)
+    v = _dev_f64(values)
+    nb = mesh.n_boundary_faces
+    if callable(boundary_condition):
+        fb0 = mesh.n_faces - nb
+        pairs = [boundary_condition(fb0 + k) for k in range(nb)]
+        bndi = np.array([p[0] for p in pairs], dtype=np.float64)
+        bnde = np.array([p[1] for p in pairs], dtype=np.float64)
+    else:
+        bndi, bnde = boundary_condition
+    bi, be = _dev_f64(bndi), _dev_f64(bnde)
+    if len(gradients) != mesh.n_cells * mesh.dim:
+        raise ValueError("gradients must hold n_cells * dim values")
+    bc = BcDesc(bi.data_ptr(), be.data_ptr())
+    check(lib().fv_compute_gradients(dm.handle, C.c_void_p(v.data_ptr()), C.byref(bc), gradients.ptr(),
+                                     stream_handle(stream)), "compute_gradients")
+    del v, bi, be
 
 
 class Preconditioner:

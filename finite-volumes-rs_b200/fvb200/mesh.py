@@ -166,6 +166,16 @@ class DeviceMesh:
         d.face_center = Pd(mesh.face_center)
         d.cell_center = Pd(mesh.cell_center)
         d.cell_volume = Pd(mesh.cell_volume)
+        # normals and the mesh-order cell faces: gradients and the Corrected scheme
+        self._keep = []
+        if getattr(mesh, "face_normal", None) is not None and getattr(mesh, "cell_faces", None) is not None:
+            fn = np.ascontiguousarray(mesh.face_normal, dtype=np.float64)
+            cp = np.ascontiguousarray(mesh.cell_face_ptr, dtype=np.int32)
+            cf = np.ascontiguousarray(mesh.cell_faces, dtype=np.int32)
+            self._keep = [fn, cp, cf]
+            d.face_normal = Pd(fn)
+            d.cell_face_ptr = Pi(cp)
+            d.cell_faces = Pi(cf)
         self.handle = C.c_void_p()
         check(lib().fv_mesh_upload(C.byref(d), stream_handle(stream), C.byref(self.handle)), "fv_mesh_upload")
 

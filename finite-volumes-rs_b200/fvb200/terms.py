@@ -3,12 +3,13 @@
 Mirrors src/fvm/terms/mod.rs:24-40 (Term), operations.rs:86-199 (+, -, unary
 -), laplacian.rs:21 (laplacian), convection.rs:24 (convection),
 source.rs:22 (source), with the schemes facengrad::Orthogonal
-(orthogonal.rs:26-46) and faceinterp::Upwind (upwind.rs:26-33).
+(orthogonal.rs:26-46), facengrad::Corrected (corrected.rs:36-67) and
+faceinterp::Upwind (upwind.rs:26-33).
 
 An expression is kept as a signed combination of at most one laplacian, one
 convection and one source term, which is exactly what the term tree computes:
-every value is a sum of +/- the individual terms.  Anything else (Corrected,
-Linear/LimitedLinear interpolation in convection, time, divergence,
+every value is a sum of +/- the individual terms.  Anything else
+(Linear/LimitedLinear interpolation in convection, time, divergence,
 linear_source) raises NotImplementedError at construction.
 """
 from __future__ import annotations
@@ -20,9 +21,15 @@ class Orthogonal:
     """facengrad::Orthogonal: two-point flux gradient 1/|c_j - c_i|."""
 
 
-class Corrected:  # pragma: no cover - name kept for API parity
-    def __init__(self, *a, **k):
-        raise NotImplementedError("facengrad::Corrected is not implemented on the device path")
+class Corrected:
+    """facengrad::Corrected(gradients, corrector_reduction): coefficient
+    1/(n.d) plus the explicit non-orthogonal correction from the cell
+    gradients (a DistributedVector / array of n_cells*dim, e.g. filled by
+    compute_gradients); corrector_reduction 0 = none ... 1 = full."""
+
+    def __init__(self, gradients, corrector_reduction: float = 1.0):
+        self.gradients = gradients
+        self.corrector_reduction = float(corrector_reduction)
 
 
 class Upwind:
@@ -54,6 +61,8 @@ class TermExpr:
                 raise NotImplementedError(f"two {k} terms in one expression")
             coef[k] = sign * c
             data[k] = other.data[k]
+            if k + "_scheme" in other.data:
+                data[k + "_scheme"] = other.data[k + "_scheme"]
         return TermExpr(coef, data)
 
     def __add__(self, other):
@@ -70,9 +79,9 @@ class TermExpr:
 
 
 def laplacian(scheme, diffusivity) -> TermExpr:
-    if not isinstance(scheme, Orthogonal):
-        raise NotImplementedError("only facengrad::Orthogonal runs on the device")
-    return TermExpr({"laplacian": 1.0}, {"laplacian": diffusivity})
+    if not isinstance(scheme, (Orthogonal, Corrected)):
+        raise NotImplementedError("only facengrad::Orthogonal and facengrad::Corrected run on the device")
+    return TermExpr({"laplacian": 1.0}, {"laplacian": diffusivity, "laplacian_scheme": scheme})
 
 
 def convection(scheme, flux) -> TermExpr:

@@ -129,12 +129,25 @@ typedef struct fv_mesh_desc {
     const double  *face_center;   /* n_faces*dim */
     const double  *cell_center;   /* n_cells*dim */
     const double  *cell_volume;
+    /* Optional, for the Corrected scheme and compute_gradients (NULL when not
+     * needed): the face normals (n_faces*dim) and every cell's faces in the
+     * mesh's own order (Mesh::cell_faces, cell_face_ptr[n_cells+1]), which is
+     * the order the gradient coefficients are summed in (compute.rs:155-203). */
+    const double  *face_normal;
+    const int32_t *cell_face_ptr;
+    const int32_t *cell_faces;
 } fv_mesh_desc;
 
-/* The term expression c_conv*convection(Upwind(F),F) + c_lap*laplacian(Orthogonal,kappa)
+/* The term expression c_conv*convection(Upwind(F),F) + c_lap*laplacian(S,kappa)
  * + c_src*source(f) of fvm/terms (laplacian.rs:35-45, convection.rs:36-45,
  * source.rs:34-40, operations.rs:86-199).  Coefficients must be -1, 0 or +1
- * (the reference's term algebra has +, - and unary - only). */
+ * (the reference's term algebra has +, - and unary - only).  The face-normal
+ * gradient scheme S is Orthogonal (orthogonal.rs:26-46) or Corrected
+ * (corrected.rs:36-67: coefficient 1/(n.d) and the explicit non-orthogonal
+ * correction kappa * grad_f.(n - d/(n.d)) * corrector_reduction on the rhs,
+ * grad_f interpolated from the cell gradients). */
+#define FV_SCHEME_ORTHOGONAL 0
+#define FV_SCHEME_CORRECTED 1
 typedef struct fv_terms_desc {
     double laplacian_coef;
     double convection_coef;
@@ -142,6 +155,9 @@ typedef struct fv_terms_desc {
     const double *diffusivity; /* n_faces, device (fv_assemble) or host (_host) */
     const double *flux;        /* n_faces */
     const double *source;      /* n_cells */
+    int32_t scheme;            /* FV_SCHEME_ORTHOGONAL or FV_SCHEME_CORRECTED */
+    double corrector_reduction;/* Corrected: 0 = no correction ... 1 = full */
+    const double *gradients;   /* Corrected: n_cells*dim cell gradients (fv_compute_gradients) */
 } fv_terms_desc;
 
 /* Boundary closure value_b = bndi*value_i + bnde per boundary face
@@ -173,6 +189,16 @@ typedef struct fv_solver_info {
 
 fv_status fv_mesh_upload(const fv_mesh_desc *desc, void *stream, fv_mesh **out);
 fv_status fv_mesh_destroy(fv_mesh *m);
+
+/* compute_gradients (fvm/tools/gradients.rs:48-86): least-squares cell
+ * gradients of a cell field, grad[c] = values[c] * own_c + sum over the
+ * cell's faces (mesh order) of value_other * g_k, a boundary face taking
+ * bndi*values[c] + bnde.  The coefficients own_c and g_k are those of
+ * Mesh::compute (compute.rs:155-203), computed at upload; the mesh must have
+ * been uploaded with cell_face_ptr / cell_faces (else FV_ERR_UNSUPPORTED).
+ * values: n_cells, grad: n_cells*dim (device). */
+fv_status fv_compute_gradients(fv_mesh *m, const double *values, const fv_bc_desc *bc, double *grad,
+                               void *stream);
 
 /* assemble(): builds the CSR pattern of cell_to_cell (dmatrix.rs:38-50) on the
  * first call (*A == NULL) and refills values into the existing pattern when

@@ -40,6 +40,11 @@ def lib():
             "or_pattern": ([i64, ip, ip, ip, ip, ip, ip, P(i64)], C.c_int),
             "or_assemble": ([C.c_int32, i64, i64, i64, ip, ip, dp, dp, dp, dp, C.c_double, C.c_double, C.c_double,
                              dp, dp, dp, dp, dp, ip, ip, dp, dp], C.c_int),
+            "or_assemble_scheme": ([C.c_int32, i64, i64, i64, ip, ip, dp, dp, dp, dp, C.c_double, C.c_double,
+                                    C.c_double, dp, dp, dp, dp, dp, ip, ip, dp, dp, C.c_int, dp, dp, C.c_double],
+                                   C.c_int),
+            "or_grad_coeffs": ([C.c_int32, i64, ip, ip, dp, dp, ip, ip, dp, dp], C.c_int),
+            "or_gradients": ([C.c_int32, i64, i64, i64, ip, ip, ip, ip, dp, dp, dp, dp, dp, dp], None),
             "or_spmv": ([i64, ip, ip, dp, dp, dp], None),
             "or_dot": ([i64, dp, dp], C.c_double),
             "or_ic0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
@@ -91,8 +96,39 @@ def pattern(mesh):
     return ptr, cols[: nnz.value]
 
 
-def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bndi=None, bnde=None):
-    """assemble() restated: returns (row_ptr, cols, vals, rhs)."""
+def grad_coeffs(mesh):
+    """Gradient coefficients of Mesh::compute: (per cell-face entry in mesh
+    order, n_entries x dim; per cell, n_cells x dim)."""
+    d, N = mesh.dim, mesh.n_cells
+    cfp, cf = _i(mesh.cell_face_ptr), _i(mesh.cell_faces)
+    gcoef = np.empty((max(int(cfp[-1]), 1), d))
+    gdiag = np.empty((N, d))
+    rc = lib().or_grad_coeffs(d, N, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
+                              _pd(_d(mesh.face_center)), _pd(_d(mesh.cell_center)), _pi(cfp), _pi(cf), _pd(gcoef),
+                              _pd(gdiag))
+    if rc != 0:
+        raise RuntimeError("oracle gradient coefficients: singular cell matrix")
+    return gcoef[: int(cfp[-1])], gdiag
+
+
+def gradients(mesh, values, bndi, bnde):
+    """compute_gradients restated: n_cells x dim."""
+    gcoef, gdiag = grad_coeffs(mesh)
+    d, N = mesh.dim, mesh.n_cells
+    out = np.empty((N, d))
+    gc = _d(gcoef) if len(gcoef) else np.zeros((1, d))
+    lib().or_gradients(d, N, mesh.n_faces, mesh.n_boundary_faces, _pi(_i(mesh.face_owner)),
+                       _pi(_i(mesh.face_neighbor)), _pi(_i(mesh.cell_face_ptr)), _pi(_i(mesh.cell_faces)), _pd(gc),
+                       _pd(_d(gdiag)), _pd(_d(values)), _pd(_d(bndi) if len(bndi) else np.zeros(1)),
+                       _pd(_d(bnde) if len(bnde) else np.zeros(1)), _pd(out))
+    return out
+
+
+def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bndi=None, bnde=None,
+             corrected=None):
+    """assemble() restated: returns (row_ptr, cols, vals, rhs).  corrected =
+    (gradients n_cells x dim, corrector_reduction) selects the Corrected
+    face-normal gradient scheme for the laplacian (Orthogonal otherwise)."""
     ptr, cols = pattern(mesh)
     F, N, Fb = mesh.n_faces, mesh.n_cells, mesh.n_boundary_faces
     z = lambda n: np.zeros(max(n, 1))  # noqa: E731
@@ -103,10 +139,18 @@ def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bnd
     bnde = _d(bnde) if bnde is not None else z(Fb)
     vals = np.empty(len(cols))
     rhs = np.empty(N)
-    rc = lib().or_assemble(mesh.dim, N, F, Fb, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
-                           _pd(_d(mesh.face_area)), _pd(_d(mesh.face_center)), _pd(_d(mesh.cell_center)),
-                           _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src, _pd(kappa), _pd(flux), _pd(source),
-                           _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols), _pd(vals), _pd(rhs))
+    if corrected is None:
+        rc = lib().or_assemble(mesh.dim, N, F, Fb, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
+                               _pd(_d(mesh.face_area)), _pd(_d(mesh.face_center)), _pd(_d(mesh.cell_center)),
+                               _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src, _pd(kappa), _pd(flux), _pd(source),
+                               _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols), _pd(vals), _pd(rhs))
+    else:
+        grad, red = corrected
+        rc = lib().or_assemble_scheme(mesh.dim, N, F, Fb, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
+                                      _pd(_d(mesh.face_area)), _pd(_d(mesh.face_center)),
+                                      _pd(_d(mesh.cell_center)), _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src,
+                                      _pd(kappa), _pd(flux), _pd(source), _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols),
+                                      _pd(vals), _pd(rhs), 1, _pd(_d(mesh.face_normal)), _pd(_d(grad)), float(red))
     if rc != 0:
         raise RuntimeError(f"oracle assemble failed: {rc}")
     return ptr, cols, vals, rhs

@@ -189,3 +189,69 @@ def read_su2(text):
             i += nm
         i += 1
     return dim, nodes, elements, boundaries
+
+
+def _mat_inv(a):
+    """Matrix::inv (core/matrix.rs:320-380) on a list of rows."""
+    n = len(a)
+    a = [row[:] for row in a]
+    out = [[1.0 if i == j else 0.0 for j in range(n)] for i in range(n)]
+    for k in range(n - 1):
+        piv = a[k][k]
+        if abs(piv) < 1e-14:
+            maxi, maxp = k, abs(piv)
+            for j in range(k + 1, n):
+                pj = abs(a[k][j])
+                if pj > maxp:
+                    maxi, maxp = j, pj
+            if maxi == k:
+                raise ZeroDivisionError("singular")
+            a[k], a[maxi] = a[maxi], a[k]
+            out[k], out[maxi] = out[maxi], out[k]
+        piv = a[k][k]
+        for i in range(k + 1, n):
+            f = (-a[i][k]) / piv
+            a[i] = [a[i][j] + a[k][j] * f for j in range(n)]
+            out[i] = [out[i][j] + out[k][j] * f for j in range(n)]
+    for k in range(n):
+        piv = a[k][k]
+        if abs(piv) < 1e-14:
+            raise ZeroDivisionError("singular")
+        a[k] = [v / piv for v in a[k]]
+        out[k] = [v / piv for v in out[k]]
+    for k in range(n - 1, 0, -1):
+        piv = a[k][k]
+        for i in range(k):
+            f = (-a[i][k]) / piv
+            a[i] = [a[i][j] + a[k][j] * f for j in range(n)]
+            out[i] = [out[i][j] + out[k][j] * f for j in range(n)]
+    return out
+
+
+def grad_coeffs(dim, cell_face_ptr, cell_faces, face_owner, face_neighbor, face_center, cell_center):
+    """Gradient coefficients of Mesh::compute (core/mesh/compute.rs:155-203):
+    per cell-face entry (mesh order) and per cell, as lists of vectors."""
+    gco, gdg = [], []
+    for c in range(len(cell_face_ptr) - 1):
+        xc = cell_center[c]
+        dg = []
+        for k in range(cell_face_ptr[c], cell_face_ptr[c + 1]):
+            f = cell_faces[k]
+            if face_neighbor[f] < 0:
+                p = face_center[f]
+            else:
+                p = cell_center[face_owner[f] if face_neighbor[f] == c else face_neighbor[f]]
+            dg.append([p[d] - xc[d] for d in range(dim)])
+        g = [[0.0] * dim for _ in range(dim)]
+        for v in dg:
+            for i in range(dim):
+                for j in range(dim):
+                    g[i][j] += v[i] * v[j]
+        gi = _mat_inv(g)
+        own = [0.0] * dim
+        for v in dg:
+            w = [_dot(gi[i], v) for i in range(dim)]
+            gco.append(w)
+            own = [own[i] - w[i] for i in range(dim)]
+        gdg.append(own)
+    return gco, gdg

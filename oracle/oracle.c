@@ -22,7 +22,11 @@
  *   terms ............... src/fvm/terms/{laplacian.rs:35-45,convection.rs:36-45,
  *                          source.rs:34-40,operations.rs:86-199}
  *   schemes ............. src/fvm/schemes/facengrad/orthogonal.rs:26-46,
+ *                          src/fvm/schemes/facengrad/corrected.rs:36-67,
  *                          src/fvm/schemes/faceinterp/upwind.rs:26-33
+ *   gradients ........... src/core/mesh/compute.rs:155-203 (coefficients),
+ *                          src/core/matrix.rs:320-380 (Matrix::inv),
+ *                          src/fvm/tools/gradients.rs:48-86 (compute_gradients)
  *   CSR ................. src/linalg/dmatrix.rs:38-50 (pattern), 136-146 (imul),
  *                          262-286 (Index by binary search), 76-88 (is_symmetric)
  *   dot ................. src/linalg/dvector.rs:63-79
@@ -116,11 +120,69 @@ int or_pattern(int64_t n_cells, const int32_t *cell_face_ptr, const int32_t *cel
  * A face value is conv*c_conv + lap*c_lap; with c in {-1,0,1} this is the one
  * rounding the reference performs for `conv - lap`, `-lap`, etc.
  */
+/* Face-normal gradient scheme of the laplacian for face f with owner centre
+ * ci and other point cj (neighbour centre, or face centre on the boundary):
+ * Orthogonal (facengrad/orthogonal.rs:26-46): t = 1/|cj - ci|, no rhs;
+ * Corrected (facengrad/corrected.rs:36-67): t = 1/(n.d), rhs = explicit
+ * correction gf.(n - t d) * reduction, gf interpolated with
+ * w = (x_f - ci).n / (d.n) on interior faces, the owner's gradient on
+ * boundary faces. */
+static double dotv(int dim, const double *a, const double *b) {
+    double x = 0.0;
+    for (int d = 0; d < dim; ++d) x += a[d] * b[d];
+    return x;
+}
+
+static void scheme_terms(int32_t dim, int scheme, int64_t f, int64_t i, int64_t j, const double *ci,
+                         const double *cj, const double *face_center, const double *face_normal,
+                         const double *grad, double red, double *t_out, double *rsch_out) {
+    double dvec[3];
+    for (int d = 0; d < dim; ++d) dvec[d] = cj[d] - ci[d];
+    if (scheme == 0) {
+        *t_out = 1.0 / sqrt(dotv(dim, dvec, dvec));
+        *rsch_out = 0.0;
+        return;
+    }
+    const double *n = face_normal + f * dim;
+    const double c_corr = 1.0 / dotv(dim, n, dvec);
+    double v[3], gf[3];
+    for (int d = 0; d < dim; ++d) v[d] = n[d] - c_corr * dvec[d];
+    if (j >= 0) {
+        double e[3];
+        const double *xf = face_center + f * dim;
+        for (int d = 0; d < dim; ++d) e[d] = xf[d] - ci[d];
+        const double w = dotv(dim, e, n) / dotv(dim, dvec, n);
+        for (int d = 0; d < dim; ++d) gf[d] = grad[i * dim + d] * (1.0 - w) + grad[j * dim + d] * w;
+    } else {
+        for (int d = 0; d < dim; ++d) gf[d] = grad[i * dim + d];
+    }
+    *t_out = c_corr;
+    *rsch_out = dotv(dim, gf, v) * red;
+}
+
+int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                       const int32_t *neighbor, const double *area, const double *face_center,
+                       const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
+                       const double *kappa, const double *flux, const double *source, const double *bndi,
+                       const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
+                       int scheme, const double *face_normal, const double *grad, double red);
+
 int or_assemble(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
                 const int32_t *neighbor, const double *area, const double *face_center,
                 const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
                 const double *kappa, const double *flux, const double *source, const double *bndi,
                 const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs) {
+    return or_assemble_scheme(dim, n_cells, n_faces, n_bfaces, owner, neighbor, area, face_center, cell_center,
+                              volume, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, row_ptr, cols, vals,
+                              rhs, 0, NULL, NULL, 0.0);
+}
+
+int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                       const int32_t *neighbor, const double *area, const double *face_center,
+                       const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
+                       const double *kappa, const double *flux, const double *source, const double *bndi,
+                       const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
+                       int scheme, const double *face_normal, const double *grad, double red) {
     const int64_t nnz = row_ptr[n_cells];
     const int64_t fb0 = n_faces - n_bfaces;
     for (int64_t k = 0; k < nnz; ++k) vals[k] = 0.0;
@@ -139,17 +201,13 @@ int or_assemble(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces,
         const int64_t j = neighbor[f];
         const double *ci = cell_center + i * dim;
         const double *cj = j >= 0 ? cell_center + j * dim : face_center + f * dim;
-        double d2 = 0.0;
-        for (int d = 0; d < dim; ++d) {
-            double dd = cj[d] - ci[d];
-            d2 += dd * dd;
-        }
-        const double dx = sqrt(d2);
-        const double t = 1.0 / dx;
-        double lap0 = 0.0, lap1 = 0.0, conv0 = 0.0, conv1 = 0.0;
+        double t, rsch;
+        scheme_terms(dim, c_lap != 0.0 ? scheme : 0, f, i, j, ci, cj, face_center, face_normal, grad, red, &t, &rsch);
+        double lap0 = 0.0, lap1 = 0.0, lap_r = 0.0, conv0 = 0.0, conv1 = 0.0;
         if (c_lap != 0.0) {
             lap0 = kappa[f] * (-t);
             lap1 = kappa[f] * t;
+            lap_r = -(kappa[f] * rsch); /* laplacian.rs:35-45 */
         }
         if (c_conv != 0.0) {
             const double F = flux[f];
@@ -172,7 +230,9 @@ int or_assemble(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces,
             li = c_conv * conv0;
             lj = c_conv * conv1;
         }
-        const double r = 0.0;
+        /* face rhs: only the Corrected laplacian has one; combined as li/lj */
+        double r = 0.0;
+        if (scheme == 1 && c_lap != 0.0) r = c_conv != 0.0 ? c_conv * 0.0 + c_lap * lap_r : c_lap * lap_r;
         li = li * area[f];
         lj = lj * area[f];
         const double ra = r * area[f];
@@ -199,6 +259,127 @@ int or_assemble(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces,
         }
     }
     return OR_OK;
+}
+
+/* ------------------------------------------------------------ gradients */
+/* Matrix::inv (core/matrix.rs:320-380): Gauss-Jordan; a pivot below 1e-14
+ * is swapped with the row given by the largest entry of the pivot row. */
+static int mat_inv(int n, double a[3][3], double out[3][3]) {
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) out[i][j] = i == j ? 1.0 : 0.0;
+    for (int k = 0; k < n - 1; ++k) {
+        double piv = a[k][k];
+        if (fabs(piv) < 1e-14) {
+            int maxi = k;
+            double maxp = fabs(piv);
+            for (int j = k + 1; j < n; ++j) {
+                double pj = fabs(a[k][j]);
+                if (pj > maxp) {
+                    maxi = j;
+                    maxp = pj;
+                }
+            }
+            if (maxi == k) return OR_ERR_INVALID;
+            for (int j = 0; j < n; ++j) {
+                double t = a[k][j];
+                a[k][j] = a[maxi][j];
+                a[maxi][j] = t;
+                t = out[k][j];
+                out[k][j] = out[maxi][j];
+                out[maxi][j] = t;
+            }
+        }
+        piv = a[k][k];
+        for (int i = k + 1; i < n; ++i) {
+            const double f = (-a[i][k]) / piv;
+            for (int j = 0; j < n; ++j) {
+                a[i][j] += a[k][j] * f;
+                out[i][j] += out[k][j] * f;
+            }
+        }
+    }
+    for (int k = 0; k < n; ++k) {
+        const double piv = a[k][k];
+        if (fabs(piv) < 1e-14) return OR_ERR_INVALID;
+        for (int j = 0; j < n; ++j) {
+            a[k][j] /= piv;
+            out[k][j] /= piv;
+        }
+    }
+    for (int k = n - 1; k >= 1; --k) {
+        const double piv = a[k][k];
+        for (int i = 0; i < k; ++i) {
+            const double f = (-a[i][k]) / piv;
+            for (int j = 0; j < n; ++j) {
+                a[i][j] += a[k][j] * f;
+                out[i][j] += out[k][j] * f;
+            }
+        }
+    }
+    return OR_OK;
+}
+
+static void grad_dgc(int dim, int64_t c, int32_t f, const int32_t *owner, const int32_t *neighbor,
+                     const double *face_center, const double *cell_center, double *dgc) {
+    const double *p;
+    if (neighbor[f] < 0) {
+        p = face_center + (int64_t)f * dim;
+    } else {
+        const int64_t co = neighbor[f] == c ? owner[f] : neighbor[f];
+        p = cell_center + co * dim;
+    }
+    for (int d = 0; d < dim; ++d) dgc[d] = p[d] - cell_center[c * dim + d];
+}
+
+/* Gradient coefficients of Mesh::compute (core/mesh/compute.rs:155-203):
+ * G = sum_k dgc_k dgc_k^T over the cell's faces in mesh order, g_k = G^-1 dgc_k,
+ * own = -sum_k g_k. */
+int or_grad_coeffs(int32_t dim, int64_t n_cells, const int32_t *owner, const int32_t *neighbor,
+                   const double *face_center, const double *cell_center, const int32_t *cf_ptr,
+                   const int32_t *cf, double *gcoef, double *gdiag) {
+    for (int64_t c = 0; c < n_cells; ++c) {
+        double g[3][3] = {{0}}, gi[3][3], dgc[3];
+        for (int32_t k = cf_ptr[c]; k < cf_ptr[c + 1]; ++k) {
+            grad_dgc(dim, c, cf[k], owner, neighbor, face_center, cell_center, dgc);
+            for (int i = 0; i < dim; ++i)
+                for (int j = 0; j < dim; ++j) g[i][j] += dgc[i] * dgc[j];
+        }
+        if (mat_inv(dim, g, gi) != OR_OK) return OR_ERR_INVALID;
+        double own[3] = {0.0, 0.0, 0.0};
+        for (int32_t k = cf_ptr[c]; k < cf_ptr[c + 1]; ++k) {
+            grad_dgc(dim, c, cf[k], owner, neighbor, face_center, cell_center, dgc);
+            for (int i = 0; i < dim; ++i) {
+                double x = 0.0;
+                for (int j = 0; j < dim; ++j) x += gi[i][j] * dgc[j];
+                gcoef[(int64_t)k * dim + i] = x;
+                own[i] -= x;
+            }
+        }
+        for (int i = 0; i < dim; ++i) gdiag[c * dim + i] = own[i];
+    }
+    return OR_OK;
+}
+
+/* compute_gradients (fvm/tools/gradients.rs:48-86) of a scalar cell field. */
+void or_gradients(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                  const int32_t *neighbor, const int32_t *cf_ptr, const int32_t *cf, const double *gcoef,
+                  const double *gdiag, const double *values, const double *bndi, const double *bnde,
+                  double *grad) {
+    const int64_t fb0 = n_faces - n_bfaces;
+    for (int64_t c = 0; c < n_cells; ++c) {
+        double g[3];
+        for (int d = 0; d < dim; ++d) g[d] = values[c] * gdiag[c * dim + d];
+        for (int32_t k = cf_ptr[c]; k < cf_ptr[c + 1]; ++k) {
+            const int32_t f = cf[k];
+            double w;
+            if (neighbor[f] >= 0)
+                w = values[neighbor[f] == c ? owner[f] : neighbor[f]];
+            else
+                w = bndi[f - fb0] * values[c] + bnde[f - fb0];
+            for (int d = 0; d < dim; ++d) g[d] += w * gcoef[(int64_t)k * dim + d];
+        }
+        for (int d = 0; d < dim; ++d) grad[c * dim + d] = g[d];
+    }
 }
 
 /* ------------------------------------------------------------- SpMV / dot */
