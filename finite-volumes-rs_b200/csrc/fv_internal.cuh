@@ -77,6 +77,17 @@ struct fv_mesh {
 
 struct fv_symbolic;  // triangular split + level schedules of a pattern (fv_precond.cu)
 
+// Level-k fill patterns of the reference (fv_fill.cu).  From the host CSR
+// pattern of A (sorted rows with diagonal), the sorted pattern of the factor
+// and, for every entry of A, its position in that pattern.
+//   kind 2 (ILU): row i = row_i_l_sparsity ∪ {i} ∪ row_i_u_sparsity
+//                 (incomplete_lower_upper.rs:30-137)
+//   kind 1 (IC):  row i = entries of A ∪ the level-ball of i
+//                 (incomplete_cholesky.rs:35-85, 148-192); fill[k] marks fill
+bool fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
+                     std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
+                     std::vector<uint8_t> &fill);
+
 // Box tiling of one sweep direction (fv_tiles.cu): boxes in dispatch order,
 // each a run of steps (rows of one level, at most 32); trow lists the rows in
 // that order; dsrc[k] (aligned with the swept side's entries) is the column j
@@ -108,6 +119,11 @@ struct fv_csr {
     int32_t *cols = nullptr;      // device
     double *vals = nullptr;       // device
     bool owns_pattern = true;     // false when the pattern belongs to an fv_mesh
+    // IC(k) fill patterns: per stored entry, 1 when it is fill (not in the
+    // matrix it was built from); the backward sweep then visits a row's
+    // entries of the matrix first and its fill after them, as the reference
+    // does (incomplete_cholesky.rs:167-192, 235-244).  Empty otherwise.
+    std::vector<uint8_t> fill_mask;
     const fv_mesh *mesh = nullptr;
     fv_symbolic *sym = nullptr;   // cached symbolic analysis (value independent)
 };

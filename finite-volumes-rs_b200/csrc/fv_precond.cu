@@ -82,6 +82,13 @@ struct fv_precond {
     int64_t n_dropped = 0;
     // FP32 copies of the factors for mixed-precision inner solves
     float *l32 = nullptr, *u32 = nullptr, *dinv32 = nullptr, *tmp32 = nullptr;
+    // level k >= 1 with fill: the factorised matrix is `fill` (the pattern of
+    // the level-k factor holding the values of `orig`, zeros elsewhere);
+    // amap[k] is the position of orig's entry k in it
+    fv_csr *fill = nullptr;
+    const fv_csr *orig = nullptr;
+    int32_t *amap = nullptr;
+    int level = 0;
 };
 
 // ------------------------------------------------------------------ symbolic
@@ -128,12 +135,18 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     s->nnz_u = nu;
     s->max_row = maxrow;
     std::vector<int32_t> lc((size_t)(nl ? nl : 1)), uc((size_t)(nu ? nu : 1));
+    const bool fill_order = !A->fill_mask.empty();
     for (int64_t i = 0; i < n; ++i) {
         int32_t a = lp[i], b = up[i];
         for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k) {
             if (col[k] < i) lc[a++] = col[k];
-            if (col[k] > i) uc[b++] = col[k];
+            if (col[k] > i && !(fill_order && A->fill_mask[k])) uc[b++] = col[k];
         }
+        // IC(k) fill: a row's fill entries come after the matrix's own entries
+        // in the backward sweep (the reference's sp_t order)
+        if (fill_order)
+            for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                if (col[k] > i && A->fill_mask[k]) uc[b++] = col[k];
     }
     // level schedules (stable: rows of a level keep ascending order)
     auto schedule = [&](bool upper, std::vector<int32_t> &level, std::vector<int32_t> &order) -> int32_t {
@@ -170,8 +183,15 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     for (int64_t i = 0; i < n && sym; ++i)
         for (int32_t k = lp[i]; k < lp[i + 1]; ++k) {
             int32_t j = lc[k];
-            int32_t p = cur[j]++;
-            if (p >= up[j + 1] || uc[p] != i) {
+            int32_t p = -1;
+            if (!fill_order) {  // U rows ascending: the entries of row j appear in order of i
+                p = cur[j]++;
+                if (p >= up[j + 1] || uc[p] != i) p = -1;
+            } else {
+                for (int32_t t = up[j]; t < up[j + 1]; ++t)
+                    if (uc[t] == i) p = t;
+            }
+            if (p < 0) {
                 sym = false;
                 break;
             }
@@ -833,7 +853,10 @@ extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     cudaFree(P->u32);
     cudaFree(P->dinv32);
     cudaFree(P->tmp32);
+    cudaFree(P->amap);
+    fv_csr *F = P->fill;
     delete P;
+    if (F) fv_csr_destroy(F);
     return FV_OK;
 }
 
@@ -879,7 +902,7 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
         return FV_ERR_INVALID;
     }
     const int64_t n = P->n;
-    if (kind == 1) {
+    if (kind == 1 && A->fill_mask.empty()) {  // a fill pattern: checked on the matrix it came from
         FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
         fv_note_launch(), k_check_symmetric<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, A->row_ptr, A->vals, sym->l_ptr, sym->l_col,
                                                                       sym->u_ptr, sym->l_tpos, P->err);
@@ -945,6 +968,121 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
     return FV_OK;
 }
 
+namespace {
+__global__ void k_scatter_vals(int64_t nnz, const int32_t *__restrict__ amap, const double *__restrict__ a,
+                               double *__restrict__ f) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+        f[amap[k]] = a[k];
+}
+}  // namespace
+
+// is_symmetric (dmatrix.rs:76-88) of a matrix, as IncompleteCholesky::build asserts it
+static fv_status check_symmetric(fv_csr *A, cudaStream_t st) {
+    fv_symbolic *sym = nullptr;
+    FV_TRY(fv_get_symbolic(A, st, &sym));
+    if (!sym->symmetric_pattern) return FV_ERR_NOT_SYMMETRIC;
+    int *bad = nullptr;
+    FV_CUDA_TRY(fv_malloc_async(&bad, sizeof(int), st));
+    FV_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+    const int64_t n = A->nrows;
+    fv_note_launch(), k_check_symmetric<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+                          n, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->u_ptr, sym->l_tpos, bad);
+    FV_CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    FV_CUDA_TRY(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaFreeAsync(bad, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    return h ? FV_ERR_NOT_SYMMETRIC : FV_OK;
+}
+
+// Scatter the values of P->orig into the fill pattern.
+static fv_status scatter_fill(fv_precond *P, cudaStream_t st) {
+    fv_csr *F = P->fill;
+    FV_CUDA_TRY(cudaMemsetAsync(F->vals, 0, sizeof(double) * (F->nnz ? F->nnz : 1), st));
+    if (P->orig->nnz) {
+        fv_note_launch(), k_scatter_vals<<<592, 256, 0, st>>>(P->orig->nnz, P->amap, P->orig->vals, F->vals);
+        FV_CUDA_TRY(cudaGetLastError());
+    }
+    return FV_OK;
+}
+
+// IC(k) / ILU(k) with fill (k >= 1; IC(1) has the pattern of A, see fv_ic_factor).
+static fv_status fill_factor(const fv_csr *Ac, int kind, int level, cudaStream_t st, fv_precond **out) {
+    fv_csr *A = const_cast<fv_csr *>(Ac);
+    if (A->nrows != A->ncols) return FV_ERR_INVALID;
+    if (kind == 1) FV_TRY(check_symmetric(A, st));
+    const int64_t n = A->nrows, nnz = A->nnz;
+    std::vector<int32_t> ptr((size_t)n + 1), col((size_t)(nnz ? nnz : 1));
+    FV_CUDA_TRY(cudaMemcpyAsync(ptr.data(), A->row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    if (nnz) FV_CUDA_TRY(cudaMemcpyAsync(col.data(), A->cols, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int32_t> fptr, fcol, amap;
+    std::vector<uint8_t> fill;
+    if (!fv_fill_pattern(kind, level, n, ptr.data(), col.data(), fptr, fcol, amap, fill)) return FV_ERR_UNSUPPORTED;
+    fv_csr *F = new fv_csr();
+    F->nrows = F->ncols = n;
+    F->nnz = (int64_t)fcol.size();
+    if (kind == 1) F->fill_mask = std::move(fill);
+    int32_t *damap = nullptr;
+    cudaError_t e = cudaMalloc(&F->row_ptr, sizeof(int32_t) * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&F->cols, sizeof(int32_t) * (F->nnz ? F->nnz : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&F->vals, sizeof(double) * (F->nnz ? F->nnz : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&damap, sizeof(int32_t) * (nnz ? nnz : 1));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(F->row_ptr, fptr.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && F->nnz)
+        e = cudaMemcpyAsync(F->cols, fcol.data(), sizeof(int32_t) * F->nnz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nnz)
+        e = cudaMemcpyAsync(damap, amap.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "fill pattern upload");
+        cudaFree(damap);
+        fv_csr_destroy(F);
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    fv_precond tmp;  // scatter through a stand-in so the values are in place before factorising
+    tmp.fill = F;
+    tmp.orig = A;
+    tmp.amap = damap;
+    fv_status s = scatter_fill(&tmp, st);
+    tmp.fill = nullptr;
+    tmp.amap = nullptr;
+    fv_precond *P = nullptr;
+    if (s == FV_OK) s = factor_common(F, kind, st, &P);
+    if (s != FV_OK) {
+        cudaFree(damap);
+        fv_csr_destroy(F);
+        return s;
+    }
+    P->fill = F;
+    P->orig = A;
+    P->amap = damap;
+    P->level = level;
+    *out = P;
+    return FV_OK;
+}
+
+/* IncompleteCholesky::from_matrix(A, level).  The reference's IC pattern of
+ * row i is A's row plus every node the walk of row_i_sparsity_edit pushes,
+ * i.e. the nodes within `level - 1` neighbour steps of A's neighbours; for
+ * level 1 that is A's own pattern, so IC(1) is IC(0). */
+extern "C" fv_status fv_ic_factor(const fv_csr *A, int32_t level, void *stream, fv_precond **out) {
+    if (!out || !A || level < 0) return FV_ERR_INVALID;
+    *out = nullptr;
+    if (level <= 1) return factor_common(A, 1, fv_stream(stream), out);
+    return fill_factor(A, 1, level, fv_stream(stream), out);
+}
+/* IncompleteLowerUpper::from_matrix(A, level): the factor pattern of
+ * row_i_l_sparsity / row_i_u_sparsity, then the row-by-row IKJ elimination
+ * with the drop rule of level 0 on that pattern. */
+extern "C" fv_status fv_ilu_factor(const fv_csr *A, int32_t level, void *stream, fv_precond **out) {
+    if (!out || !A || level < 0) return FV_ERR_INVALID;
+    *out = nullptr;
+    if (level == 0) return factor_common(A, 2, fv_stream(stream), out);
+    return fill_factor(A, 2, level, fv_stream(stream), out);
+}
+
 extern "C" fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out) {
     if (!out) return FV_ERR_INVALID;
     *out = nullptr;
@@ -959,7 +1097,12 @@ extern "C" fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **
 extern "C" fv_status fv_precond_refactor(fv_precond *P, void *stream) {
     if (!P) return FV_ERR_INVALID;
     fv_precond *q = P;
-    return factor_common(P->A, P->kind, fv_stream(stream), &q);
+    cudaStream_t st = fv_stream(stream);
+    if (P->fill) {  // level k: new values of the original matrix into the fill pattern
+        if (P->kind == 1) FV_TRY(check_symmetric(const_cast<fv_csr *>(P->orig), st));
+        FV_TRY(scatter_fill(P, st));
+    }
+    return factor_common(P->A, P->kind, st, &q);
 }
 
 extern "C" fv_status fv_precond_apply(fv_precond *P, const double *r, double *z, void *stream) {

@@ -122,6 +122,8 @@ _SIGS = {
     "fv_spmv_host": [vp, dp, dp, vp],
     "fv_ic0_factor": [vp, vp, P(vp)],
     "fv_ilu0_factor": [vp, vp, P(vp)],
+    "fv_ic_factor": [vp, C.c_int32, vp, P(vp)],
+    "fv_ilu_factor": [vp, C.c_int32, vp, P(vp)],
     "fv_precond_refactor": [vp, vp],
     "fv_precond_apply": [vp, vp, vp, vp],
     "fv_precond_apply_host": [vp, dp, dp, vp],

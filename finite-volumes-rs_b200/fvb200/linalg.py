@@ -281,10 +281,8 @@ class IncompleteCholesky(Preconditioner):
 
     @classmethod
     def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteCholesky":
-        if level != 0:
-            raise NotImplementedError("IC(k) with k > 0 is not implemented on the device path")
         h = C.c_void_p()
-        check(lib().fv_ic0_factor(matrix.handle, stream_handle(stream), C.byref(h)), "IncompleteCholesky")
+        check(lib().fv_ic_factor(matrix.handle, int(level), stream_handle(stream), C.byref(h)), "IncompleteCholesky")
         return cls(h, matrix.nrows(), matrix)
 
 
@@ -294,10 +292,9 @@ class IncompleteLowerUpper(Preconditioner):
 
     @classmethod
     def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteLowerUpper":
-        if level != 0:
-            raise NotImplementedError("ILU(k) with k > 0 is not implemented on the device path")
         h = C.c_void_p()
-        check(lib().fv_ilu0_factor(matrix.handle, stream_handle(stream), C.byref(h)), "IncompleteLowerUpper")
+        check(lib().fv_ilu_factor(matrix.handle, int(level), stream_handle(stream), C.byref(h)),
+              "IncompleteLowerUpper")
         return cls(h, matrix.nrows(), matrix)
 
 

@@ -223,6 +223,14 @@ fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double *y_host, vo
 /* IncompleteCholesky::from_matrix(A, 0) / IncompleteLowerUpper::from_matrix(A, 0). */
 fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out);
 fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out);
+/* IncompleteCholesky / IncompleteLowerUpper ::from_matrix(A, level) for any
+ * level (incomplete_cholesky.rs:35-85,148-205; incomplete_lower_upper.rs:
+ * 30-137,200-266): the reference's level-k patterns (depth-first walks over
+ * the matrix graph, restated in their visiting order), then the level-0
+ * numerics on that pattern with zeros at fill positions.  IC(1) has the
+ * pattern of A (the reference's walk adds no node for level 1). */
+fv_status fv_ic_factor(const fv_csr *A, int32_t level, void *stream, fv_precond **out);
+fv_status fv_ilu_factor(const fv_csr *A, int32_t level, void *stream, fv_precond **out);
 /* Value-only refactorisation of P after the values of the matrix it was built
  * from changed (same pattern, same fv_csr object); reuses the symbolic
  * analysis (triangular split, level schedules) and the factor storage. */

@@ -48,6 +48,8 @@ def lib():
             "or_spmv": ([i64, ip, ip, dp, dp, dp], None),
             "or_dot": ([i64, dp, dp], C.c_double),
             "or_ic0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
+            "or_ic_create_fill": ([i64, ip, ip, dp, P(C.c_ubyte), P(C.c_int)], vp),
+            "or_fill_pattern": ([C.c_int, C.c_int, i64, ip, ip, ip, ip, P(C.c_ubyte)], i64),
             "or_ilu0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
             "or_precond_apply": ([vp, dp, dp], None),
             "or_precond_free": ([vp], None),
@@ -168,15 +170,48 @@ def dot(a, b):
     return lib().or_dot(len(a), _pd(a), _pd(b))
 
 
-class Precond:
-    """IncompleteCholesky / IncompleteLowerUpper restated (level 0)."""
+def fill_pattern(kind, level, ptr, cols):
+    """Sorted level-k factor pattern (kind "ic" / "ilu") of the reference's
+    depth-first walks, and a 0/1 fill flag per entry."""
+    ptr, cols = _i(ptr), _i(cols)
+    n = len(ptr) - 1
+    k = 1 if kind == "ic" else 2
+    tot = lib().or_fill_pattern(k, int(level), n, _pi(ptr), _pi(cols), None, None, None)
+    fptr = np.zeros(n + 1, np.int32)
+    fcol = np.zeros(max(tot, 1), np.int32)
+    fill = np.zeros(max(tot, 1), np.uint8)
+    lib().or_fill_pattern(k, int(level), n, _pi(ptr), _pi(cols), _pi(fptr), _pi(fcol),
+                          fill.ctypes.data_as(P(C.c_ubyte)))
+    return fptr, fcol[:tot], fill[:tot]
 
-    def __init__(self, kind, ptr, cols, vals):
+
+class Precond:
+    """IncompleteCholesky / IncompleteLowerUpper restated.  level >= 1: the
+    level-0 numerics on the level-k pattern with zeros at fill positions (IC
+    sums a row's fill entries after its matrix entries in the backward sweep,
+    as the reference's sp_t does)."""
+
+    def __init__(self, kind, ptr, cols, vals, level=0):
         self.n = len(ptr) - 1
-        self._keep = (_i(ptr), _i(cols), _d(vals))
         st = C.c_int()
-        f = lib().or_ic0_create if kind == "ic" else lib().or_ilu0_create
-        self.h = f(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]), C.byref(st))
+        fill = None
+        if level > 0 and not (kind == "ic" and level == 1):
+            fptr, fcol, fill = fill_pattern(kind, level, ptr, cols)
+            fv_ = np.zeros(len(fcol))
+            ptr_, cols_, vals_ = _i(ptr), _i(cols), _d(vals)
+            for i in range(self.n):
+                a0, a1, f0, f1 = ptr_[i], ptr_[i + 1], fptr[i], fptr[i + 1]
+                pos = np.searchsorted(fcol[f0:f1], cols_[a0:a1]) + f0
+                fv_[pos] = vals_[a0:a1]
+            ptr, cols, vals = fptr, fcol, fv_
+        self._keep = (_i(ptr), _i(cols), _d(vals), fill)
+        if kind == "ic":
+            fl = fill.ctypes.data_as(P(C.c_ubyte)) if fill is not None else None
+            self.h = lib().or_ic_create_fill(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]),
+                                             fl, C.byref(st))
+        else:
+            self.h = lib().or_ilu0_create(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]),
+                                          C.byref(st))
         self.status = st.value
         self.kind = kind
 

@@ -382,6 +382,96 @@ void or_gradients(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bface
     }
 }
 
+/* -------------------------------------------------------- level-k patterns */
+/* The depth-first walks of the reference's level-k patterns: a stack (last
+ * pushed first), a visited mark per walk, a path length per pushed node.
+ *   mode 0: row_i_u_sparsity (incomplete_lower_upper.rs:30-83)
+ *   mode 1: row_i_l_sparsity (incomplete_lower_upper.rs:86-137)
+ *   mode 2: row_i_sparsity_edit (incomplete_cholesky.rs:35-85)
+ * Appends the nodes the walk collects to out (unsorted), returns their count. */
+static int64_t level_walk(int mode, int64_t i, int level, const int32_t *ptr, const int32_t *col, int64_t *mark,
+                          int64_t tag, int32_t *dist, int32_t *stack, int32_t *out) {
+    int64_t top = 0, cnt = 0;
+    stack[top++] = (int32_t)i;
+    mark[i] = tag;
+    dist[i] = 0;
+    while (top > 0) {
+        int32_t k = stack[--top];
+        int32_t lk = dist[k];
+        for (int32_t t = ptr[k]; t < ptr[k + 1]; ++t) {
+            int32_t j = col[t];
+            if (j == k || mark[j] == tag) continue;
+            mark[j] = tag;
+            if (mode == 2) {
+                if (lk < level) {
+                    stack[top++] = j;
+                    dist[j] = lk + 1;
+                    out[cnt++] = j;
+                }
+            } else if (mode == 0) {
+                if (j < i && lk < level) {
+                    stack[top++] = j;
+                    dist[j] = lk + 1;
+                } else if (j > i) {
+                    out[cnt++] = j;
+                }
+            } else {
+                if (j > i && lk < level) {
+                    stack[top++] = j;
+                    dist[j] = lk + 1;
+                } else if (j < i) {
+                    out[cnt++] = j;
+                }
+            }
+        }
+    }
+    return cnt;
+}
+
+/* Sorted pattern of the level-k factor (kind 1 = IC, 2 = ILU) of the
+ * pattern (ptr, col): two calls, the first with fptr/fcol/fill NULL returns
+ * the entry count.  fill[k] = 1 for entries not in the input pattern. */
+int64_t or_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col, int32_t *fptr,
+                        int32_t *fcol, unsigned char *fill) {
+    int64_t *mark = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+    int32_t *dist = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n ? n : 1));
+    int32_t *stack = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n ? n : 1));
+    int32_t *row = (int32_t *)malloc(sizeof(int32_t) * (size_t)(2 * n + 2));
+    for (int64_t i = 0; i < n; ++i) mark[i] = -1;
+    int64_t total = 0;
+    if (fptr) fptr[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t m = 0;
+        if (kind == 2) {
+            m += level_walk(1, i, level, ptr, col, mark, 2 * i, dist, stack, row + m);
+            row[m++] = (int32_t)i;
+            m += level_walk(0, i, level, ptr, col, mark, 2 * i + 1, dist, stack, row + m);
+        } else {
+            m += level_walk(2, i, level, ptr, col, mark, 2 * i, dist, stack, row + m);
+            for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) row[m++] = col[t];
+        }
+        qsort(row, (size_t)m, sizeof(int32_t), cmp_i32);
+        int64_t u = 0;
+        for (int64_t q = 0; q < m; ++q)
+            if (q == 0 || row[q] != row[q - 1]) row[u++] = row[q];
+        if (fcol) {
+            for (int64_t q = 0; q < u; ++q) {
+                fcol[total + q] = row[q];
+                int in_a = 0;
+                for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) in_a |= col[t] == row[q];
+                fill[total + q] = (unsigned char)!in_a;
+            }
+            fptr[i + 1] = (int32_t)(total + u);
+        }
+        total += u;
+    }
+    free(mark);
+    free(dist);
+    free(stack);
+    free(row);
+    return total;
+}
+
 /* ------------------------------------------------------------- SpMV / dot */
 void or_spmv(int64_t n, const int32_t *ptr, const int32_t *col, const double *val, const double *x, double *y) {
     for (int64_t i = 0; i < n; ++i) {
@@ -444,7 +534,18 @@ static int is_symmetric(int64_t n, const int32_t *ptr, const int32_t *col, const
 
 /* IncompleteCholesky::from_matrix(A, 0): build (incomplete_cholesky.rs:148-202)
  * and compute (:87-145).  Level 0 adds no fill. */
+or_precond *or_ic_create_fill(int64_t n, const int32_t *ptr, const int32_t *col, const double *val,
+                              const unsigned char *fill, int *status);
 or_precond *or_ic0_create(int64_t n, const int32_t *ptr, const int32_t *col, const double *val, int *status) {
+    return or_ic_create_fill(n, ptr, col, val, NULL, status);
+}
+
+/* IncompleteCholesky::build + compute on a (possibly filled) sorted pattern.
+ * fill[k] = 1 marks entries that are fill (zeros, not entries of the
+ * matrix): sp_t lists a row's matrix entries first and its fill after them
+ * (incomplete_cholesky.rs:167-192), which is the order the backward sweep sums in. */
+or_precond *or_ic_create_fill(int64_t n, const int32_t *ptr, const int32_t *col, const double *val,
+                              const unsigned char *fill, int *status) {
     *status = OR_OK;
     if (!is_symmetric(n, ptr, col, val)) {
         *status = OR_ERR_NOT_SYMMETRIC;
@@ -477,8 +578,11 @@ or_precond *or_ic0_create(int64_t n, const int32_t *ptr, const int32_t *col, con
                 p->l.col[a] = j;
                 p->l.val[a++] = val[k];
             }
-            if (j >= i) p->spt_col[b++] = j;
+            if (j >= i && !(fill && fill[k])) p->spt_col[b++] = j;
         }
+        if (fill)
+            for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                if (col[k] >= i && fill[k]) p->spt_col[b++] = col[k];
     }
     p->l.ptr[n] = (int32_t)a;
     p->spt_ptr[n] = (int32_t)b;
