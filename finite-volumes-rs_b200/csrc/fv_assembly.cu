@@ -79,7 +79,60 @@ struct AssembleArgs {
     const double4 *fnorm, *fcen;
     const double *grad;
     double red;
+    // time derivative, linear source, divergence
+    double c_time, dt, a_next, a_last, a_last_2;
+    int time_scheme;
+    const double *prev, *prev2, *dens, *densp, *densp2;
+    double c_lin, c_div;
+    const double *lin, *divflux;
 };
+
+// Cell terms of the expression (assembly.rs:26-32): lhs and rhs per unit
+// volume.  At most two terms carry a nonzero cell value on each side, so the
+// coefficient form equals the term tree's evaluation in any order.
+__device__ __forceinline__ void cell_terms(const AssembleArgs &a, int64_t i, double srci, double &l, double &r) {
+    double tl = 0.0, tr = 0.0;
+    if (a.c_time != 0.0) {
+        if (a.time_scheme == FV_TIME_EULER) {  // schemes/time/euler.rs
+            const double r0 = a.dens ? a.dens[i] : 1.0, r1 = a.dens ? a.densp[i] : 1.0;
+            tl = 1.0 * (1.0 / a.dt) * r0;
+            tr = a.prev[i] / a.dt * r1;
+        } else {  // schemes/time/backward.rs
+            const double r0 = a.dens ? a.dens[i] : 1.0, r1 = a.dens ? a.densp[i] : 1.0,
+                         r2 = a.dens ? a.densp2[i] : 1.0;
+            tl = 1.0 * (a.a_next / a.dt) * r0;
+            tr = (a.prev[i] * a.a_last * r1 - a.prev2[i] * a.a_last_2 * r2) / a.dt;
+        }
+    }
+    const double ll = a.c_lin != 0.0 ? a.lin[i] : 0.0;
+    if (a.c_time != 0.0 && a.c_lin != 0.0)
+        l = a.c_time * tl + a.c_lin * ll;
+    else if (a.c_time != 0.0)
+        l = a.c_time * tl;
+    else if (a.c_lin != 0.0)
+        l = a.c_lin * ll;
+    else
+        l = 0.0;
+    const double sr = -srci;  // Source::cell_terms rhs
+    if (a.c_time != 0.0 && a.c_src != 0.0)
+        r = a.c_time * tr + a.c_src * sr;
+    else if (a.c_time != 0.0)
+        r = a.c_time * tr;
+    else if (a.c_src != 0.0)
+        r = a.c_src * sr;
+    else
+        r = 0.0;
+}
+
+// Face rhs of the expression: the Corrected laplacian's -(kappa * explicit)
+// (lap_r) and the divergence's -F, combined like li / lj.
+__device__ __forceinline__ double face_rhs(const AssembleArgs &a, bool corr, double lap_r, int f) {
+    const bool has_div = a.c_div != 0.0;
+    if (corr && has_div) return a.c_lap * lap_r + a.c_div * (-a.divflux[f]);
+    if (corr) return (a.c_conv != 0.0) ? a.c_conv * 0.0 + a.c_lap * lap_r : a.c_lap * lap_r;
+    if (has_div) return a.c_div * (-a.divflux[f]);
+    return 0.0;
+}
 
 // Face coefficients (li, lj) before the area factor, exactly as the
 // reference's term tree evaluates them.
@@ -295,9 +348,8 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
         if (c[q] == (int)i) pd = q;
     const double4 ci4 = a.cell[i];
     const double V = ci4.w;
-    // cell loop (assembly.rs:26-32): no term in scope carries a cell lhs
-    const double lcell = 0.0;
-    const double rcell = a.c_src != 0.0 ? a.c_src * (-a.src[i]) : 0.0;
+    double lcell, rcell;  // cell loop (assembly.rs:26-32)
+    cell_terms(a, i, a.c_src != 0.0 ? a.src[i] : 0.0, lcell, rcell);
     double diag = lcell * V;
     double rhs = rcell * V;
     for (int k = s; k < e; ++k) {
@@ -338,7 +390,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
         const double A = a.area[f];
         li = li * A;
         lj = lj * A;
-        const double ra = 0.0 * A;
+        const double ra = face_rhs(a, false, 0.0, f) * A;
         if (j < 0) {
             const double bi = a.bndi[f - a.fb0], be = a.bnde[f - a.fb0];
             diag += li;
@@ -435,8 +487,8 @@ __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(A
         pd += (f1 && jj[k] < (int)i) ? 1 : 0;
     }
     const double V = ci4.w;
-    const double lcell = 0.0;
-    const double rcell = a.c_src != 0.0 ? a.c_src * (-srci) : 0.0;
+    double lcell = 0.0, rcell = 0.0;  // cell loop (assembly.rs:26-32)
+    if (live) cell_terms(a, i, srci, lcell, rcell);
     double diag = lcell * V;
     double rhs = rcell * V;
     double acc[MAXF];
@@ -510,11 +562,8 @@ __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(A
             const double A = ar[k];
             li = li * A;
             lj = lj * A;
-            double r = 0.0;
-            if (CORR) {  // laplacian rhs -(kappa * explicit), combined like li/lj
-                const double lap_r = -(kp[k] * rsch);
-                r = (a.c_conv != 0.0) ? a.c_conv * 0.0 + a.c_lap * lap_r : a.c_lap * lap_r;
-            }
+            // face rhs: the Corrected laplacian's -(kappa * explicit), the divergence's -F
+            const double r = face_rhs(a, CORR, CORR ? -(kp[k] * rsch) : 0.0, fe[k] & 0x7fffffff);
             const double ra = r * A;
             if (jj[k] < 0) {
                 const int fb = (fe[k] & 0x7fffffff) - (int)a.fb0;
@@ -925,6 +974,32 @@ extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const f
     args.fcen = m->face_center;
     args.grad = nullptr;
     args.red = terms->corrector_reduction;
+    args.c_time = terms->time_coef;
+    args.time_scheme = terms->time_scheme;
+    args.dt = terms->dt;
+    args.prev = terms->previous;
+    args.prev2 = terms->previous_2;
+    args.dens = terms->density;
+    args.densp = terms->density_previous;
+    args.densp2 = terms->density_previous_2;
+    args.c_lin = terms->linear_source_coef;
+    args.lin = terms->linear_source;
+    args.c_div = terms->divergence_coef;
+    args.divflux = terms->divergence_flux;
+    args.a_next = args.a_last = args.a_last_2 = 0.0;
+    if (args.c_time != 0.0) {
+        if ((args.time_scheme != FV_TIME_EULER && args.time_scheme != FV_TIME_BACKWARD) || !args.prev ||
+            !(args.dt != 0.0) || (args.time_scheme == FV_TIME_BACKWARD && (!args.prev2 || !(terms->dt_2 != 0.0))) ||
+            (args.dens && (!args.densp || (args.time_scheme == FV_TIME_BACKWARD && !args.densp2))))
+            return FV_ERR_INVALID;
+        if (args.time_scheme == FV_TIME_BACKWARD) {  // Backward::new (backward.rs:23-28); powi(2) is x*x
+            const double wn = terms->dt / terms->dt_2;
+            args.a_next = (1.0 + 2.0 * wn) / (1.0 + wn);
+            args.a_last = ((1.0 + wn) * (1.0 + wn)) / (1.0 + wn);
+            args.a_last_2 = (wn * wn) / (1.0 + wn);
+        }
+    }
+    if ((args.c_lin != 0.0 && !args.lin) || (args.c_div != 0.0 && !args.divflux)) return FV_ERR_INVALID;
     if (terms->scheme == FV_SCHEME_CORRECTED && terms->laplacian_coef != 0.0) {
         if (!m->face_normal || !m->cf_pad) return FV_ERR_UNSUPPORTED;
         if (!terms->gradients) return FV_ERR_INVALID;
@@ -958,14 +1033,27 @@ extern "C" fv_status fv_assemble_host(fv_mesh *m, const fv_terms_desc *terms, co
     cudaStream_t st = fv_stream(stream);
     const int64_t N = m->n_cells, F = m->n_faces, Fb = m->n_bfaces;
     double *buf = nullptr;
-    const size_t tot = (size_t)(2 * F + 2 * N + 2 * Fb + N * m->dim);
+    const size_t tot = (size_t)(3 * F + 8 * N + 2 * Fb + N * m->dim);
     FV_CUDA_TRY(fv_malloc_async(&buf, sizeof(double) * tot, st));
     double *dk = buf, *dfl = buf + F, *ds = buf + 2 * F, *db = buf + 2 * F + N, *dbi = buf + 2 * F + 2 * N,
-           *dbe = dbi + Fb, *dg = dbe + Fb;
+           *dbe = dbi + Fb, *dg = dbe + Fb, *dx = dg + N * m->dim;
     fv_terms_desc t = *terms;
     if (terms->gradients) {
         FV_CUDA_TRY(cudaMemcpyAsync(dg, terms->gradients, sizeof(double) * N * m->dim, cudaMemcpyHostToDevice, st));
         t.gradients = dg;
+    }
+    // per-cell fields of the time / linear-source terms and the divergence flux
+    const double **cellf[6] = {&t.previous, &t.previous_2, &t.density, &t.density_previous,
+                               &t.density_previous_2, &t.linear_source};
+    for (int q = 0; q < 6; ++q)
+        if (*cellf[q]) {
+            FV_CUDA_TRY(cudaMemcpyAsync(dx + q * N, *cellf[q], sizeof(double) * N, cudaMemcpyHostToDevice, st));
+            *cellf[q] = dx + q * N;
+        }
+    if (terms->divergence_flux) {
+        FV_CUDA_TRY(cudaMemcpyAsync(dx + 6 * N, terms->divergence_flux, sizeof(double) * F, cudaMemcpyHostToDevice,
+                                    st));
+        t.divergence_flux = dx + 6 * N;
     }
     if (terms->diffusivity) {
         FV_CUDA_TRY(cudaMemcpyAsync(dk, terms->diffusivity, sizeof(double) * F, cudaMemcpyHostToDevice, st));

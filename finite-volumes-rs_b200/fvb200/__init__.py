@@ -13,4 +13,6 @@ from .linalg import (  # noqa: F401
     conjugate_gradient,
 )
 from .mesh import DeviceMesh, Mesh  # noqa: F401
-from .terms import Corrected, Orthogonal, Upwind, convection, laplacian, source  # noqa: F401
+from .terms import (  # noqa: F401
+    Backward, Corrected, Euler, Orthogonal, Upwind, convection, divergence, laplacian, linear_source, source, time,
+)

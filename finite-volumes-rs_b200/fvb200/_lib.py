@@ -60,6 +60,11 @@ class TermsDesc(C.Structure):
         ("laplacian_coef", C.c_double), ("convection_coef", C.c_double), ("source_coef", C.c_double),
         ("diffusivity", C.c_void_p), ("flux", C.c_void_p), ("source", C.c_void_p),
         ("scheme", C.c_int32), ("corrector_reduction", C.c_double), ("gradients", C.c_void_p),
+        ("time_coef", C.c_double), ("time_scheme", C.c_int32), ("dt", C.c_double), ("dt_2", C.c_double),
+        ("previous", C.c_void_p), ("previous_2", C.c_void_p), ("density", C.c_void_p),
+        ("density_previous", C.c_void_p), ("density_previous_2", C.c_void_p),
+        ("linear_source_coef", C.c_double), ("linear_source", C.c_void_p),
+        ("divergence_coef", C.c_double), ("divergence_flux", C.c_void_p),
     ]
 
 

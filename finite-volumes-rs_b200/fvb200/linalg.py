@@ -166,6 +166,32 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
         t.scheme = 1
         t.corrector_reduction = sch.corrector_reduction
         t.gradients = g.data_ptr()
+    def arr(a):
+        t = _dev_f64(a)
+        keep.append(t)
+        return t.data_ptr()
+
+    ts = equation.data.get("time")
+    if ts is not None:
+        t.time_coef = equation.coefficient("time")
+        t.dt = ts.dt
+        t.previous = arr(ts.previous)
+        if ts.__class__.__name__ == "Euler":
+            t.time_scheme = 1
+            if ts.densities is not None:
+                t.density, t.density_previous = arr(ts.densities[0]), arr(ts.densities[1])
+        else:
+            t.time_scheme = 2
+            t.dt_2 = ts.dt_2
+            t.previous_2 = arr(ts.previous_2)
+            if ts.densities is not None:
+                t.density, t.density_previous, t.density_previous_2 = (arr(d) for d in ts.densities)
+    if "linear_source" in equation.data:
+        t.linear_source_coef = equation.coefficient("linear_source")
+        t.linear_source = arr(equation.data["linear_source"])
+    if "divergence" in equation.data:
+        t.divergence_coef = equation.coefficient("divergence")
+        t.divergence_flux = arr(equation.data["divergence"])
     nb = mesh.n_boundary_faces
     if callable(boundary_condition):
         fb0 = mesh.n_faces - nb

@@ -8,9 +8,10 @@ faceinterp::Upwind (upwind.rs:26-33).
 
 An expression is kept as a signed combination of at most one laplacian, one
 convection and one source term, which is exactly what the term tree computes:
-every value is a sum of +/- the individual terms.  Anything else
-(Linear/LimitedLinear interpolation in convection, time, divergence,
-linear_source) raises NotImplementedError at construction.
+every value is a sum of +/- the individual terms.  The transient and extra
+terms time (Euler / Backward), linear_source and divergence are kept the same
+way.  Anything else (Linear/LimitedLinear interpolation in convection)
+raises NotImplementedError at construction.
 """
 from __future__ import annotations
 
@@ -77,6 +78,9 @@ class TermExpr:
     def coefficients(self):
         return (self.coef.get("laplacian", 0.0), self.coef.get("convection", 0.0), self.coef.get("source", 0.0))
 
+    def coefficient(self, kind: str) -> float:
+        return self.coef.get(kind, 0.0)
+
 
 def laplacian(scheme, diffusivity) -> TermExpr:
     if not isinstance(scheme, (Orthogonal, Corrected)):
@@ -96,13 +100,39 @@ def source(values) -> TermExpr:
     return TermExpr({"source": 1.0}, {"source": values})
 
 
-def time(*a, **k):  # pragma: no cover - name kept for API parity
-    raise NotImplementedError("terms::time is not implemented on the device path")
+class Euler:
+    """schemes::time::Euler (euler.rs): cell lhs (1/dt) rho, rhs previous/dt rho_previous."""
+
+    def __init__(self, previous, dt: float, density=None, density_previous=None):
+        if (density is None) != (density_previous is None):
+            raise ValueError("Euler: give both densities or neither")
+        self.previous, self.dt = previous, float(dt)
+        self.densities = None if density is None else (density, density_previous)
 
 
-def divergence(*a, **k):  # pragma: no cover
-    raise NotImplementedError("terms::divergence is not implemented on the device path")
+class Backward:
+    """schemes::time::Backward (backward.rs): second-order backward difference
+    with variable step (dt now, dt_2 the previous step)."""
+
+    def __init__(self, previous, previous_2, dt: float, dt_2: float, densities=None):
+        self.previous, self.previous_2, self.dt, self.dt_2 = previous, previous_2, float(dt), float(dt_2)
+        if densities is not None and len(densities) != 3:
+            raise ValueError("Backward: densities = (now, previous, previous_2)")
+        self.densities = densities
 
 
-def linear_source(*a, **k):  # pragma: no cover
-    raise NotImplementedError("terms::linear_source is not implemented on the device path")
+def time(scheme) -> TermExpr:
+    """terms::time (time.rs:19-35) with Euler or Backward."""
+    if not isinstance(scheme, (Euler, Backward)):
+        raise NotImplementedError("terms::time runs with schemes::time::Euler or Backward")
+    return TermExpr({"time": 1.0}, {"time": scheme})
+
+
+def linear_source(coefficients) -> TermExpr:
+    """terms::linear_source (source.rs:61-79): cell lhs = coefficient."""
+    return TermExpr({"linear_source": 1.0}, {"linear_source": coefficients})
+
+
+def divergence(flux) -> TermExpr:
+    """terms::divergence (divergence.rs:22-43): face rhs -flux."""
+    return TermExpr({"divergence": 1.0}, {"divergence": flux})

@@ -158,7 +158,31 @@ typedef struct fv_terms_desc {
     int32_t scheme;            /* FV_SCHEME_ORTHOGONAL or FV_SCHEME_CORRECTED */
     double corrector_reduction;/* Corrected: 0 = no correction ... 1 = full */
     const double *gradients;   /* Corrected: n_cells*dim cell gradients (fv_compute_gradients) */
+    /* Transient and further terms, each with a coefficient -1, 0 or +1 in the
+     * same expression:
+     *   time(Euler(previous, dt)) (terms/time.rs:19-35, schemes/time/euler.rs):
+     *     cell lhs (1/dt)*rho, cell rhs previous/dt*rho_prev;
+     *   time(Backward(previous, previous_2, dt, dt_2)) (schemes/time/backward.rs):
+     *     cell lhs (a_next/dt)*rho, rhs (previous*a_last*rho_prev
+     *     - previous_2*a_last_2*rho_prev_2)/dt with the reference's a_* of dt/dt_2;
+     *   linear_source(c) (terms/source.rs:61-79): cell lhs c;
+     *   divergence(F) (terms/divergence.rs:22-43): face rhs -F.
+     * Densities are optional (NULL: 1). */
+    double time_coef;
+    int32_t time_scheme;       /* FV_TIME_EULER or FV_TIME_BACKWARD */
+    double dt, dt_2;
+    const double *previous;    /* n_cells */
+    const double *previous_2;  /* n_cells (Backward) */
+    const double *density;     /* n_cells, optional */
+    const double *density_previous;
+    const double *density_previous_2;
+    double linear_source_coef;
+    const double *linear_source;   /* n_cells */
+    double divergence_coef;
+    const double *divergence_flux; /* n_faces */
 } fv_terms_desc;
+#define FV_TIME_EULER 1
+#define FV_TIME_BACKWARD 2
 
 /* Boundary closure value_b = bndi*value_i + bnde per boundary face
  * (assembly.rs:64-73, bcs/mod.rs:33).  Dirichlet g: (0,g); zero gradient: (1,0). */

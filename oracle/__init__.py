@@ -26,6 +26,12 @@ P = C.POINTER
 dp, ip, i64, vp = P(C.c_double), P(C.c_int32), C.c_int64, C.c_void_p
 
 
+class OrExtra(C.Structure):
+    _fields_ = [("c_time", C.c_double), ("c_lin", C.c_double), ("c_div", C.c_double), ("time_scheme", C.c_int),
+                ("dt", C.c_double), ("dt_2", C.c_double), ("prev", dp), ("prev2", dp), ("dens", dp), ("densp", dp),
+                ("densp2", dp), ("lin", dp), ("divflux", dp)]
+
+
 class OrInfo(C.Structure):
     _fields_ = [("iterations", i64), ("initial_residual", C.c_double), ("final_residual", C.c_double),
                 ("history_len", i64), ("restarts", C.c_int32)]
@@ -43,6 +49,9 @@ def lib():
             "or_assemble_scheme": ([C.c_int32, i64, i64, i64, ip, ip, dp, dp, dp, dp, C.c_double, C.c_double,
                                     C.c_double, dp, dp, dp, dp, dp, ip, ip, dp, dp, C.c_int, dp, dp, C.c_double],
                                    C.c_int),
+            "or_assemble_full": ([C.c_int32, i64, i64, i64, ip, ip, dp, dp, dp, dp, C.c_double, C.c_double,
+                                  C.c_double, dp, dp, dp, dp, dp, ip, ip, dp, dp, C.c_int, dp, dp, C.c_double,
+                                  P(OrExtra)], C.c_int),
             "or_grad_coeffs": ([C.c_int32, i64, ip, ip, dp, dp, ip, ip, dp, dp], C.c_int),
             "or_gradients": ([C.c_int32, i64, i64, i64, ip, ip, ip, ip, dp, dp, dp, dp, dp, dp], None),
             "or_spmv": ([i64, ip, ip, dp, dp, dp], None),
@@ -127,10 +136,15 @@ def gradients(mesh, values, bndi, bnde):
 
 
 def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bndi=None, bnde=None,
-             corrected=None):
+             corrected=None, extra=None):
     """assemble() restated: returns (row_ptr, cols, vals, rhs).  corrected =
     (gradients n_cells x dim, corrector_reduction) selects the Corrected
-    face-normal gradient scheme for the laplacian (Orthogonal otherwise)."""
+    face-normal gradient scheme for the laplacian (Orthogonal otherwise).
+    extra = dict(c_time, time_scheme ("euler" | "backward"), dt, dt_2,
+    previous, previous_2, densities, c_lin, lin, c_div, divflux) adds the
+    transient / linear-source / divergence terms."""
+    if extra is not None:
+        return _assemble_full(mesh, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, corrected, extra)
     ptr, cols = pattern(mesh)
     F, N, Fb = mesh.n_faces, mesh.n_cells, mesh.n_boundary_faces
     z = lambda n: np.zeros(max(n, 1))  # noqa: E731
@@ -153,6 +167,54 @@ def assemble(mesh, c_lap, c_conv, c_src, kappa=None, flux=None, source=None, bnd
                                       _pd(_d(mesh.cell_center)), _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src,
                                       _pd(kappa), _pd(flux), _pd(source), _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols),
                                       _pd(vals), _pd(rhs), 1, _pd(_d(mesh.face_normal)), _pd(_d(grad)), float(red))
+    if rc != 0:
+        raise RuntimeError(f"oracle assemble failed: {rc}")
+    return ptr, cols, vals, rhs
+
+
+def _assemble_full(mesh, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, corrected, extra):
+    ptr, cols = pattern(mesh)
+    F, N, Fb = mesh.n_faces, mesh.n_cells, mesh.n_boundary_faces
+    z = lambda n: np.zeros(max(n, 1))  # noqa: E731
+    kappa = _d(kappa) if kappa is not None else z(F)
+    flux = _d(flux) if flux is not None else z(F)
+    source = _d(source) if source is not None else z(N)
+    bndi = _d(bndi) if bndi is not None else z(Fb)
+    bnde = _d(bnde) if bnde is not None else z(Fb)
+    keep = []
+
+    def arr(a):
+        if a is None:
+            return None
+        t = _d(a)
+        keep.append(t)
+        return _pd(t)
+
+    ex = OrExtra()
+    ex.c_time = float(extra.get("c_time", 0.0))
+    ex.c_lin = float(extra.get("c_lin", 0.0))
+    ex.c_div = float(extra.get("c_div", 0.0))
+    ex.time_scheme = 1 if extra.get("time_scheme", "euler") == "euler" else 2
+    ex.dt = float(extra.get("dt", 0.0))
+    ex.dt_2 = float(extra.get("dt_2", 0.0))
+    ex.prev = arr(extra.get("previous"))
+    ex.prev2 = arr(extra.get("previous_2"))
+    dens = extra.get("densities")
+    if dens is not None:
+        ex.dens, ex.densp = arr(dens[0]), arr(dens[1])
+        if len(dens) > 2:
+            ex.densp2 = arr(dens[2])
+    ex.lin = arr(extra.get("lin"))
+    ex.divflux = arr(extra.get("divflux"))
+    scheme, grad, red = (0, z(N * mesh.dim), 0.0) if corrected is None else (1, _d(corrected[0]), corrected[1])
+    vals = np.empty(len(cols))
+    rhs = np.empty(N)
+    rc = lib().or_assemble_full(mesh.dim, N, F, Fb, _pi(_i(mesh.face_owner)), _pi(_i(mesh.face_neighbor)),
+                                _pd(_d(mesh.face_area)), _pd(_d(mesh.face_center)), _pd(_d(mesh.cell_center)),
+                                _pd(_d(mesh.cell_volume)), c_lap, c_conv, c_src, _pd(kappa), _pd(flux), _pd(source),
+                                _pd(bndi), _pd(bnde), _pi(ptr), _pi(cols), _pd(vals), _pd(rhs), scheme,
+                                _pd(_d(mesh.face_normal)) if scheme else None, _pd(_d(grad)), float(red),
+                                C.byref(ex))
     if rc != 0:
         raise RuntimeError(f"oracle assemble failed: {rc}")
     return ptr, cols, vals, rhs

@@ -24,6 +24,9 @@
  *   schemes ............. src/fvm/schemes/facengrad/orthogonal.rs:26-46,
  *                          src/fvm/schemes/facengrad/corrected.rs:36-67,
  *                          src/fvm/schemes/faceinterp/upwind.rs:26-33
+ *   transient terms ..... src/fvm/terms/time.rs:19-35, src/fvm/schemes/time/{euler.rs,backward.rs},
+ *                          src/fvm/terms/source.rs:61-79 (linear_source),
+ *                          src/fvm/terms/divergence.rs:22-43
  *   gradients ........... src/core/mesh/compute.rs:155-203 (coefficients),
  *                          src/core/matrix.rs:320-380 (Matrix::inv),
  *                          src/fvm/tools/gradients.rs:48-86 (compute_gradients)
@@ -167,14 +170,32 @@ int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_
                        const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
                        int scheme, const double *face_normal, const double *grad, double red);
 
+/* Extra terms of an expression: time(Euler | Backward) (terms/time.rs,
+ * schemes/time/euler.rs, backward.rs), linear_source (terms/source.rs:61-79),
+ * divergence (terms/divergence.rs:22-43).  coef = {c_time, c_lin, c_div},
+ * time_scheme 1 Euler / 2 Backward; dens* may be NULL (density 1). */
+typedef struct {
+    double c_time, c_lin, c_div;
+    int time_scheme;
+    double dt, dt_2;
+    const double *prev, *prev2, *dens, *densp, *densp2, *lin, *divflux;
+} or_extra;
+
+int or_assemble_full(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                     const int32_t *neighbor, const double *area, const double *face_center,
+                     const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
+                     const double *kappa, const double *flux, const double *source, const double *bndi,
+                     const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
+                     int scheme, const double *face_normal, const double *grad, double red, const or_extra *ex);
+
 int or_assemble(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
                 const int32_t *neighbor, const double *area, const double *face_center,
                 const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
                 const double *kappa, const double *flux, const double *source, const double *bndi,
                 const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs) {
-    return or_assemble_scheme(dim, n_cells, n_faces, n_bfaces, owner, neighbor, area, face_center, cell_center,
-                              volume, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, row_ptr, cols, vals,
-                              rhs, 0, NULL, NULL, 0.0);
+    return or_assemble_full(dim, n_cells, n_faces, n_bfaces, owner, neighbor, area, face_center, cell_center,
+                            volume, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, row_ptr, cols, vals,
+                            rhs, 0, NULL, NULL, 0.0, NULL);
 }
 
 int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
@@ -183,13 +204,59 @@ int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_
                        const double *kappa, const double *flux, const double *source, const double *bndi,
                        const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
                        int scheme, const double *face_normal, const double *grad, double red) {
+    return or_assemble_full(dim, n_cells, n_faces, n_bfaces, owner, neighbor, area, face_center, cell_center,
+                            volume, c_lap, c_conv, c_src, kappa, flux, source, bndi, bnde, row_ptr, cols, vals,
+                            rhs, scheme, face_normal, grad, red, NULL);
+}
+
+/* the cell terms of the time schemes (euler.rs:37-47, backward.rs:44-66) */
+static void time_cell(const or_extra *ex, int64_t c, double *tl, double *tr) {
+    if (ex->time_scheme == 1) {
+        const double r0 = ex->dens ? ex->dens[c] : 1.0, r1 = ex->dens ? ex->densp[c] : 1.0;
+        *tl = 1.0 * (1.0 / ex->dt) * r0;
+        *tr = ex->prev[c] / ex->dt * r1;
+    } else {
+        const double wn = ex->dt / ex->dt_2;
+        const double a_next = (1.0 + 2.0 * wn) / (1.0 + wn);
+        const double a_last = ((1.0 + wn) * (1.0 + wn)) / (1.0 + wn);
+        const double a_last_2 = (wn * wn) / (1.0 + wn);
+        const double r0 = ex->dens ? ex->dens[c] : 1.0, r1 = ex->dens ? ex->densp[c] : 1.0,
+                     r2 = ex->dens ? ex->densp2[c] : 1.0;
+        *tl = 1.0 * (a_next / ex->dt) * r0;
+        *tr = (ex->prev[c] * a_last * r1 - ex->prev2[c] * a_last_2 * r2) / ex->dt;
+    }
+}
+
+int or_assemble_full(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                     const int32_t *neighbor, const double *area, const double *face_center,
+                     const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
+                     const double *kappa, const double *flux, const double *source, const double *bndi,
+                     const double *bnde, const int32_t *row_ptr, const int32_t *cols, double *vals, double *rhs,
+                     int scheme, const double *face_normal, const double *grad, double red, const or_extra *ex) {
+    const or_extra none = {0};
+    if (!ex) ex = &none;
     const int64_t nnz = row_ptr[n_cells];
     const int64_t fb0 = n_faces - n_bfaces;
     for (int64_t k = 0; k < nnz; ++k) vals[k] = 0.0;
-    /* cell loop (assembly.rs:26-32): no term in scope has a cell lhs */
+    /* cell loop (assembly.rs:26-32); at most two nonzero terms per side, so
+     * the signed sum equals the term tree's value in any order */
     for (int64_t c = 0; c < n_cells; ++c) {
+        double tl = 0.0, tr = 0.0;
+        if (ex->c_time != 0.0) time_cell(ex, c, &tl, &tr);
         double l = 0.0;
-        double r = c_src != 0.0 ? c_src * (-source[c]) : 0.0;
+        if (ex->c_time != 0.0 && ex->c_lin != 0.0)
+            l = ex->c_time * tl + ex->c_lin * ex->lin[c];
+        else if (ex->c_time != 0.0)
+            l = ex->c_time * tl;
+        else if (ex->c_lin != 0.0)
+            l = ex->c_lin * ex->lin[c];
+        double r = 0.0;
+        if (ex->c_time != 0.0 && c_src != 0.0)
+            r = ex->c_time * tr + c_src * (-source[c]);
+        else if (ex->c_time != 0.0)
+            r = ex->c_time * tr;
+        else if (c_src != 0.0)
+            r = c_src * (-source[c]);
         int64_t kd = csr_find(row_ptr, cols, c, (int32_t)c);
         if (kd < 0) return OR_ERR_INVALID;
         vals[kd] = l * volume[c];
@@ -230,9 +297,15 @@ int or_assemble_scheme(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_
             li = c_conv * conv0;
             lj = c_conv * conv1;
         }
-        /* face rhs: only the Corrected laplacian has one; combined as li/lj */
+        /* face rhs: the Corrected laplacian's and the divergence's (-F); combined as li/lj */
         double r = 0.0;
-        if (scheme == 1 && c_lap != 0.0) r = c_conv != 0.0 ? c_conv * 0.0 + c_lap * lap_r : c_lap * lap_r;
+        const int corr = scheme == 1 && c_lap != 0.0;
+        if (corr && ex->c_div != 0.0)
+            r = c_lap * lap_r + ex->c_div * (-ex->divflux[f]);
+        else if (corr)
+            r = c_conv != 0.0 ? c_conv * 0.0 + c_lap * lap_r : c_lap * lap_r;
+        else if (ex->c_div != 0.0)
+            r = ex->c_div * (-ex->divflux[f]);
         li = li * area[f];
         lj = lj * area[f];
         const double ra = r * area[f];
