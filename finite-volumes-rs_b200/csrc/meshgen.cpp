@@ -18,7 +18,10 @@
 #include "fv_b200.h"
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdio>
+#include <string>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -642,6 +645,106 @@ extern "C" fv_status fv_host_fields_generate(const fv_host_mesh *m, uint64_t see
             for (int64_t c = 0; c < m->n_cells; ++c) source_cell[c] = source_uniform ? rs.uniform() : source_const;
         }
         return FV_OK;
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
+}
+
+// Mesh::read_su2 (core/mesh/io.rs:228-533): NPOIN node lines (the first dim
+// values), NELEM element lines (VTK kind then its nodes; trailing indices
+// ignored), MARKER_TAG / MARKER_ELEMS boundary lines (markers numbered 0, 1,
+// ... in file order, a face's key = its sorted nodes), then the same face
+// numbering and geometry as fv_host_mesh_from_elements.
+extern "C" fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_host_mesh **out) {
+    if (!path || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    FILE *fp = fopen(path, "r");
+    if (!fp) return FV_ERR_INVALID;
+    std::vector<std::string> lines;
+    {
+        char buf[4096];
+        std::string cur;
+        while (fgets(buf, sizeof(buf), fp)) {
+            cur += buf;
+            if (!cur.empty() && cur.back() == '\n') {
+                cur.pop_back();
+                if (!cur.empty() && cur.back() == '\r') cur.pop_back();
+                lines.push_back(cur);
+                cur.clear();
+            }
+        }
+        if (!cur.empty()) lines.push_back(cur);
+        fclose(fp);
+    }
+    auto value_after = [](const std::string &l, const char *key, long long &v) -> bool {
+        size_t p = l.find(key);
+        if (p == std::string::npos) return false;
+        v = atoll(l.c_str() + p + strlen(key));
+        return true;
+    };
+    auto tokens = [](const std::string &l) {
+        std::vector<std::string> t;
+        size_t i = 0;
+        while (i < l.size()) {
+            while (i < l.size() && isspace((unsigned char)l[i])) ++i;
+            size_t j = i;
+            while (j < l.size() && !isspace((unsigned char)l[j])) ++j;
+            if (j > i) t.push_back(l.substr(i, j - i));
+            i = j;
+        }
+        return t;
+    };
+    try {
+        long long ndime = 0;
+        for (const auto &l : lines)
+            if (value_after(l, "NDIME=", ndime)) break;
+        const int d = dim > 0 ? dim : (int)ndime;
+        if (d != 2 && d != 3) return FV_ERR_INVALID;
+        std::vector<double> nodes;
+        std::vector<int32_t> kind, eptr(1, 0), enodes, bptr(1, 0), bnodes, bmark;
+        int marker = -1;
+        for (size_t li = 0; li < lines.size(); ++li) {
+            long long cnt = 0;
+            if (value_after(lines[li], "NPOIN=", cnt)) {
+                for (long long q = 0; q < cnt; ++q) {
+                    if (li + 1 + q >= lines.size()) return FV_ERR_INVALID;
+                    auto t = tokens(lines[li + 1 + q]);
+                    if ((int)t.size() < d) return FV_ERR_INVALID;
+                    for (int c = 0; c < d; ++c) nodes.push_back(strtod(t[c].c_str(), nullptr));
+                }
+                li += (size_t)cnt;
+            } else if (value_after(lines[li], "NELEM=", cnt)) {
+                for (long long q = 0; q < cnt; ++q) {
+                    if (li + 1 + q >= lines.size()) return FV_ERR_INVALID;
+                    auto t = tokens(lines[li + 1 + q]);
+                    if (t.empty()) return FV_ERR_INVALID;
+                    const int k = atoi(t[0].c_str());
+                    const int nn = vtk_nnodes(k);
+                    if (nn < 0 || (int)t.size() < 1 + nn) return FV_ERR_INVALID;
+                    kind.push_back(k);
+                    for (int c = 0; c < nn; ++c) enodes.push_back(atoi(t[1 + c].c_str()));
+                    eptr.push_back((int32_t)enodes.size());
+                }
+                li += (size_t)cnt;
+            } else if (lines[li].find("MARKER_TAG=") != std::string::npos) {
+                ++marker;
+            } else if (value_after(lines[li], "MARKER_ELEMS=", cnt)) {
+                if (marker < 0) return FV_ERR_INVALID;
+                for (long long q = 0; q < cnt; ++q) {
+                    if (li + 1 + q >= lines.size()) return FV_ERR_INVALID;
+                    auto t = tokens(lines[li + 1 + q]);
+                    if (t.size() < 3) return FV_ERR_INVALID;
+                    for (size_t c = 1; c < t.size(); ++c) bnodes.push_back(atoi(t[c].c_str()));
+                    bptr.push_back((int32_t)bnodes.size());
+                    bmark.push_back(marker);
+                }
+                li += (size_t)cnt;
+            }
+        }
+        if (kind.empty() || nodes.empty()) return FV_ERR_INVALID;
+        return fv_host_mesh_from_elements(d, (int64_t)(nodes.size() / d), nodes.data(), (int64_t)kind.size(),
+                                          kind.data(), eptr.data(), enodes.data(), (int64_t)bmark.size(),
+                                          bptr.data(), bnodes.data(), bmark.data(), out);
     } catch (const std::bad_alloc &) {
         return FV_ERR_ALLOC;
     }

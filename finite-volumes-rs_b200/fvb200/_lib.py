@@ -109,6 +109,7 @@ vp = C.c_void_p
 _SIGS = {
     # host mesh
     "fv_host_mesh_from_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, P(P(HostMesh_))],
+    "fv_host_mesh_read_su2": [C.c_char_p, C.c_int32, P(P(HostMesh_))],
     "fv_host_mesh_generate_square": [C.c_int32, C.c_double, C.c_uint64, P(P(HostMesh_))],
     "fv_host_mesh_generate_cube": [C.c_int32, C.c_double, C.c_uint64, P(P(HostMesh_))],
     "fv_host_fields_generate": [P(HostMesh_), C.c_uint64, C.c_double, C.c_double, dp, C.c_double, C.c_int32,

@@ -92,6 +92,13 @@ class Mesh:
         return cls(out)
 
     @classmethod
+    def read_su2(cls, path, dim: int = 0) -> "Mesh":
+        """Mesh::read_su2 (core/mesh/io.rs:489-533); dim 0 = NDIME of the file."""
+        out = C.POINTER(HostMesh_)()
+        check(lib().fv_host_mesh_read_su2(str(path).encode(), int(dim), C.byref(out)), "Mesh.read_su2")
+        return cls(out)
+
+    @classmethod
     def square(cls, n: int, jitter: float = 0.0, seed: int = 0) -> "Mesh":
         out = C.POINTER(HostMesh_)()
         check(lib().fv_host_mesh_generate_square(n, jitter, seed, C.byref(out)), "Mesh.square")

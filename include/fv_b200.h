@@ -84,6 +84,10 @@ typedef struct fv_host_mesh {
 /* Build from an element list, as Mesh::read_su2 does (io.rs:489-533).
  * elem_kind uses VTK ids: 5 triangle, 9 quad, 10 tetrahedron, 12 hexahedron.
  * Boundary faces are given as node lists with a marker id (SU2 MARKER_ELEMS). */
+/* Mesh::read_su2 (io.rs:228-533): an SU2 file (NDIME, NPOIN, NELEM, MARKER_TAG
+ * / MARKER_ELEMS) into the same host mesh as fv_host_mesh_from_elements.
+ * dim 0 takes NDIME from the file. */
+fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_host_mesh **out);
 fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, const double *nodes,
                                      int64_t n_elems, const int32_t *elem_kind,
                                      const int32_t *elem_node_ptr, const int32_t *elem_nodes,

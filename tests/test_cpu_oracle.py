@@ -63,6 +63,8 @@ def test_square_su2_known_answer(fv):
     assert np.linalg.norm(sf) < np.finfo(float).eps * 10
     ref = mesh_ref.build(2, nodes, elements, boundaries)
     _mesh_arrays_equal(m, ref)
+    # the library's own SU2 reader gives the same mesh
+    _mesh_arrays_equal(fv.Mesh.read_su2(SQUARE_SU2), ref)
 
 
 def _square_elements(n):
