@@ -104,6 +104,8 @@ bool fv_build_tile_plans(int64_t n, int dim, const double *cell, const int32_t *
                          const int32_t *fwd_order, const int32_t *bwd_order, int ring, fv_tile_plan &fwd,
                          fv_tile_plan &bwd);
 #define FV_TILE_RING 8
+#define FV_TILE_MAXL 4              // entries per row on the swept side in the tiled layout
+#define FV_TILE_PAD (-2147483647 - 1)  // unused entry of a slot
 
 // Rows a sweep may skip: row i is skipped when done[group[i] * stride] != 0
 // (rows of the problems of a batch that have converged).

@@ -24,6 +24,7 @@
 // unchanged, which is what skipping them does in the reference.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "fv_internal.cuh"
@@ -42,10 +43,16 @@ struct fv_symbolic {
     // box tiling of the two sweeps ([0] forward over L, [1] backward over U);
     // absent (tiled = false) for matrices without mesh geometry or without an
     // acyclic box order
+    // Steps are laid out as 32 slots each (slot = 32 * step + lane); per slot
+    // the row (-1 idle), the entries' positions in the swept side's value
+    // array and their dependency sources (4 per slot, FV_TILE_PAD when unused),
+    // and the slot of the row in the other direction's plan.
     bool tiled = false, tiles_tried = false;
     int32_t t_nb[2] = {0, 0};
-    int32_t *t_box_step[2] = {nullptr, nullptr}, *t_sptr[2] = {nullptr, nullptr};
-    int32_t *t_trow[2] = {nullptr, nullptr}, *t_dsrc[2] = {nullptr, nullptr};
+    int64_t t_nslots[2] = {0, 0};
+    int32_t *t_box_step[2] = {nullptr, nullptr};
+    int32_t *t_slot_row[2] = {nullptr, nullptr}, *t_slot_src[2] = {nullptr, nullptr};
+    int32_t *t_slot_ds[2] = {nullptr, nullptr}, *t_slot_next[2] = {nullptr, nullptr};
     double t_lane_use[2] = {0, 0}, t_ring_share[2] = {0, 0}, t_edge = 0;
 };
 
@@ -60,9 +67,10 @@ void fv_symbolic_free(fv_symbolic *s) {
     cudaFree(s->l_tpos);
     for (int d = 0; d < 2; ++d) {
         cudaFree(s->t_box_step[d]);
-        cudaFree(s->t_sptr[d]);
-        cudaFree(s->t_trow[d]);
-        cudaFree(s->t_dsrc[d]);
+        cudaFree(s->t_slot_row[d]);
+        cudaFree(s->t_slot_src[d]);
+        cudaFree(s->t_slot_ds[d]);
+        cudaFree(s->t_slot_next[d]);
     }
     delete s;
 }
@@ -89,6 +97,13 @@ struct fv_precond {
     const fv_csr *orig = nullptr;
     int32_t *amap = nullptr;
     int level = 0;
+    // box-tiled sweeps: per-slot records (factor values in slot order) and
+    // slot-ordered right-hand sides, FP64 and FP32; rebuilt when the factors change
+    void *t_rec64[2] = {nullptr, nullptr}, *t_rec32[2] = {nullptr, nullptr};
+    double *t_rhs64[2] = {nullptr, nullptr};
+    float *t_rhs32[2] = {nullptr, nullptr};
+    unsigned t_rec64_epoch = 0, t_rec32_version = 0;
+    unsigned f32_version = 0;  // incremented by every fv_precond_make_f32
 };
 
 // ------------------------------------------------------------------ symbolic
@@ -242,23 +257,53 @@ static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
     FV_CUDA_TRY(cudaMemcpyAsync(cells.data(), A->mesh->cell, sizeof(double4) * n, cudaMemcpyDeviceToHost, st));
     FV_CUDA_TRY(cudaStreamSynchronize(st));
     fv_tile_plan tp[2];
+    if (s->max_lower > FV_TILE_MAXL || s->max_upper > FV_TILE_MAXL) return FV_OK;
     if (!fv_build_tile_plans(n, A->mesh->dim, (const double *)cells.data(), lp.data(), lc.data(), up.data(),
                              uc.data(), s->h_fwd_level.data(), s->h_bwd_level.data(), fo.data(), bo.data(),
                              FV_TILE_RING, tp[0], tp[1]))
         return FV_OK;
+    // slot layout of both directions
+    std::vector<int32_t> srow[2], ssrc[2], sds[2], snext[2], row_slot[2];
+    for (int d = 0; d < 2; ++d) {
+        const int64_t nslots = 32LL * tp[d].nsteps;
+        srow[d].assign((size_t)nslots, -1);
+        ssrc[d].assign((size_t)nslots * FV_TILE_MAXL, -1);
+        sds[d].assign((size_t)nslots * FV_TILE_MAXL, FV_TILE_PAD);
+        row_slot[d].assign((size_t)n, -1);
+        const std::vector<int32_t> &ptr = d == 0 ? lp : up;
+        for (int32_t st = 0; st < tp[d].nsteps; ++st)
+            for (int32_t u = tp[d].sptr[st]; u < tp[d].sptr[st + 1]; ++u) {
+                const int64_t slot = 32LL * st + (u - tp[d].sptr[st]);
+                const int32_t row = tp[d].trow[u];
+                srow[d][slot] = row;
+                row_slot[d][row] = (int32_t)slot;
+                for (int32_t k = ptr[row]; k < ptr[row + 1]; ++k) {
+                    ssrc[d][slot * FV_TILE_MAXL + (k - ptr[row])] = k;
+                    sds[d][slot * FV_TILE_MAXL + (k - ptr[row])] = tp[d].dsrc[k];
+                }
+            }
+        if (32LL * tp[d].nsteps >= 0x7fffffffLL) return FV_OK;
+    }
+    for (int d = 0; d < 2; ++d) {  // the forward sweep writes the backward sweep's rhs in its slot order
+        snext[d].assign(srow[d].size(), -1);
+        for (size_t slot = 0; slot < srow[d].size(); ++slot)
+            if (d == 0 && srow[d][slot] >= 0) snext[d][slot] = row_slot[1][srow[d][slot]];
+    }
     cudaError_t e = cudaSuccess;
-    auto up_load = [&](int32_t **d, const std::vector<int32_t> &h) {
+    auto up_load = [&](int32_t **dp, const std::vector<int32_t> &h) {
         if (e != cudaSuccess) return;
-        e = cudaMalloc(d, sizeof(int32_t) * (h.size() ? h.size() : 1));
+        e = cudaMalloc(dp, sizeof(int32_t) * (h.size() ? h.size() : 1));
         if (e == cudaSuccess && h.size())
-            e = cudaMemcpyAsync(*d, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, st);
+            e = cudaMemcpyAsync(*dp, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, st);
     };
     for (int d = 0; d < 2; ++d) {
         up_load(&s->t_box_step[d], tp[d].box_step);
-        up_load(&s->t_sptr[d], tp[d].sptr);
-        up_load(&s->t_trow[d], tp[d].trow);
-        up_load(&s->t_dsrc[d], tp[d].dsrc);
+        up_load(&s->t_slot_row[d], srow[d]);
+        up_load(&s->t_slot_src[d], ssrc[d]);
+        up_load(&s->t_slot_ds[d], sds[d]);
+        up_load(&s->t_slot_next[d], snext[d]);
         s->t_nb[d] = tp[d].nb;
+        s->t_nslots[d] = 32LL * tp[d].nsteps;
         s->t_lane_use[d] = tp[d].lane_use;
         s->t_ring_share[d] = tp[d].ring_share;
     }
@@ -551,112 +596,6 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
     leave(&ctrl[0], &ctrl[1]);
 }
 
-// The same sweep over box tiles (fv_tiles.cu): one warp takes a box (tickets
-// in the boxes' dispatch order) and runs its steps in level order.  A lane's
-// dependency comes either from the warp's shared-memory ring (a row of one of
-// the box's last FV_TILE_RING steps) or from the vector (polled like k_sweep).
-// The next step's row data and first polls are issued before the current step
-// waits, so a chain of rows inside a box costs shared-memory latency per level
-// instead of an L2 round trip.
-template <typename T, int MAXL>
-struct TileRow {
-    int i;  // row, or -1 for an idle lane
-    int m;
-    int ds[MAXL];
-    T v[MAXL], xv[MAXL];
-    unsigned pending;
-    T s, d;
-};
-
-template <typename T, bool UNIT, int MAXL>
-__device__ __forceinline__ void tile_load(TileRow<T, MAXL> &R, int step, const int32_t *__restrict__ sptr,
-                                          const int32_t *__restrict__ trow, const int32_t *__restrict__ ptr,
-                                          const int32_t *__restrict__ dsrc, const T *__restrict__ val,
-                                          const T *__restrict__ dinv, const T *rhs, const T *x,
-                                          const fv_row_skip &rs) {
-    const int lane = threadIdx.x & 31;
-    const int r0 = __ldg(&sptr[step]);
-    R.i = -1;
-    R.m = 0;
-    R.pending = 0;
-    if (lane >= __ldg(&sptr[step + 1]) - r0) return;
-    const int i = __ldg(&trow[r0 + lane]);
-    if (rs.group && rs.done[(int64_t)__ldg(&rs.group[i]) * rs.stride]) return;
-    R.i = i;
-    const int k0 = __ldg(&ptr[i]);
-    R.m = __ldg(&ptr[i + 1]) - k0;
-#pragma unroll
-    for (int q = 0; q < MAXL; ++q)
-        if (q < R.m) {
-            R.ds[q] = __ldg(&dsrc[k0 + q]);
-            R.v[q] = __ldg(&val[k0 + q]);
-        }
-    R.s = rhs[i];
-    R.d = UNIT ? T(1) : __ldg(&dinv[i]);
-#pragma unroll
-    for (int q = 0; q < MAXL; ++q)
-        if (q < R.m && R.ds[q] >= 0 && !fv_slot_ready(&x[R.ds[q]], R.xv[q])) R.pending |= 1u << q;
-}
-
-template <typename T, bool UNIT, int MAXL>
-__global__ void __launch_bounds__(256) k_sweep_tiled(int64_t nb, const int32_t *__restrict__ box_step,
-                                                     const int32_t *__restrict__ sptr,
-                                                     const int32_t *__restrict__ trow,
-                                                     const int32_t *__restrict__ ptr,
-                                                     const int32_t *__restrict__ dsrc, const T *__restrict__ val,
-                                                     const T *__restrict__ dinv, const T *rhs, T *x, T *rhs_reset,
-                                                     T *next_reset, unsigned *ctrl, int *err, const int *skip,
-                                                     fv_row_skip rs) {
-    __shared__ T ring_all[8][FV_TILE_RING * 32];
-    if (skip && *(volatile const int *)skip) return;
-    T *ring = ring_all[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    int64_t b;
-    while (take_chunk(&ctrl[0], nb, b)) {
-        const int s0 = __ldg(&box_step[b]), s1 = __ldg(&box_step[b + 1]);
-        TileRow<T, MAXL> cur, nxt;
-        nxt.i = -1;
-        nxt.m = 0;
-        nxt.pending = 0;
-        tile_load<T, UNIT, MAXL>(cur, s0, sptr, trow, ptr, dsrc, val, dinv, rhs, x, rs);
-        for (int st = s0; st < s1; ++st) {
-            if (st + 1 < s1) tile_load<T, UNIT, MAXL>(nxt, st + 1, sptr, trow, ptr, dsrc, val, dinv, rhs, x, rs);
-            if (cur.i >= 0) {
-                if (cur.pending) {
-                    const unsigned long long t0 = fv_globaltimer();
-                    for (unsigned it = 1; cur.pending; ++it) {
-#pragma unroll
-                        for (int q = 0; q < MAXL; ++q)
-                            if ((cur.pending >> q) & 1u)
-                                if (fv_slot_ready(&x[cur.ds[q]], cur.xv[q])) cur.pending &= ~(1u << q);
-                        if (cur.pending && (it & 255u) == 0) {
-                            if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
-                                if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
-#pragma unroll
-                                for (int q = 0; q < MAXL; ++q)
-                                    if ((cur.pending >> q) & 1u) cur.xv[q] = T(NAN);
-                                cur.pending = 0;
-                            }
-                        }
-                    }
-                }
-                T s = cur.s;
-#pragma unroll
-                for (int q = 0; q < MAXL; ++q)
-                    if (q < cur.m) s = s - cur.v[q] * (cur.ds[q] < 0 ? ring[-cur.ds[q] - 1] : cur.xv[q]);
-                const T r = UNIT ? s : cur.d * s;
-                ring[((st - s0) % FV_TILE_RING) * 32 + lane] = r;
-                fv_publish(&x[cur.i], r);
-                if (rhs_reset) fv_reset_slot(&rhs_reset[cur.i]);
-                if (next_reset) fv_reset_slot(&next_reset[cur.i]);
-            }
-            __syncwarp();
-            cur = nxt;
-        }
-    }
-    leave(&ctrl[0], &ctrl[1]);
-}
-
 template <typename T, bool UNIT>
 static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
                          const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
@@ -678,26 +617,261 @@ static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int3
                                                                   next_reset, ctrl, err, skip, rs);
 }
 
-// Tiled sweep of direction d (0 forward over L, 1 backward over U).
+// The same sweep over box tiles (fv_tiles.cu).  A warp takes a box (tickets
+// in the boxes' dispatch order, every box after the boxes it depends on) and
+// runs its steps in level order, one row per lane.  All static data of a step
+// -- the row, its factor entries, where each dependency comes from, the slot
+// of the row in the next sweep -- sits in one record per (step, lane), and
+// the step's right-hand side in a slot-ordered array; both are streamed into
+// shared memory with cp.async D steps ahead, so a step waits only for the
+// values it depends on: from the warp's ring of its last FV_TILE_RING steps
+// (rows of the same box) or, polled like k_sweep, from the vector.
+struct __align__(16) TileRec64 {
+    double v[FV_TILE_MAXL];
+    double d;
+    int32_t ds[FV_TILE_MAXL];
+    int32_t row, next;
+};
+struct __align__(16) TileRec32 {
+    float v[FV_TILE_MAXL];
+    float d;
+    int32_t row, next, pad;
+    int32_t ds[FV_TILE_MAXL];
+};
+static_assert(sizeof(TileRec64) == 64 && sizeof(TileRec32) == 48, "tile record layout");
+template <typename T>
+using TileRec = typename std::conditional<sizeof(T) == 8, TileRec64, TileRec32>::type;
+
+constexpr int kTileWarps = 4;  // warps per block
+constexpr int kTileDepth = 6;  // steps in flight per warp
+
+template <typename T>
+constexpr size_t tile_smem() {
+    return (size_t)kTileWarps * 32 * (kTileDepth * (sizeof(TileRec<T>) + sizeof(T)) + FV_TILE_RING * sizeof(T));
+}
+
+template <typename T>
+__global__ void k_tile_records(int64_t nslots, const int32_t *__restrict__ slot_row,
+                               const int32_t *__restrict__ slot_src, const int32_t *__restrict__ slot_ds,
+                               const int32_t *__restrict__ slot_next, const T *__restrict__ val,
+                               const T *__restrict__ dinv, TileRec<T> *__restrict__ rec) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nslots; u += (int64_t)gridDim.x * blockDim.x) {
+        TileRec<T> r;
+        r.row = slot_row[u];
+        r.next = slot_next[u];
+#pragma unroll
+        for (int q = 0; q < FV_TILE_MAXL; ++q) {
+            const int32_t src = slot_src[u * FV_TILE_MAXL + q];
+            r.v[q] = src >= 0 ? val[src] : T(0);
+            r.ds[q] = slot_ds[u * FV_TILE_MAXL + q];
+        }
+        r.d = (dinv && r.row >= 0) ? dinv[r.row] : T(1);
+        if constexpr (sizeof(T) == 4) r.pad = 0;
+        rec[u] = r;
+    }
+}
+
+template <typename T>
+__global__ void k_tile_rhs(int64_t nslots, const int32_t *__restrict__ slot_row, const T *__restrict__ r,
+                           T *__restrict__ out) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nslots; u += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t row = slot_row[u];
+        out[u] = row >= 0 ? r[row] : T(0);
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void *smem, const void *gmem) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(a), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 template <typename T, bool UNIT>
-static void launch_tiled(const fv_symbolic *s, int d, int maxl, cudaStream_t st, const int32_t *ptr, const T *val,
-                         const T *dinv, const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl, int *err,
-                         const int *skip, fv_row_skip rs) {
-    const int64_t nb = s->t_nb[d];
-    const int G = (int)std::max<int64_t>(1, std::min<int64_t>((nb + 7) / 8, 148 * 4));
-    if (maxl <= 4)
-        fv_note_launch(), k_sweep_tiled<T, UNIT, 4><<<G, 256, 0, st>>>(
-                              nb, s->t_box_step[d], s->t_sptr[d], s->t_trow[d], ptr, s->t_dsrc[d], val, dinv, rhs,
-                              x, rhs_reset, next_reset, ctrl, err, skip, rs);
-    else
-        fv_note_launch(), k_sweep_tiled<T, UNIT, 8><<<G, 256, 0, st>>>(
-                              nb, s->t_box_step[d], s->t_sptr[d], s->t_trow[d], ptr, s->t_dsrc[d], val, dinv, rhs,
-                              x, rhs_reset, next_reset, ctrl, err, skip, rs);
+__global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, const int32_t *__restrict__ box_step,
+                                                                 const TileRec<T> *__restrict__ rec,
+                                                                 const T *__restrict__ rhs_slot, T *x, T *next_rhs,
+                                                                 T *rhs_reset, T *next_reset, unsigned *ctrl,
+                                                                 int *err, const int *skip, fv_row_skip rs) {
+    using R = TileRec<T>;
+    extern __shared__ __align__(16) unsigned char tile_smem_raw[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    R *recbuf = reinterpret_cast<R *>(tile_smem_raw) + (size_t)w * kTileDepth * 32;
+    T *rhsbuf = reinterpret_cast<T *>(tile_smem_raw + (size_t)kTileWarps * kTileDepth * 32 * sizeof(R)) +
+                (size_t)w * kTileDepth * 32;
+    T *ring = reinterpret_cast<T *>(tile_smem_raw + (size_t)kTileWarps * kTileDepth * 32 * (sizeof(R) + sizeof(T))) +
+              (size_t)w * FV_TILE_RING * 32;
+    if (skip && *(volatile const int *)skip) return;
+    int64_t b;
+    while (take_chunk(&ctrl[0], nb, b)) {
+        const int s0 = __ldg(&box_step[b]), s1 = __ldg(&box_step[b + 1]);
+        // a box holds rows of one connected component: one problem of a batch
+        if (rs.group) {
+            const int row0 = rec[(int64_t)32 * s0].row;
+            if (rs.done[(int64_t)__ldg(&rs.group[row0]) * rs.stride]) continue;
+        }
+        auto issue = [&](int step, int bi) {
+            if (step < s1) {
+                const int64_t u = (int64_t)32 * step + lane;
+                const unsigned char *src = reinterpret_cast<const unsigned char *>(&rec[u]);
+                unsigned char *dst = reinterpret_cast<unsigned char *>(&recbuf[bi * 32 + lane]);
+#pragma unroll
+                for (int c = 0; c < (int)(sizeof(R) / 16); ++c) cp_async16(dst + 16 * c, src + 16 * c);
+                cp_async_small<sizeof(T)>(&rhsbuf[bi * 32 + lane], &rhs_slot[u]);
+            }
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int k = 0; k < kTileDepth; ++k) issue(s0 + k, k);
+        for (int st = s0; st < s1; ++st) {
+            cp_async_wait<kTileDepth - 1>();
+            const int bi = (st - s0) % kTileDepth;
+            const R r = recbuf[bi * 32 + lane];
+            const T rh = rhsbuf[bi * 32 + lane];
+            issue(st + kTileDepth, bi);
+            if (r.row >= 0) {
+                T xv[FV_TILE_MAXL];
+                unsigned pending = 0;
+#pragma unroll
+                for (int q = 0; q < FV_TILE_MAXL; ++q) {
+                    xv[q] = T(0);
+                    if (r.ds[q] >= 0 && !fv_slot_ready(&x[r.ds[q]], xv[q])) pending |= 1u << q;
+                }
+                if (pending) {
+                    const unsigned long long t0 = fv_globaltimer();
+                    for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                        for (int q = 0; q < FV_TILE_MAXL; ++q)
+                            if ((pending >> q) & 1u)
+                                if (fv_slot_ready(&x[r.ds[q]], xv[q])) pending &= ~(1u << q);
+                        if (pending && (it & 255u) == 0) {
+                            if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
+                                if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+#pragma unroll
+                                for (int q = 0; q < FV_TILE_MAXL; ++q)
+                                    if ((pending >> q) & 1u) xv[q] = T(NAN);
+                                pending = 0;
+                            }
+                        }
+                    }
+                }
+                T s = rh;
+#pragma unroll
+                for (int q = 0; q < FV_TILE_MAXL; ++q)
+                    if (r.ds[q] != FV_TILE_PAD) s = s - r.v[q] * (r.ds[q] < 0 ? ring[-r.ds[q] - 1] : xv[q]);
+                const T res = UNIT ? s : r.d * s;
+                ring[((st - s0) % FV_TILE_RING) * 32 + lane] = res;
+                fv_publish(&x[r.row], res);
+                if (next_rhs) next_rhs[r.next] = res;
+                if (rhs_reset) fv_reset_slot(&rhs_reset[r.row]);
+                if (next_reset) fv_reset_slot(&next_reset[r.row]);
+            }
+            __syncwarp();
+        }
+    }
+    cp_async_wait<0>();
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+template <typename T, bool UNIT>
+static int tile_grid(int64_t nb) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaFuncSetAttribute(k_sweep_tiled<T, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem<T>());
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_tiled<T, UNIT>, kTileWarps * 32,
+                                                          tile_smem<T>()) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    }
+    return (int)std::max<int64_t>(1, std::min<int64_t>((nb + kTileWarps - 1) / kTileWarps, 148LL * per_sm));
 }
 
 static bool use_tiles(const fv_precond *P) {
     const fv_symbolic *s = P->sym;
-    return P->schedule == 2 && s->tiled && s->max_lower <= 8 && s->max_upper <= 8;
+    return P->schedule == 2 && s->tiled;
+}
+
+// Records of both directions for precision T, rebuilt when the factors changed.
+template <typename T>
+static fv_status tile_prepare(fv_precond *P, cudaStream_t st) {
+    const fv_symbolic *s = P->sym;
+    void **rec = sizeof(T) == 8 ? P->t_rec64 : P->t_rec32;
+    T **rhs = reinterpret_cast<T **>(sizeof(T) == 8 ? (void **)P->t_rhs64 : (void **)P->t_rhs32);
+    const unsigned version = sizeof(T) == 8 ? P->epoch : P->f32_version;
+    unsigned &seen = sizeof(T) == 8 ? P->t_rec64_epoch : P->t_rec32_version;
+    for (int d = 0; d < 2; ++d) {
+        if (!rec[d]) {
+            FV_CUDA_TRY(cudaMalloc(&rec[d], sizeof(TileRec<T>) * (s->t_nslots[d] ? s->t_nslots[d] : 1)));
+            FV_CUDA_TRY(cudaMalloc(&rhs[d], sizeof(T) * (s->t_nslots[d] ? s->t_nslots[d] : 1)));
+            seen = version - 1;
+        }
+    }
+    if (seen != version) {
+        const T *lv, *uv, *dv;
+        if constexpr (sizeof(T) == 8) {
+            lv = P->l_val;
+            uv = P->u_val;
+            dv = P->dinv;
+        } else {
+            lv = P->l32;
+            uv = P->u32;
+            dv = P->dinv32;
+        }
+        for (int d = 0; d < 2; ++d) {
+            const int64_t ns = s->t_nslots[d];
+            if (!ns) continue;
+            const unsigned G = (unsigned)std::min<int64_t>((ns + 255) / 256, 148 * 16);
+            const T *dinv = (d == 0 && P->kind == 2) ? nullptr : dv;  // ILU's forward sweep has a unit diagonal
+            fv_note_launch(), k_tile_records<T><<<G, 256, 0, st>>>(ns, s->t_slot_row[d], s->t_slot_src[d],
+                                                                   s->t_slot_ds[d], s->t_slot_next[d],
+                                                                   d == 0 ? lv : uv, dinv,
+                                                                   reinterpret_cast<TileRec<T> *>(rec[d]));
+            FV_CUDA_TRY(cudaGetLastError());
+        }
+        seen = version;
+    }
+    return FV_OK;
+}
+
+// Both tiled sweeps: z = M^-1 r (same contract as the level-chunk sweeps).
+template <typename T>
+static fv_status tiled_apply(fv_precond *P, const T *r, T *z, T *tmp, cudaStream_t st, const int *skip,
+                             const fv_row_skip &rs) {
+    const fv_symbolic *s = P->sym;
+    FV_TRY(tile_prepare<T>(P, st));
+    void **rec = sizeof(T) == 8 ? P->t_rec64 : P->t_rec32;
+    T **rhs = reinterpret_cast<T **>(sizeof(T) == 8 ? (void **)P->t_rhs64 : (void **)P->t_rhs32);
+    const int64_t ns0 = s->t_nslots[0];
+    if (ns0) {
+        const unsigned G = (unsigned)std::min<int64_t>((ns0 + 255) / 256, 148 * 16);
+        fv_note_launch(), k_tile_rhs<T><<<G, 256, 0, st>>>(ns0, s->t_slot_row[0], r, rhs[0]);
+        FV_CUDA_TRY(cudaGetLastError());
+    }
+    const size_t smem = tile_smem<T>();
+    if (P->kind == 2) {
+        const int G = tile_grid<T, true>(s->t_nb[0]);
+        fv_note_launch(), k_sweep_tiled<T, true><<<G, kTileWarps * 32, smem, st>>>(
+                              s->t_nb[0], s->t_box_step[0], reinterpret_cast<const TileRec<T> *>(rec[0]), rhs[0], tmp,
+                              rhs[1], nullptr, z, P->ctrl, P->err, skip, rs);
+    } else {
+        const int G = tile_grid<T, false>(s->t_nb[0]);
+        fv_note_launch(), k_sweep_tiled<T, false><<<G, kTileWarps * 32, smem, st>>>(
+                              s->t_nb[0], s->t_box_step[0], reinterpret_cast<const TileRec<T> *>(rec[0]), rhs[0], tmp,
+                              rhs[1], nullptr, z, P->ctrl, P->err, skip, rs);
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    const int G = tile_grid<T, false>(s->t_nb[1]);
+    fv_note_launch(), k_sweep_tiled<T, false><<<G, kTileWarps * 32, smem, st>>>(
+                          s->t_nb[1], s->t_box_step[1], reinterpret_cast<const TileRec<T> *>(rec[1]), rhs[1], z,
+                          nullptr, tmp, nullptr, P->ctrl + 2, P->err, skip, rs);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
 }
 
 static int sweep_grid(int64_t n) {
@@ -719,19 +893,7 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const int64_t n = P->n;
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
-    if (use_tiles(P)) {
-        if (P->kind == 2)
-            launch_tiled<double, true>(s, 0, s->max_lower, st, s->l_ptr, P->l_val, nullptr, r, P->tmp, nullptr, z,
-                                       P->ctrl, P->err, skip, rs);
-        else
-            launch_tiled<double, false>(s, 0, s->max_lower, st, s->l_ptr, P->l_val, P->dinv, r, P->tmp, nullptr, z,
-                                        P->ctrl, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        launch_tiled<double, false>(s, 1, s->max_upper, st, s->u_ptr, P->u_val, P->dinv, P->tmp, z, P->tmp, nullptr,
-                                    P->ctrl + 2, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        return FV_OK;
-    }
+    if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
     if (P->kind == 2)
         launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -784,6 +946,7 @@ fv_status fv_precond_make_f32(fv_precond *P, cudaStream_t st) {
     if (s->nnz_u) fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(s->nnz_u, P->u_val, P->u32);
     fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(n, P->dinv, P->dinv32);
     FV_CUDA_TRY(cudaGetLastError());
+    P->f32_version += 1;
     return FV_OK;
 }
 
@@ -795,19 +958,7 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
     if (!P->l32) return FV_ERR_INVALID;
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
-    if (use_tiles(P)) {
-        if (P->kind == 2)
-            launch_tiled<float, true>(s, 0, s->max_lower, st, s->l_ptr, P->l32, nullptr, r, P->tmp32, nullptr, z,
-                                      P->ctrl, P->err, skip, rs);
-        else
-            launch_tiled<float, false>(s, 0, s->max_lower, st, s->l_ptr, P->l32, P->dinv32, r, P->tmp32, nullptr, z,
-                                       P->ctrl, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        launch_tiled<float, false>(s, 1, s->max_upper, st, s->u_ptr, P->u32, P->dinv32, P->tmp32, z, P->tmp32,
-                                   nullptr, P->ctrl + 2, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        return FV_OK;
-    }
+    if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
     if (P->kind == 2)
         launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -825,7 +976,7 @@ extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t
     if (!P || request < -1 || request > 2) return FV_ERR_INVALID;
     fv_symbolic *s = P->sym;
     if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
-    if (request == 2 && !(s->tiled && s->max_lower <= 8 && s->max_upper <= 8)) return FV_ERR_UNSUPPORTED;
+    if (request == 2 && !s->tiled) return FV_ERR_UNSUPPORTED;
     if (request >= 0) P->schedule = request == 2 ? 2 : 1;
     if (active) *active = use_tiles(P) ? 2 : 1;
     if (stats) {
@@ -854,6 +1005,12 @@ extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     cudaFree(P->dinv32);
     cudaFree(P->tmp32);
     cudaFree(P->amap);
+    for (int d = 0; d < 2; ++d) {
+        cudaFree(P->t_rec64[d]);
+        cudaFree(P->t_rec32[d]);
+        cudaFree(P->t_rhs64[d]);
+        cudaFree(P->t_rhs32[d]);
+    }
     fv_csr *F = P->fill;
     delete P;
     if (F) fv_csr_destroy(F);
