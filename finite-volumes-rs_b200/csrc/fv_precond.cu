@@ -693,27 +693,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// External dependencies (not in the ring) are polled kTileLead steps before
-// the step runs, from the records already in shared memory; values that were
-// produced long ago are then in registers when the step starts.
-constexpr int kTileLead = 3;
-
-template <typename T>
-struct TilePoll {
-    T xv[FV_TILE_MAXL];
-    unsigned pending;
-};
-
-template <typename T>
-__device__ __forceinline__ void tile_poll(const TileRec<T> &r, const T *x, TilePoll<T> &p) {
-    p.pending = 0;
-#pragma unroll
-    for (int q = 0; q < FV_TILE_MAXL; ++q) {
-        p.xv[q] = T(0);
-        if (r.row >= 0 && r.ds[q] >= 0 && !fv_slot_ready(&x[r.ds[q]], p.xv[q])) p.pending |= 1u << q;
-    }
-}
-
 template <typename T, bool UNIT>
 __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, const int32_t *__restrict__ box_step,
                                                                  const TileRec<T> *__restrict__ rec,
@@ -721,7 +700,6 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, con
                                                                  T *rhs_reset, T *next_reset, unsigned *ctrl,
                                                                  int *err, const int *skip, fv_row_skip rs) {
     using R = TileRec<T>;
-    static_assert(kTileLead + 1 <= kTileDepth, "look-ahead within the records in flight");
     extern __shared__ __align__(16) unsigned char tile_smem_raw[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     R *recbuf = reinterpret_cast<R *>(tile_smem_raw) + (size_t)w * kTileDepth * 32;
@@ -751,39 +729,34 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, con
         };
 #pragma unroll
         for (int k = 0; k < kTileDepth; ++k) issue(s0 + k, k);
-        // first polls of the first kTileLead steps
-        cp_async_wait<kTileDepth - kTileLead>();
-        TilePoll<T> pipe[kTileLead + 1];
-#pragma unroll
-        for (int k = 0; k < kTileLead; ++k) {
-            pipe[k].pending = 0;
-            if (s0 + k < s1) tile_poll<T>(recbuf[k * 32 + lane], x, pipe[k]);
-        }
         for (int st = s0; st < s1; ++st) {
-            cp_async_wait<kTileDepth - kTileLead - 1>();
+            cp_async_wait<kTileDepth - 1>();
             const int bi = (st - s0) % kTileDepth;
             const R r = recbuf[bi * 32 + lane];
             const T rh = rhsbuf[bi * 32 + lane];
-            pipe[kTileLead].pending = 0;
-            if (st + kTileLead < s1)
-                tile_poll<T>(recbuf[((st + kTileLead - s0) % kTileDepth) * 32 + lane], x, pipe[kTileLead]);
             issue(st + kTileDepth, bi);
             if (r.row >= 0) {
-                TilePoll<T> &cur = pipe[0];
-                if (cur.pending) {
+                T xv[FV_TILE_MAXL];
+                unsigned pending = 0;
+#pragma unroll
+                for (int q = 0; q < FV_TILE_MAXL; ++q) {
+                    xv[q] = T(0);
+                    if (r.ds[q] >= 0 && !fv_slot_ready(&x[r.ds[q]], xv[q])) pending |= 1u << q;
+                }
+                if (pending) {
                     const unsigned long long t0 = fv_globaltimer();
-                    for (unsigned it = 1; cur.pending; ++it) {
+                    for (unsigned it = 1; pending; ++it) {
 #pragma unroll
                         for (int q = 0; q < FV_TILE_MAXL; ++q)
-                            if ((cur.pending >> q) & 1u)
-                                if (fv_slot_ready(&x[r.ds[q]], cur.xv[q])) cur.pending &= ~(1u << q);
-                        if (cur.pending && (it & 255u) == 0) {
+                            if ((pending >> q) & 1u)
+                                if (fv_slot_ready(&x[r.ds[q]], xv[q])) pending &= ~(1u << q);
+                        if (pending && (it & 255u) == 0) {
                             if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
                                 if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
 #pragma unroll
                                 for (int q = 0; q < FV_TILE_MAXL; ++q)
-                                    if ((cur.pending >> q) & 1u) cur.xv[q] = T(NAN);
-                                cur.pending = 0;
+                                    if ((pending >> q) & 1u) xv[q] = T(NAN);
+                                pending = 0;
                             }
                         }
                     }
@@ -791,7 +764,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, con
                 T s = rh;
 #pragma unroll
                 for (int q = 0; q < FV_TILE_MAXL; ++q)
-                    if (r.ds[q] != FV_TILE_PAD) s = s - r.v[q] * (r.ds[q] < 0 ? ring[-r.ds[q] - 1] : cur.xv[q]);
+                    if (r.ds[q] != FV_TILE_PAD) s = s - r.v[q] * (r.ds[q] < 0 ? ring[-r.ds[q] - 1] : xv[q]);
                 const T res = UNIT ? s : r.d * s;
                 ring[((st - s0) % FV_TILE_RING) * 32 + lane] = res;
                 fv_publish(&x[r.row], res);
@@ -799,8 +772,6 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, con
                 if (rhs_reset) fv_reset_slot(&rhs_reset[r.row]);
                 if (next_reset) fv_reset_slot(&next_reset[r.row]);
             }
-#pragma unroll
-            for (int k = 0; k < kTileLead; ++k) pipe[k] = pipe[k + 1];
             __syncwarp();
         }
     }
