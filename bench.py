@@ -484,7 +484,8 @@ def batch_problems(fv, count, seed, rank):
 
 
 def batch_arm(args, rank, world, local_rank):
-    """Batched mixed-precision CG + IC(0) over 1,024 independent 2D problems."""
+    """Batched CG + IC(0) over 1,024 independent 2D problems, FP64 or FP32 inner
+    with FP64 refinement (the faster of the two in a warm-up trial by default)."""
     import torch
     torch.cuda.set_device(local_rank)
     from fvb200.build import build
@@ -508,17 +509,35 @@ def batch_arm(args, rank, world, local_rank):
     x = fv.DistributedVector.from_size(mb.n_cells)
     tile, tile_times = autotune_tile(A, mb.cell_offsets, P, b, x)
     solver = BatchCG(A, mb.cell_offsets, tile)
-    opts = dict(precision="mixed", outer_tolerance=BATCH_OUTER_TOL, inner_relative_tolerance=1e-2, max_outer=30,
-                max_iterations=20000)
+    # both precisions reach the same FP64 target |b - A x| / |b| <= 1e-10 per problem
+    opts_by = {"mixed": dict(precision="mixed", outer_tolerance=BATCH_OUTER_TOL, inner_relative_tolerance=1e-2,
+                             max_outer=30, max_iterations=20000),
+               "fp64": dict(precision="fp64", relative_tolerance=BATCH_OUTER_TOL,
+                            absolute_tolerance=BATCH_OUTER_TOL, max_iterations=20000)}
+    choice = args.batch_precision if args.batch_precision != "auto" else "mixed"
 
-    def step():
+    def step(prec=None):
         nonlocal b
         _, b = fv.assemble(eq, bc, mb, lhs=A)
         P.refactor()
-        return solver.solve(P, b, x, **opts)
+        return solver.solve(P, b, x, **opts_by[prec or choice])
 
-    for _ in range(args.warmup):
-        out = step()
+    # precision autotune: one warm-up step of each, the faster one is timed
+    trial = {}
+    for k in range(args.warmup):
+        prec = None
+        if args.batch_precision == "auto" and k < 2:
+            prec = ("mixed", "fp64")[k]
+        w0 = torch.cuda.Event(enable_timing=True)
+        w1 = torch.cuda.Event(enable_timing=True)
+        w0.record(stream)
+        out = step(prec)
+        w1.record(stream)
+        torch.cuda.synchronize()
+        if prec:
+            trial[prec] = w0.elapsed_time(w1) / 1e3
+            if len(trial) == 2:
+                choice = min(trial, key=trial.get)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -543,20 +562,20 @@ def batch_arm(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
     out = outs[-1]
-    # the same batch in FP64 (reference semantics per problem, rtol 1e-8), one timed step
+    # the other precision, one timed step (the same accuracy target)
+    other = "fp64" if choice == "mixed" else "mixed"
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
+    xo = fv.DistributedVector.from_size(mb.n_cells)
     f0.record(stream)
     _, b = fv.assemble(eq, bc, mb, lhs=A)
     P.refactor()
-    x64 = fv.DistributedVector.from_size(mb.n_cells)
-    out64 = solver.solve(P, b, x64, precision="fp64", relative_tolerance=RTOL, absolute_tolerance=RTOL,
-                         max_iterations=20000)
+    out_other = solver.solve(P, b, xo, **opts_by[other])
     f1.record(stream)
     torch.cuda.synchronize()
-    t_fp64_batch = f0.elapsed_time(f1) / 1e3
-    del x64
+    t_other = f0.elapsed_time(f1) / 1e3
+    del xo
     # accuracy: every problem's true FP64 residual; error against a tight FP64
     # solve on a sample of problems (each solved alone, plain FP64 path)
     rng = np.random.default_rng(11)
@@ -587,7 +606,8 @@ def batch_arm(args, rank, world, local_rank):
     # drawn from the same distribution, so solves/s = 1 / mean(time)
     plain_solves = 1.0 / float(np.mean(plain_t))
     return dict(elapsed=elapsed, out=out, launches=launches, clocks=clocks, t_mesh=t_mesh, N=mb.n_cells,
-                t_fp64_batch=t_fp64_batch, it64_max=int(np.max(out64["iterations"])),
+                choice=choice, trial=trial, other=other, t_other=t_other,
+                other_it_max=int(np.max(out_other["iterations"])),
                 nnz=A.shape()[2], tile=tile, tile_times=tile_times, errs=errs, plain_solves=plain_solves,
                 sample=len(sample), sides=sides, levels=P.levels()[2:], schedule=sweep_schedule(P))
 
@@ -616,7 +636,11 @@ def serve_arm(args, rank, world, local_rank):
         else:
             r.side = max(4, int(round(r.side / 4.0)) * 4)
             r.cells = 6 * r.side ** 3
-    srv = Server(fv, workers=args.serve_workers, max_wave_cells=24_000_000, max_wave_requests=256)
+    import functools
+
+    from fvb200.serve import solve_wave
+    srv = Server(fv, workers=args.serve_workers, max_wave_cells=24_000_000, max_wave_requests=256,
+                 solve_fn=functools.partial(solve_wave, precision=args.serve_precision))
     t0 = time.time()
     keys = sorted({(r.kind, r.side) for r in reqs})
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
@@ -656,8 +680,10 @@ def serve_arm(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": round(stats["solves_per_s"], 3), "unit": "solves/s", "n_gpus": world,
         "steps": 1, "warmup": 1, "ms_per_step": round(stats["wall_s"] * 1e3, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-refinement", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-inner/f64-refinement" if args.serve_precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": args.workload, "arrival_rate_per_s": args.serve_rate,
+                   "precision": args.serve_precision,
                    "arrival_window_s": args.serve_duration, "requests": len(reqs),
                    "mix": "50% 2D diffusion (CG+IC0) / 50% 3D convection-diffusion (BiCGStab+ILU0)",
                    "sizes": "lognormal, 1st/99th pct 10k/2M cells, clipped; 2D sides x16, 3D sides x4",
@@ -682,22 +708,27 @@ def main_batch(args, rank, world, local_rank):
     out = res["out"]
     its = out["iterations"]
     cells = np.diff(np.asarray([0] + list(np.cumsum([2 * int(s) ** 2 for s in res["sides"]]))))
+    mixed = res["choice"] == "mixed"
+    prec_name = {"mixed": "FP32 CG + FP32 IC(0) inside FP64 refinement", "fp64": "FP64 CG + IC(0)"}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(res["elapsed"] / K * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-refinement", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-refinement" if mixed else "f64",
+        "data": "synthetic",
         "config": {"workload": args.workload, "problems": args.batch_count, "cells_total": res["N"],
                    "nnz": res["nnz"], "sides": "log-uniform [32,512]", "solver": "batched CG+IC(0)",
-                   "precision": "FP32 CG + FP32 IC(0) inside FP64 refinement", "outer_tolerance": BATCH_OUTER_TOL,
+                   "precision": prec_name[res["choice"]], "precision_choice": args.batch_precision,
+                   "target": f"|b-Ax|/|b| <= {BATCH_OUTER_TOL} per problem",
                    "tile_rows": res["tile"], "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "precision_trial_s": {k: round(v, 3) for k, v in res["trial"].items()},
+        f"{res['other']}_batched_solves_per_s": round(args.batch_count / res["t_other"], 3),
+        f"{res['other']}_batched_iterations_max": res["other_it_max"],
         "dof_iters_per_s": round(float(np.sum(cells * its)) * K * world / res["elapsed"], 1),
         "max_rel_err_vs_fp64": max(res["errs"]) if res["errs"] else None, "err_sample": res["sample"],
         "max_final_residual": float(np.max(out["final_residual"])),
         "plain_fp64_solves_per_s": round(res["plain_solves"], 4),
-        "fp64_batched_solves_per_s": round(args.batch_count / res["t_fp64_batch"], 3),
-        "fp64_batched_iterations_max": res["it64_max"],
         "speedup_vs_plain_fp64": round(value / res["plain_solves"] / world, 2),
-        "outer_steps_max": int(np.max(out["outer_steps"])), "inner_iterations_max": int(np.max(its)),
+        "outer_steps_max": int(np.max(out["outer_steps"])), "iterations_max": int(np.max(its)),
         "fp64_fallback_problems": int(np.sum(out["fp64_fallback"])),
         "launched_iterations": int(out["launched_iterations"]), "levels_fwd_bwd": list(res["levels"]),
         "sweep_schedule": res["schedule"],
@@ -718,6 +749,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=1024)
     ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--batch-precision", default="auto", choices=["auto", "mixed", "fp64"])
+    ap.add_argument("--serve-precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-duration", type=float, default=0.25)
     ap.add_argument("--serve-workers", type=int, default=3)

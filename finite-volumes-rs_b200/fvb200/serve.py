@@ -106,8 +106,11 @@ def request_fields(m, req: Request):
 BYTES_PER_CELL = {"2d": 700, "3d": 1100}   # resident estimate: mesh, CSR, factors, FP32 copies, vectors
 
 
-def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol=1e-10, keep_solution=False):
-    """Pack requests of one kind into one batch and solve it on `stream`."""
+def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol=1e-10, keep_solution=False,
+               precision="mixed"):
+    """Pack requests of one kind into one batch and solve it on `stream` to
+    |b - A x| / |b| <= outer_tol per request: FP32 Krylov inside FP64
+    refinement (precision "mixed") or FP64 throughout ("fp64")."""
     import torch
     kind = reqs[0].kind
     with torch.cuda.stream(stream):
@@ -133,9 +136,14 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
         P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(A, 0, stream=stream)
         x = fv.DistributedVector.from_size(mb.n_cells)
         solver = BatchCG(A, mb.cell_offsets, tile_rows, stream=stream)
-        out = solver.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-2,
-                           max_outer=30, max_iterations=20000, stream=stream,
-                           solver="cg" if kind == "2d" else "bicgstab")
+        if precision == "mixed":
+            out = solver.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-2,
+                               max_outer=30, max_iterations=20000, stream=stream,
+                               solver="cg" if kind == "2d" else "bicgstab")
+        else:
+            out = solver.solve(P, b, x, precision="fp64", relative_tolerance=outer_tol,
+                               absolute_tolerance=outer_tol, max_iterations=20000, stream=stream,
+                               solver="cg" if kind == "2d" else "bicgstab")
         xs = x.data.cpu().numpy() if keep_solution else None
         stream.synchronize()
         for k, r in enumerate(reqs):
