@@ -140,8 +140,6 @@ class Clocks:
 def sweep_schedule(P):
     """Which sweep schedule the preconditioner uses, with its box-tile plan."""
     act, st = P.schedule()
-    if act == 3:
-        return {"kind": "level chunks, row records"}
     if act != 2:
         return {"kind": "level chunks"}
     return {"kind": "box tiles", "box_edge_cells": float(st[0]), "boxes": int(st[1]),

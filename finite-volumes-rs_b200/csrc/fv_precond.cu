@@ -104,11 +104,6 @@ struct fv_precond {
     float *t_rhs32[2] = {nullptr, nullptr};
     unsigned t_rec64_epoch = 0, t_rec32_version = 0;
     unsigned f32_version = 0;  // incremented by every fv_precond_make_f32
-    // level-chunk sweeps with one record per row in level order (schedule 3)
-    void *c_rec64[2] = {nullptr, nullptr}, *c_rec32[2] = {nullptr, nullptr};
-    unsigned c_rec64_epoch = 0, c_rec32_version = 0;
-    const int32_t *c_rec64_group = nullptr, *c_rec32_group = nullptr;  // row groups the records carry
-    bool c_rec64_built = false, c_rec32_built = false;
 };
 
 // ------------------------------------------------------------------ symbolic
@@ -879,127 +874,6 @@ static fv_status tiled_apply(fv_precond *P, const T *r, T *z, T *tmp, cudaStream
     return FV_OK;
 }
 
-// Level-chunk sweep whose rows come as records in level order (the same
-// 64 / 48-byte layout as the tiled records: entries, columns, 1/diagonal,
-// row, and the row's group for batches).  A warp's chunk is one coalesced
-// load of 32 records; its right-hand sides and dependency polls follow
-// directly from it, two dependent round trips instead of four (position ->
-// row -> row bounds -> entries -> polls).  Arithmetic as k_sweep.
-template <typename T>
-__global__ void k_chunk_records(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ ptr,
-                                const int32_t *__restrict__ col, const T *__restrict__ val,
-                                const T *__restrict__ dinv, const int32_t *__restrict__ group,
-                                TileRec<T> *__restrict__ rec) {
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
-        TileRec<T> r;
-        const int32_t row = order[u];
-        const int32_t k0 = ptr[row], m = ptr[row + 1] - k0;
-        r.row = row;
-        r.next = group ? group[row] : -1;
-#pragma unroll
-        for (int q = 0; q < FV_TILE_MAXL; ++q) {
-            r.v[q] = q < m ? val[k0 + q] : T(0);
-            r.ds[q] = q < m ? col[k0 + q] : FV_TILE_PAD;
-        }
-        r.d = dinv ? dinv[row] : T(1);
-        if constexpr (sizeof(T) == 4) r.pad = 0;
-        rec[u] = r;
-    }
-}
-
-template <typename T, bool UNIT>
-__global__ void __launch_bounds__(256) k_sweep_rec(int64_t n, const TileRec<T> *__restrict__ rec, const T *rhs,
-                                                   T *x, T *rhs_reset, T *next_reset, unsigned *ctrl, int *err,
-                                                   const int *skip, fv_row_skip rs) {
-    if (skip && *(volatile const int *)skip) return;
-    const int64_t nchunks = (n + 31) / 32;
-    int64_t chunk;
-    while (take_chunk(&ctrl[0], nchunks, chunk)) {
-        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
-        if (idx >= n) continue;
-        const TileRec<T> r = rec[idx];
-        const int i = r.row;
-        // converged problem of a batch: its rows and their dependencies are skipped together
-        if (rs.group && rs.done[(int64_t)r.next * rs.stride]) continue;
-        T s = rhs[i];
-        T xv[FV_TILE_MAXL];
-        unsigned pending = 0;
-#pragma unroll
-        for (int q = 0; q < FV_TILE_MAXL; ++q) {
-            xv[q] = T(0);
-            if (r.ds[q] != FV_TILE_PAD && !fv_slot_ready(&x[r.ds[q]], xv[q])) pending |= 1u << q;
-        }
-        if (pending) {
-            const unsigned long long t0 = fv_globaltimer();
-            for (unsigned it = 1; pending; ++it) {
-#pragma unroll
-                for (int q = 0; q < FV_TILE_MAXL; ++q)
-                    if ((pending >> q) & 1u)
-                        if (fv_slot_ready(&x[r.ds[q]], xv[q])) pending &= ~(1u << q);
-                if (pending && (it & 255u) == 0) {
-                    if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
-                        if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
-#pragma unroll
-                        for (int q = 0; q < FV_TILE_MAXL; ++q)
-                            if ((pending >> q) & 1u) xv[q] = T(NAN);
-                        pending = 0;
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < FV_TILE_MAXL; ++q)
-            if (r.ds[q] != FV_TILE_PAD) s = s - r.v[q] * xv[q];
-        const T res = UNIT ? s : r.d * s;
-        fv_publish(&x[i], res);
-        if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
-        if (next_reset) fv_reset_slot(&next_reset[i]);
-    }
-    leave(&ctrl[0], &ctrl[1]);
-}
-
-static bool use_chunk_records(const fv_precond *P) {
-    const fv_symbolic *s = P->sym;
-    return P->schedule == 3 && s->max_lower <= FV_TILE_MAXL && s->max_upper <= FV_TILE_MAXL;
-}
-
-template <typename T>
-static fv_status chunk_records_prepare(fv_precond *P, cudaStream_t st, const fv_row_skip &rs) {
-    const fv_symbolic *s = P->sym;
-    const int64_t n = P->n;
-    void **rec = sizeof(T) == 8 ? P->c_rec64 : P->c_rec32;
-    const unsigned version = sizeof(T) == 8 ? P->epoch : P->f32_version;
-    unsigned &seen = sizeof(T) == 8 ? P->c_rec64_epoch : P->c_rec32_version;
-    const int32_t *&grp = sizeof(T) == 8 ? P->c_rec64_group : P->c_rec32_group;
-    bool &built = sizeof(T) == 8 ? P->c_rec64_built : P->c_rec32_built;
-    for (int d = 0; d < 2; ++d)
-        if (!rec[d]) FV_CUDA_TRY(cudaMalloc(&rec[d], sizeof(TileRec<T>) * (n ? n : 1)));
-    if (built && seen == version && grp == rs.group) return FV_OK;
-    const T *lv, *uv, *dv;
-    if constexpr (sizeof(T) == 8) {
-        lv = P->l_val;
-        uv = P->u_val;
-        dv = P->dinv;
-    } else {
-        lv = P->l32;
-        uv = P->u32;
-        dv = P->dinv32;
-    }
-    const unsigned G = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
-    if (n) {
-        fv_note_launch(), k_chunk_records<T><<<G, 256, 0, st>>>(n, s->fwd_order, s->l_ptr, s->l_col, lv,
-                                                                P->kind == 2 ? nullptr : dv, rs.group,
-                                                                reinterpret_cast<TileRec<T> *>(rec[0]));
-        fv_note_launch(), k_chunk_records<T><<<G, 256, 0, st>>>(n, s->bwd_order, s->u_ptr, s->u_col, uv, dv, rs.group,
-                                                                reinterpret_cast<TileRec<T> *>(rec[1]));
-        FV_CUDA_TRY(cudaGetLastError());
-    }
-    seen = version;
-    grp = rs.group;
-    built = true;
-    return FV_OK;
-}
-
 static int sweep_grid(int64_t n) {
     int64_t warps = (n + 31) / 32;
     int64_t blocks = (warps + 7) / 8;
@@ -1020,22 +894,6 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
-    if (use_chunk_records(P)) {
-        FV_TRY(chunk_records_prepare<double>(P, st, rs));
-        const TileRec64 *rf = reinterpret_cast<const TileRec64 *>(P->c_rec64[0]);
-        const TileRec64 *rb = reinterpret_cast<const TileRec64 *>(P->c_rec64[1]);
-        if (P->kind == 2)
-            fv_note_launch(), k_sweep_rec<double, true><<<G, 256, 0, st>>>(n, rf, r, P->tmp, nullptr, z, P->ctrl,
-                                                                           P->err, skip, rs);
-        else
-            fv_note_launch(), k_sweep_rec<double, false><<<G, 256, 0, st>>>(n, rf, r, P->tmp, nullptr, z, P->ctrl,
-                                                                            P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        fv_note_launch(), k_sweep_rec<double, false><<<G, 256, 0, st>>>(n, rb, P->tmp, z, P->tmp, nullptr,
-                                                                        P->ctrl + 2, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        return FV_OK;
-    }
     if (P->kind == 2)
         launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -1101,22 +959,6 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
-    if (use_chunk_records(P)) {
-        FV_TRY(chunk_records_prepare<float>(P, st, rs));
-        const TileRec32 *rf = reinterpret_cast<const TileRec32 *>(P->c_rec32[0]);
-        const TileRec32 *rb = reinterpret_cast<const TileRec32 *>(P->c_rec32[1]);
-        if (P->kind == 2)
-            fv_note_launch(), k_sweep_rec<float, true><<<G, 256, 0, st>>>(n, rf, r, P->tmp32, nullptr, z, P->ctrl,
-                                                                          P->err, skip, rs);
-        else
-            fv_note_launch(), k_sweep_rec<float, false><<<G, 256, 0, st>>>(n, rf, r, P->tmp32, nullptr, z, P->ctrl,
-                                                                           P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        fv_note_launch(), k_sweep_rec<float, false><<<G, 256, 0, st>>>(n, rb, P->tmp32, z, P->tmp32, nullptr,
-                                                                       P->ctrl + 2, P->err, skip, rs);
-        FV_CUDA_TRY(cudaGetLastError());
-        return FV_OK;
-    }
     if (P->kind == 2)
         launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
@@ -1131,13 +973,12 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
 }
 
 extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
-    if (!P || request < -1 || request > 3) return FV_ERR_INVALID;
+    if (!P || request < -1 || request > 2) return FV_ERR_INVALID;
     fv_symbolic *s = P->sym;
     if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
     if (request == 2 && !s->tiled) return FV_ERR_UNSUPPORTED;
-    if (request == 3 && (s->max_lower > FV_TILE_MAXL || s->max_upper > FV_TILE_MAXL)) return FV_ERR_UNSUPPORTED;
-    if (request >= 0) P->schedule = request == 0 ? 1 : request;
-    if (active) *active = use_tiles(P) ? 2 : (use_chunk_records(P) ? 3 : 1);
+    if (request >= 0) P->schedule = request == 2 ? 2 : 1;
+    if (active) *active = use_tiles(P) ? 2 : 1;
     if (stats) {
         stats[0] = s->t_edge;
         stats[1] = s->t_nb[0];
@@ -1165,8 +1006,6 @@ extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     cudaFree(P->tmp32);
     cudaFree(P->amap);
     for (int d = 0; d < 2; ++d) {
-        cudaFree(P->c_rec64[d]);
-        cudaFree(P->c_rec32[d]);
         cudaFree(P->t_rec64[d]);
         cudaFree(P->t_rec32[d]);
         cudaFree(P->t_rhs64[d]);

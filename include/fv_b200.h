@@ -277,12 +277,11 @@ fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bw
                             int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream);
 /* Sweep schedule of P.  request: -1 query only; 0 or 1 level chunks (the
  * default); 2 box tiles, available when the matrix was assembled on a mesh
- * whose box order exists (FV_ERR_UNSUPPORTED otherwise); 3 level chunks whose
- * rows come as one record each in level order (rows with at most 4 entries on
- * each side).  *active receives 1, 2 or 3.  stats (optional, 6 doubles): box
- * edge in mean cell sizes, number of boxes, lane use of the forward /
- * backward steps, share of dependencies read from shared memory forward /
- * backward (zeros without a tiling).  All schedules give the same bits. */
+ * whose box order exists (FV_ERR_UNSUPPORTED otherwise).  *active receives
+ * 1 (level chunks) or 2 (box tiles).  stats (optional, 6 doubles): box edge
+ * in mean cell sizes, number of boxes, lane use of the forward / backward
+ * steps, share of dependencies read from shared memory forward / backward
+ * (zeros without a tiling).  Both schedules give the same bits. */
 fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats);
 fv_status fv_precond_destroy(fv_precond *P);
 /* The box-tile plan fv_ic0_factor / fv_ilu0_factor make for a matrix
