@@ -5,6 +5,7 @@ import raises, and every device entry point reports CUDA errors as FvError.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 from pathlib import Path
@@ -157,6 +158,23 @@ _SIGS = {
 }
 
 _lib = None
+_exiting = False
+
+
+def _mark_exit():
+    global _exiting
+    _exiting = True
+
+
+# Python runs atexit handlers before it tears modules down.  From then on the
+# finalizers of device objects skip their native frees: the process is ending
+# (the driver reclaims everything), and native calls from finalizers that run
+# during interpreter teardown, after other libraries' own teardown, are not safe.
+atexit.register(_mark_exit)
+
+
+def exiting() -> bool:
+    return _exiting
 
 
 def lib() -> C.CDLL:

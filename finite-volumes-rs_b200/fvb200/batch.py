@@ -15,7 +15,7 @@ import time
 
 import numpy as np
 
-from ._lib import BatchInfo, BatchOptions, check, lib
+from ._lib import BatchInfo, BatchOptions, check, exiting, lib
 from .streams import stream_handle
 
 FV_BATCH_FP64, FV_BATCH_MIXED = 0, 1
@@ -72,6 +72,8 @@ class MeshBatch:
         return self._device[dev]
 
     def __del__(self):
+        if exiting():
+            return
         try:
             for dm in self._device.values():
                 dm.close()
@@ -118,6 +120,8 @@ class BatchCG:
             self.handle = C.c_void_p()
 
     def __del__(self):
+        if exiting():
+            return
         try:
             self.close()
         except Exception:

@@ -31,7 +31,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import COLLECT_FN, REDUCE_FN, FvComm, FvError, SolverInfo, check, lib
+from ._lib import COLLECT_FN, REDUCE_FN, FvComm, FvError, SolverInfo, check, exiting, lib
 from .linalg import DistributedMatrix, LinearSolverInfo, LinearSolverOptions, _dev_f64
 from .streams import stream_handle
 
@@ -266,6 +266,8 @@ class RankSystem:
         self.matrix.close()
 
     def __del__(self):
+        if exiting():
+            return
         try:
             self.close()
         except Exception:

@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import BcDesc, FvError, SolverInfo, SolverOptions, TermsDesc, check, lib
+from ._lib import BcDesc, FvError, SolverInfo, SolverOptions, TermsDesc, check, exiting, lib
 from .streams import stream_handle
 
 
@@ -125,6 +125,8 @@ class DistributedMatrix:
             self.handle = C.c_void_p()
 
     def __del__(self):
+        if exiting():
+            return
         try:
             self.close()
         except Exception:
@@ -295,6 +297,8 @@ class Preconditioner:
             self.handle = C.c_void_p()
 
     def __del__(self):
+        if exiting():
+            return
         try:
             self.close()
         except Exception:

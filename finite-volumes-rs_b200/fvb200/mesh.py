@@ -11,7 +11,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import HostMesh_, MeshDesc, check, lib
+from ._lib import HostMesh_, MeshDesc, check, exiting, lib
 
 VTK_TRIANGLE, VTK_QUAD, VTK_TETRA, VTK_HEXAHEDRON = 5, 9, 10, 12
 
@@ -56,6 +56,8 @@ class Mesh:
         self._device = {}
 
     def __del__(self):
+        if exiting():
+            return
         try:
             for dm in self._device.values():
                 dm.close()
@@ -192,6 +194,8 @@ class DeviceMesh:
             self.handle = C.c_void_p()
 
     def __del__(self):
+        if exiting():
+            return
         try:
             self.close()
         except Exception:
