@@ -229,6 +229,12 @@ def test_cabi_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_graft_entry_build(fv):
+    """The entry point's build() runs end to end (library, oracle, package import)."""
+    import __graft_entry__
+    __graft_entry__.build()
+
+
 def test_term_algebra(fv):
     k = np.ones(4)
     e = -fv.laplacian(fv.Orthogonal(), k) - fv.source(k)
