@@ -631,6 +631,17 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
 
 }  // namespace
 
+cudaError_t fv_mesh_launch_grad_coeffs(fv_mesh *m, int *dbad, cudaStream_t st) {
+    const unsigned G = (unsigned)((m->n_cells + 127) / 128);
+    if (m->dim == 2)
+        fv_note_launch(), k_grad_coeffs<2><<<G, 128, 0, st>>>(m->n_cells, m->cell, m->face_cells, m->face_center,
+                                                               m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag, dbad);
+    else
+        fv_note_launch(), k_grad_coeffs<3><<<G, 128, 0, st>>>(m->n_cells, m->cell, m->face_cells, m->face_center,
+                                                               m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag, dbad);
+    return cudaGetLastError();
+}
+
 #include <atomic>
 #include <mutex>
 static std::atomic<unsigned long long> g_launches{0};
@@ -830,18 +841,7 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
             e = cudaMemcpyAsync(m->gcf_ptr, d->cell_face_ptr, sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess && ng)
             e = cudaMemcpyAsync(m->gcf_face, d->cell_faces, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) {
-            const unsigned G = (unsigned)((N + 127) / 128);
-            if (dim == 2)
-                fv_note_launch(), k_grad_coeffs<2><<<G, 128, 0, st>>>(N, m->cell, m->face_cells, m->face_center,
-                                                                       m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag,
-                                                                       dbad);
-            else
-                fv_note_launch(), k_grad_coeffs<3><<<G, 128, 0, st>>>(N, m->cell, m->face_cells, m->face_center,
-                                                                       m->gcf_ptr, m->gcf_face, m->gcoef, m->gdiag,
-                                                                       dbad);
-            e = cudaGetLastError();
-        }
+        if (e == cudaSuccess) e = fv_mesh_launch_grad_coeffs(m, dbad, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&gbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging vectors go out of scope

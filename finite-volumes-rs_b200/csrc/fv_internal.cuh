@@ -75,6 +75,11 @@ struct fv_mesh {
     int64_t nnz = -1;
 };
 
+// Gradient coefficients of Mesh::compute (compute.rs:155-203) for a mesh whose
+// cell, face_cells, face_center, gcf_ptr and gcf_face are resident; a cell with
+// a singular gradient matrix sets *dbad.
+cudaError_t fv_mesh_launch_grad_coeffs(fv_mesh *m, int *dbad, cudaStream_t st);
+
 struct fv_symbolic;  // triangular split + level schedules of a pattern (fv_precond.cu)
 
 // Level-k fill patterns of the reference (fv_fill.cu).  From the host CSR

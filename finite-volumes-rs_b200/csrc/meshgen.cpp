@@ -28,6 +28,12 @@
 #include <new>
 #include <vector>
 
+#define FV_RETURN_IF(expr)            \
+    do {                              \
+        const fv_status _s = (expr);  \
+        if (_s != FV_OK) return _s;   \
+    } while (0)
+
 namespace {
 
 // ---------------------------------------------------------------- RNG
@@ -309,6 +315,9 @@ extern "C" fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, co
         for (int64_t b = 0; b < n_bfaces; ++b) {
             int len = bface_node_ptr[b + 1] - bface_node_ptr[b];
             if (len < 2 || len > 4 || bface_marker[b] < 0) return FV_ERR_INVALID;
+            for (int q = 0; q < len; ++q)
+                if (bface_nodes[bface_node_ptr[b] + q] < 0 || bface_nodes[bface_node_ptr[b] + q] >= n_nodes)
+                    return FV_ERR_INVALID;
             FaceKey k = make_key(bface_nodes + bface_node_ptr[b], len);
             bnd.find_or_insert(k, bface_marker[b]);
         }
@@ -318,6 +327,10 @@ extern "C" fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, co
             int nn = vtk_nnodes(k);
             if (nn < 0 || elem_node_ptr[e + 1] - elem_node_ptr[e] != nn) return FV_ERR_INVALID;
             if ((dim == 2) != (k == 5 || k == 9)) return FV_ERR_INVALID;
+            for (int q = 0; q < nn; ++q) {
+                const int32_t id = elem_nodes[elem_node_ptr[e] + q];
+                if (id < 0 || id >= n_nodes) return FV_ERR_INVALID;
+            }
             total_local += (k == 5 ? 3 : (k == 12 ? 6 : 4));
         }
         if (total_local >= 0x7fffffffLL) return FV_ERR_INVALID;
@@ -475,12 +488,35 @@ extern "C" fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, co
     }
 }
 
-extern "C" fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out) {
-    if (n < 1 || n > 8192 || !out) return FV_ERR_INVALID;
+// An element list as fv_host_mesh_from_elements / fv_mesh_build_elements take it.
+namespace {
+struct Elements {
+    int32_t dim = 0;
+    std::vector<double> nodes;
+    std::vector<int32_t> kind, ptr, en, bptr, bn, bm;
+};
+
+fv_status to_host(const Elements &el, fv_host_mesh **out) {
+    return fv_host_mesh_from_elements(el.dim, (int64_t)(el.nodes.size() / el.dim), el.nodes.data(),
+                                      (int64_t)el.kind.size(), el.kind.data(), el.ptr.data(), el.en.data(),
+                                      (int64_t)el.bm.size(), el.bptr.data(), el.bn.data(), el.bm.data(), out);
+}
+
+fv_status to_device(const Elements &el, void *stream, fv_mesh **out, fv_host_mesh **host_out) {
+    return fv_mesh_build_elements(el.dim, (int64_t)(el.nodes.size() / el.dim), el.nodes.data(),
+                                  (int64_t)el.kind.size(), el.kind.data(), el.ptr.data(), el.en.data(),
+                                  (int64_t)el.bm.size(), el.bptr.data(), el.bn.data(), el.bm.data(), stream, out,
+                                  host_out);
+}
+
+fv_status square_elements(int32_t n, double jitter, uint64_t seed, Elements &el) {
+    if (n < 1 || n > 8192) return FV_ERR_INVALID;
     try {
         const int64_t np = (int64_t)(n + 1) * (n + 1);
         const double h = 1.0 / n;
-        std::vector<double> nodes((size_t)np * 2);
+        el.dim = 2;
+        std::vector<double> &nodes = el.nodes;
+        nodes.assign((size_t)np * 2, 0.0);
         Rng rng(seed);
         for (int j = 0; j <= n; ++j)
             for (int i = 0; i <= n; ++i) {
@@ -494,7 +530,10 @@ extern "C" fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint
                 nodes[p * 2 + 1] = y;
             }
         const int64_t ne = 2LL * n * n;
-        std::vector<int32_t> kind((size_t)ne, 5), ptr((size_t)ne + 1), en((size_t)ne * 3);
+        el.kind.assign((size_t)ne, 5);
+        el.ptr.assign((size_t)ne + 1, 0);
+        el.en.assign((size_t)ne * 3, 0);
+        std::vector<int32_t> &ptr = el.ptr, &en = el.en;
         int64_t e = 0;
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
@@ -505,7 +544,7 @@ extern "C" fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint
             }
         for (int64_t q = 0; q <= ne; ++q) ptr[q] = (int32_t)(3 * q);
         // one boundary marker (id 0) holding every boundary edge
-        std::vector<int32_t> bptr, bn, bm;
+        std::vector<int32_t> &bptr = el.bptr, &bn = el.bn, &bm = el.bm;
         bptr.push_back(0);
         auto add_edge = [&](int32_t u, int32_t v) {
             bn.push_back(u);
@@ -519,20 +558,21 @@ extern "C" fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint
             add_edge(i * (n + 1), (i + 1) * (n + 1));
             add_edge(i * (n + 1) + n, (i + 1) * (n + 1) + n);
         }
-        return fv_host_mesh_from_elements(2, np, nodes.data(), ne, kind.data(), ptr.data(), en.data(),
-                                          (int64_t)bm.size(), bptr.data(), bn.data(), bm.data(), out);
+        return FV_OK;
     } catch (const std::bad_alloc &) {
         return FV_ERR_ALLOC;
     }
 }
 
-extern "C" fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out) {
-    if (n < 1 || n > 1000 || !out) return FV_ERR_INVALID;
+fv_status cube_elements(int32_t n, double jitter, uint64_t seed, Elements &el) {
+    if (n < 1 || n > 1000) return FV_ERR_INVALID;
     try {
         const int64_t n1 = n + 1;
         const int64_t np = n1 * n1 * n1;
         const double h = 1.0 / n;
-        std::vector<double> nodes((size_t)np * 3);
+        el.dim = 3;
+        std::vector<double> &nodes = el.nodes;
+        nodes.assign((size_t)np * 3, 0.0);
         Rng rng(seed);
         for (int k = 0; k <= n; ++k)
             for (int j = 0; j <= n; ++j)
@@ -549,7 +589,10 @@ extern "C" fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64
                     nodes[p * 3 + 2] = z;
                 }
         const int64_t ne = 6LL * n * n * n;
-        std::vector<int32_t> kind((size_t)ne, 10), ptr((size_t)ne + 1), en((size_t)ne * 4);
+        el.kind.assign((size_t)ne, 10);
+        el.ptr.assign((size_t)ne + 1, 0);
+        el.en.assign((size_t)ne * 4, 0);
+        std::vector<int32_t> &ptr = el.ptr, &en = el.en;
         // Kuhn split: the 6 monotone paths from corner (0,0,0) to (1,1,1).
         const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
         const int64_t stride[3] = {1, n1, n1 * n1};
@@ -581,7 +624,7 @@ extern "C" fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64
             if (k == n) m |= 32u;
             return m;
         };
-        std::vector<int32_t> bptr, bn, bm;
+        std::vector<int32_t> &bptr = el.bptr, &bn = el.bn, &bm = el.bm;
         bptr.push_back(0);
         int32_t fn[24];
         int fs[8];
@@ -598,11 +641,41 @@ extern "C" fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64
                 }
             }
         }
-        return fv_host_mesh_from_elements(3, np, nodes.data(), ne, kind.data(), ptr.data(), en.data(),
-                                          (int64_t)bm.size(), bptr.data(), bn.data(), bm.data(), out);
+        return FV_OK;
     } catch (const std::bad_alloc &) {
         return FV_ERR_ALLOC;
     }
+}
+}  // namespace
+
+extern "C" fv_status fv_host_mesh_generate_square(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out) {
+    if (!out) return FV_ERR_INVALID;
+    Elements el;
+    FV_RETURN_IF(square_elements(n, jitter, seed, el));
+    return to_host(el, out);
+}
+
+extern "C" fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64_t seed, fv_host_mesh **out) {
+    if (!out) return FV_ERR_INVALID;
+    Elements el;
+    FV_RETURN_IF(cube_elements(n, jitter, seed, el));
+    return to_host(el, out);
+}
+
+extern "C" fv_status fv_mesh_build_square(int32_t n, double jitter, uint64_t seed, void *stream, fv_mesh **out,
+                                          fv_host_mesh **host_out) {
+    if (!out) return FV_ERR_INVALID;
+    Elements el;
+    FV_RETURN_IF(square_elements(n, jitter, seed, el));
+    return to_device(el, stream, out, host_out);
+}
+
+extern "C" fv_status fv_mesh_build_cube(int32_t n, double jitter, uint64_t seed, void *stream, fv_mesh **out,
+                                        fv_host_mesh **host_out) {
+    if (!out) return FV_ERR_INVALID;
+    Elements el;
+    FV_RETURN_IF(cube_elements(n, jitter, seed, el));
+    return to_device(el, stream, out, host_out);
 }
 
 extern "C" fv_status fv_host_fields_generate(const fv_host_mesh *m, uint64_t seed, double kappa0, double sigma,
@@ -655,9 +728,9 @@ extern "C" fv_status fv_host_fields_generate(const fv_host_mesh *m, uint64_t see
 // ignored), MARKER_TAG / MARKER_ELEMS boundary lines (markers numbered 0, 1,
 // ... in file order, a face's key = its sorted nodes), then the same face
 // numbering and geometry as fv_host_mesh_from_elements.
-extern "C" fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_host_mesh **out) {
-    if (!path || !out) return FV_ERR_INVALID;
-    *out = nullptr;
+namespace {
+fv_status su2_elements(const char *path, int32_t dim, Elements &el) {
+    if (!path) return FV_ERR_INVALID;
     FILE *fp = fopen(path, "r");
     if (!fp) return FV_ERR_INVALID;
     std::vector<std::string> lines;
@@ -700,8 +773,12 @@ extern "C" fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_hos
             if (value_after(l, "NDIME=", ndime)) break;
         const int d = dim > 0 ? dim : (int)ndime;
         if (d != 2 && d != 3) return FV_ERR_INVALID;
-        std::vector<double> nodes;
-        std::vector<int32_t> kind, eptr(1, 0), enodes, bptr(1, 0), bnodes, bmark;
+        el.dim = d;
+        std::vector<double> &nodes = el.nodes;
+        std::vector<int32_t> &kind = el.kind, &eptr = el.ptr, &enodes = el.en, &bptr = el.bptr, &bnodes = el.bn,
+                             &bmark = el.bm;
+        eptr.assign(1, 0);
+        bptr.assign(1, 0);
         int marker = -1;
         for (size_t li = 0; li < lines.size(); ++li) {
             long long cnt = 0;
@@ -742,10 +819,26 @@ extern "C" fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_hos
             }
         }
         if (kind.empty() || nodes.empty()) return FV_ERR_INVALID;
-        return fv_host_mesh_from_elements(d, (int64_t)(nodes.size() / d), nodes.data(), (int64_t)kind.size(),
-                                          kind.data(), eptr.data(), enodes.data(), (int64_t)bmark.size(),
-                                          bptr.data(), bnodes.data(), bmark.data(), out);
+        return FV_OK;
     } catch (const std::bad_alloc &) {
         return FV_ERR_ALLOC;
     }
+}
+}  // namespace
+
+extern "C" fv_status fv_host_mesh_read_su2(const char *path, int32_t dim, fv_host_mesh **out) {
+    if (!path || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    Elements el;
+    FV_RETURN_IF(su2_elements(path, dim, el));
+    return to_host(el, out);
+}
+
+extern "C" fv_status fv_mesh_build_su2(const char *path, int32_t dim, void *stream, fv_mesh **out,
+                                       fv_host_mesh **host_out) {
+    if (!path || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    Elements el;
+    FV_RETURN_IF(su2_elements(path, dim, el));
+    return to_device(el, stream, out, host_out);
 }

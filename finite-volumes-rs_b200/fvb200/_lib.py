@@ -117,6 +117,10 @@ _SIGS = {
                                 dp, dp, dp],
     # device objects
     "fv_mesh_upload": [P(MeshDesc), vp, P(vp)],
+    "fv_mesh_build_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_build_su2": [C.c_char_p, C.c_int32, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_build_square": [C.c_int32, C.c_double, C.c_uint64, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_build_cube": [C.c_int32, C.c_double, C.c_uint64, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_destroy": [vp],
     "fv_compute_gradients": [vp, vp, P(BcDesc), vp, vp],
     "fv_assemble": [vp, P(TermsDesc), P(BcDesc), P(vp), vp, vp],

@@ -72,9 +72,9 @@ class MeshBatch:
         return self._device[dev]
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             for dm in self._device.values():
                 dm.close()
         except Exception:
@@ -120,9 +120,9 @@ class BatchCG:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             self.close()
         except Exception:
             pass

@@ -266,9 +266,9 @@ class RankSystem:
         self.matrix.close()
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             self.close()
         except Exception:
             pass

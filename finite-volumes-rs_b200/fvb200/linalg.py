@@ -125,9 +125,9 @@ class DistributedMatrix:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             self.close()
         except Exception:
             pass
@@ -297,9 +297,9 @@ class Preconditioner:
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             self.close()
         except Exception:
             pass

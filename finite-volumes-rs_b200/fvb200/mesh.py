@@ -56,9 +56,9 @@ class Mesh:
         self._device = {}
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             for dm in self._device.values():
                 dm.close()
             if self._h:
@@ -68,9 +68,26 @@ class Mesh:
             pass
 
     # -- construction ------------------------------------------------------
+    # Every constructor takes on_device: False builds faces and geometry on the
+    # host (fv_host_mesh_*); True builds them on the current GPU
+    # (fv_mesh_build_*), keeps that device mesh for assemble and reads the same
+    # arrays back into this object.
+    @classmethod
+    def _built_on_device(cls, call, what, stream) -> "Mesh":
+        import torch
+
+        from .streams import stream_handle
+        dev = torch.cuda.current_device()
+        h = C.c_void_p()
+        out = C.POINTER(HostMesh_)()
+        check(call(stream_handle(stream), C.byref(h), C.byref(out)), what)
+        m = cls(out)
+        m._device[dev] = DeviceMesh.adopt(m, h)
+        return m
+
     @classmethod
     def from_elements(cls, dim, nodes, elem_kind, elem_node_ptr, elem_nodes, bface_node_ptr=None,
-                      bface_nodes=None, bface_marker=None) -> "Mesh":
+                      bface_nodes=None, bface_marker=None, on_device: bool = False, stream=None) -> "Mesh":
         nodes = np.ascontiguousarray(nodes, dtype=np.float64).reshape(-1)
         ek = np.ascontiguousarray(elem_kind, dtype=np.int32)
         ep = np.ascontiguousarray(elem_node_ptr, dtype=np.int32)
@@ -85,8 +102,14 @@ class Mesh:
             bn = np.ascontiguousarray(bface_nodes, dtype=np.int32)
             bm = np.ascontiguousarray(bface_marker, dtype=np.int32)
             nb = len(bm)
-        out = C.POINTER(HostMesh_)()
         P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        if on_device:
+            return cls._built_on_device(
+                lambda st, h, o: lib().fv_mesh_build_elements(
+                    dim, len(nodes) // dim, P(nodes, C.c_double), len(ek), P(ek, C.c_int32), P(ep, C.c_int32),
+                    P(en, C.c_int32), nb, P(bp, C.c_int32), P(bn, C.c_int32), P(bm, C.c_int32), st, h, o),
+                "Mesh.from_elements(on_device)", stream)
+        out = C.POINTER(HostMesh_)()
         check(lib().fv_host_mesh_from_elements(dim, len(nodes) // dim, P(nodes, C.c_double), len(ek),
                                                P(ek, C.c_int32), P(ep, C.c_int32), P(en, C.c_int32), nb,
                                                P(bp, C.c_int32), P(bn, C.c_int32), P(bm, C.c_int32),
@@ -94,20 +117,29 @@ class Mesh:
         return cls(out)
 
     @classmethod
-    def read_su2(cls, path, dim: int = 0) -> "Mesh":
+    def read_su2(cls, path, dim: int = 0, on_device: bool = False, stream=None) -> "Mesh":
         """Mesh::read_su2 (core/mesh/io.rs:489-533); dim 0 = NDIME of the file."""
+        if on_device:
+            return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_su2(str(path).encode(), int(dim), st, h, o),
+                                        "Mesh.read_su2(on_device)", stream)
         out = C.POINTER(HostMesh_)()
         check(lib().fv_host_mesh_read_su2(str(path).encode(), int(dim), C.byref(out)), "Mesh.read_su2")
         return cls(out)
 
     @classmethod
-    def square(cls, n: int, jitter: float = 0.0, seed: int = 0) -> "Mesh":
+    def square(cls, n: int, jitter: float = 0.0, seed: int = 0, on_device: bool = False, stream=None) -> "Mesh":
+        if on_device:
+            return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_square(n, jitter, seed, st, h, o),
+                                        "Mesh.square(on_device)", stream)
         out = C.POINTER(HostMesh_)()
         check(lib().fv_host_mesh_generate_square(n, jitter, seed, C.byref(out)), "Mesh.square")
         return cls(out)
 
     @classmethod
-    def cube(cls, n: int, jitter: float = 0.0, seed: int = 0) -> "Mesh":
+    def cube(cls, n: int, jitter: float = 0.0, seed: int = 0, on_device: bool = False, stream=None) -> "Mesh":
+        if on_device:
+            return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_cube(n, jitter, seed, st, h, o),
+                                        "Mesh.cube(on_device)", stream)
         out = C.POINTER(HostMesh_)()
         check(lib().fv_host_mesh_generate_cube(n, jitter, seed, C.byref(out)), "Mesh.cube")
         return cls(out)
@@ -188,15 +220,24 @@ class DeviceMesh:
         self.handle = C.c_void_p()
         check(lib().fv_mesh_upload(C.byref(d), stream_handle(stream), C.byref(self.handle)), "fv_mesh_upload")
 
+    @classmethod
+    def adopt(cls, mesh: Mesh, handle: C.c_void_p) -> "DeviceMesh":
+        """Wrap an fv_mesh built on the device (fv_mesh_build_*) for this mesh."""
+        dm = cls.__new__(cls)
+        dm.mesh = mesh
+        dm._keep = []
+        dm.handle = handle
+        return dm
+
     def close(self):
         if self.handle:
             lib().fv_mesh_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def __del__(self):
-        if exiting():
-            return
         try:
+            if exiting():  # module globals may already be gone at interpreter teardown
+                return
             self.close()
         except Exception:
             pass

@@ -218,6 +218,28 @@ typedef struct fv_solver_info {
 fv_status fv_mesh_upload(const fv_mesh_desc *desc, void *stream, fv_mesh **out);
 fv_status fv_mesh_destroy(fv_mesh *m);
 
+/* Mesh::read_su2's face numbering (io.rs:364-533, mod.rs:451-529) and
+ * Mesh::compute (compute.rs:12-375) on the device: from the element list of
+ * fv_host_mesh_from_elements (host pointers) to a resident fv_mesh, gradient
+ * coefficients included, with no host pass over faces or cells.  The arrays
+ * equal fv_host_mesh_from_elements' bit for bit; host_out (optional, NULL to
+ * skip) receives them as an fv_host_mesh (free with fv_host_mesh_free).
+ * Replaces the caller-side Mesh::read_su2 + Mesh::compute before assemble. */
+fv_status fv_mesh_build_elements(int32_t dim, int64_t n_nodes, const double *nodes,
+                                 int64_t n_elems, const int32_t *elem_kind,
+                                 const int32_t *elem_node_ptr, const int32_t *elem_nodes,
+                                 int64_t n_bfaces, const int32_t *bface_node_ptr,
+                                 const int32_t *bface_nodes, const int32_t *bface_marker,
+                                 void *stream, fv_mesh **out, fv_host_mesh **host_out);
+/* The same from an SU2 file (the parser of fv_host_mesh_read_su2) and from the
+ * synthetic generators (fv_host_mesh_generate_square / _cube). */
+fv_status fv_mesh_build_su2(const char *path, int32_t dim, void *stream, fv_mesh **out,
+                            fv_host_mesh **host_out);
+fv_status fv_mesh_build_square(int32_t n, double jitter, uint64_t seed, void *stream, fv_mesh **out,
+                               fv_host_mesh **host_out);
+fv_status fv_mesh_build_cube(int32_t n, double jitter, uint64_t seed, void *stream, fv_mesh **out,
+                             fv_host_mesh **host_out);
+
 /* compute_gradients (fvm/tools/gradients.rs:48-86): least-squares cell
  * gradients of a cell field, grad[c] = values[c] * own_c + sum over the
  * cell's faces (mesh order) of value_other * g_k, a boundary face taking

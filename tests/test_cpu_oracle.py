@@ -247,3 +247,20 @@ def test_term_algebra(fv):
         fv.laplacian(fv.Orthogonal(), k) + fv.laplacian(fv.Orthogonal(), k)
     with pytest.raises(NotImplementedError):
         fv.laplacian(object(), k)
+
+
+def test_host_builder_rejects_bad_node_ids(fv):
+    """Element or boundary node ids outside [0, n_nodes) are FV_ERR_INVALID, not a read out of bounds."""
+    from fvb200._lib import FvError
+    nodes = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
+    kinds, eptr = np.array([5], np.int32), np.array([0, 3], np.int32)
+    bptr = np.array([0, 2, 4, 6], np.int32)
+    bm = np.zeros(3, np.int32)
+    good_bn = np.array([0, 1, 1, 2, 2, 0], np.int32)
+    m = fv.Mesh.from_elements(2, nodes, kinds, eptr, np.array([0, 1, 2], np.int32), bptr, good_bn, bm)
+    assert m.n_cells == 1 and m.n_boundary_faces == 3
+    for en, bn in ((np.array([0, 1, 3], np.int32), good_bn), (np.array([0, 1, 2], np.int32),
+                                                                np.array([0, 1, 1, 2, 2, -1], np.int32))):
+        with pytest.raises(FvError) as ei:
+            fv.Mesh.from_elements(2, nodes, kinds, eptr, en, bptr, bn, bm)
+        assert "FV_ERR_INVALID" in str(ei.value)
