@@ -62,19 +62,40 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def make_problem(fv, wl, seed):
+def make_problem(fv, wl, seed, on_device=False):
     if wl["kind"] == "3d":
-        m = fv.Mesh.cube(wl["n"], wl["jitter"], seed)
+        m = fv.Mesh.cube(wl["n"], wl["jitter"], seed, on_device=on_device)
         kappa0 = float(np.linalg.norm(wl["velocity"])) * (1.0 / wl["n"]) / 3.0
         kf, fl, sc = m.fields(seed, kappa0, wl["sigma"], velocity=wl["velocity"], source_uniform=True)
         coef = (-1.0, 1.0, -1.0)
     else:
-        m = fv.Mesh.square(wl["n"], wl["jitter"], seed)
+        m = fv.Mesh.square(wl["n"], wl["jitter"], seed, on_device=on_device)
         kf, _, sc = m.fields(seed, 1.0, wl["sigma"], source_const=1.0)
         fl = None
         coef = (-1.0, 0.0, -1.0)
     nb = m.n_boundary_faces
     return dict(mesh=m, kappa=kf, flux=fl, source=sc, bndi=np.zeros(nb), bnde=np.zeros(nb), coef=coef)
+
+
+def device_mesh_build_s(fv, wl, seed):
+    """Wall time of fv_mesh_build_cube / _square: the element list generated on
+    the host, then faces, geometry and gradient coefficients on the GPU, no
+    read back."""
+    import ctypes as C
+
+    import torch
+
+    from fvb200._lib import check, lib
+    from fvb200.streams import stream_handle
+    h = C.c_void_p()
+    fn = lib().fv_mesh_build_cube if wl["kind"] == "3d" else lib().fv_mesh_build_square
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    check(fn(wl["n"], wl["jitter"], seed, stream_handle(None), C.byref(h), None), "fv_mesh_build")
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    lib().fv_mesh_destroy(h)
+    return t
 
 
 def equation(fv, prob, tensors):
@@ -176,9 +197,10 @@ def gpu_arm(args, rank, world, local_rank):
     from fvb200._lib import lib
     wl = WORKLOADS[args.workload]
     t0 = time.time()
-    prob = make_problem(fv, wl, seed=1000 + rank)
+    prob = make_problem(fv, wl, seed=1000 + rank, on_device=True)
     mesh = prob["mesh"]
     t_mesh = time.time() - t0
+    t_mesh_dev = device_mesh_build_s(fv, wl, 1000 + rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
     T = {k: torch.as_tensor(prob[k], device=dev) for k in ("kappa", "source", "bndi", "bnde")}
@@ -361,6 +383,7 @@ def gpu_arm(args, rank, world, local_rank):
                   "launch_ms": round(kern[k][1] * 1e3, 4), "algorithmic_bytes": int(kern[k][0])} for k in kern}
     res = dict(
         elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
+        t_mesh_dev=t_mesh_dev,
         e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
         e2e_lat_ms=e2e_lat_ms, e2e_clocks=e2e_clocks, phase_ms=phase_ms,
         kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
@@ -810,6 +833,8 @@ def main():
         "gpu_launches": int(res["launches"]),
         "clocks": res["clocks"],
         "mesh_build_s": round(res["t_mesh"], 2),
+        "mesh_build": {"where": "device (fv_mesh_build_*)", "with_read_back_and_fields_s": round(res["t_mesh"], 2),
+                       "elements_then_device_build_s": round(res["t_mesh_dev"], 3)},
     }
     if res.get("mixed_info"):
         line["dtype"] = "f32-inner/f64-refinement"

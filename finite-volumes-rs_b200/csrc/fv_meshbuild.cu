@@ -231,26 +231,11 @@ __global__ void k_faces(int64_t F, const int32_t *__restrict__ gorder, const int
     face_len[f] = c_flen[kind_index(kind[rec_elem[r]])];
 }
 
-// calc_face_data (compute.rs:267-321) for face f, its nodes in the discoverer's local order.
+// calc_face_data (compute.rs:267-321) of face f from its node ids (any count).
 template <int DIM>
-__global__ void k_face_geom(int64_t F, const int32_t *__restrict__ face_src, const int32_t *__restrict__ rec_elem,
-                            const int32_t *__restrict__ efp, const int32_t *__restrict__ kind,
-                            const int32_t *__restrict__ eptr, const int32_t *__restrict__ en,
-                            const double *__restrict__ nodes, const int32_t *__restrict__ fnp,
-                            int32_t *__restrict__ face_nodes, double *__restrict__ area,
-                            double4 *__restrict__ normal4, double4 *__restrict__ center4) {
-    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= F) return;
-    const int32_t r = face_src[f];
-    const int32_t e = rec_elem[r];
-    const int ki = kind_index(kind[e]);
-    const int l = r - efp[e];
-    const int len = c_flen[ki];
-    int32_t fn[4];
-    for (int q = 0; q < len; ++q) {
-        fn[q] = en[eptr[e] + c_slot[ki][l][q]];
-        face_nodes[fnp[f] + q] = fn[q];
-    }
+__device__ __forceinline__ void face_geom(int64_t f, const int32_t *fn, int len, const double *__restrict__ nodes,
+                                          double *__restrict__ area, double4 *__restrict__ normal4,
+                                          double4 *__restrict__ center4) {
     double c[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < len; ++i)
 #pragma unroll
@@ -309,6 +294,39 @@ __global__ void k_face_geom(int64_t F, const int32_t *__restrict__ face_src, con
     area[f] = a;
     normal4[f] = make_double4(nrm[0], nrm[1], nrm[2], 0.0);
     center4[f] = make_double4(ctr[0], ctr[1], ctr[2], 0.0);
+}
+
+// Face f of the element build, its nodes in the discoverer's local order.
+template <int DIM>
+__global__ void k_face_geom(int64_t F, const int32_t *__restrict__ face_src, const int32_t *__restrict__ rec_elem,
+                            const int32_t *__restrict__ efp, const int32_t *__restrict__ kind,
+                            const int32_t *__restrict__ eptr, const int32_t *__restrict__ en,
+                            const double *__restrict__ nodes, const int32_t *__restrict__ fnp,
+                            int32_t *__restrict__ face_nodes, double *__restrict__ area,
+                            double4 *__restrict__ normal4, double4 *__restrict__ center4) {
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    const int32_t r = face_src[f];
+    const int32_t e = rec_elem[r];
+    const int ki = kind_index(kind[e]);
+    const int l = r - efp[e];
+    const int len = c_flen[ki];
+    int32_t fn[4];
+    for (int q = 0; q < len; ++q) {
+        fn[q] = en[eptr[e] + c_slot[ki][l][q]];
+        face_nodes[fnp[f] + q] = fn[q];
+    }
+    face_geom<DIM>(f, fn, len, nodes, area, normal4, center4);
+}
+
+// Faces given as node lists (fv_mesh_build_faces).
+template <int DIM>
+__global__ void k_face_geom_list(int64_t F, const int32_t *__restrict__ fnp, const int32_t *__restrict__ fnodes,
+                                 const double *__restrict__ nodes, double *__restrict__ area,
+                                 double4 *__restrict__ normal4, double4 *__restrict__ center4) {
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    face_geom<DIM>(f, fnodes + fnp[f], fnp[f + 1] - fnp[f], nodes, area, normal4, center4);
 }
 
 __global__ void k_cell_faces(int64_t M, int64_t L, const int32_t *__restrict__ perm, const int32_t *__restrict__ gid1,
@@ -444,6 +462,56 @@ __global__ void k_cf_fill(int64_t N, const int32_t *__restrict__ cptr, const int
             cf_pad[c * padf + k] = k < n ? make_int2(face[k], other[k]) : make_int2(0, -2);
 }
 
+// add_cell (mod.rs:489-529) for explicit cell lists: with k the position of a
+// (cell, face) entry in cell_faces (k grows with the cell), the face's owner
+// is the cell of its smallest k and its neighbour the cell of the second
+// smallest, unless the face is tagged.
+__global__ void k_first_listing(int64_t N, const int32_t *__restrict__ cptr, const int32_t *__restrict__ cfaces,
+                                int32_t *__restrict__ rec_cell, int32_t *__restrict__ first) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    for (int32_t k = cptr[c]; k < cptr[c + 1]; ++k) {
+        rec_cell[k] = (int32_t)c;
+        atomicMin(&first[cfaces[k]], k);
+    }
+}
+
+__global__ void k_second_listing(int64_t L, const int32_t *__restrict__ cfaces, const int32_t *__restrict__ first,
+                                 int32_t *__restrict__ second) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= L) return;
+    const int32_t f = cfaces[k];
+    if (first[f] != (int32_t)k) atomicMin(&second[f], (int32_t)k);
+}
+
+__global__ void k_listed_cells(int64_t F, const int32_t *__restrict__ first, const int32_t *__restrict__ second,
+                               const int32_t *__restrict__ rec_cell, const int32_t *__restrict__ patch,
+                               int2 *__restrict__ face_cells, int *flags) {
+    const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int bad = 0;
+    if (f < F) {
+        const int32_t k1 = first[f], k2 = second[f];
+        if (k1 == INT32_MAX) {
+            bad = kBadOpenFace;
+            face_cells[f] = make_int2(0, -1);
+        } else {
+            const int32_t owner = rec_cell[k1];
+            int32_t nb = -1;
+            if (k2 != INT32_MAX && patch[f] < 0) nb = rec_cell[k2];
+            if (nb == owner) bad |= kBadSelf;
+            if (patch[f] < 0 && nb < 0) bad |= kBadOpenFace;
+            face_cells[f] = make_int2(owner, nb);
+        }
+    }
+    const unsigned bm = __ballot_sync(0xffffffffu, bad != 0);
+    if (bm && bad) atomicOr(flags, bad);
+}
+
+__global__ void k_fill_i32(int64_t n, int32_t v, int32_t *__restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v;
+}
+
 int bitlen(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
 
 inline unsigned blocks(int64_t n) { return (unsigned)((n + kB - 1) / kB); }
@@ -473,11 +541,11 @@ fv_status fail(cudaError_t e, const char *what) {
 }
 
 fv_status flag_status(int flags) {
-    if (flags & kBadElement) fv_internal_set_error_text("fv_mesh_build_elements: invalid element (kind, node count or dimension)");
-    else if (flags & kBadNode) fv_internal_set_error_text("fv_mesh_build_elements: element node id out of range");
-    else if (flags & kBadOpenFace) fv_internal_set_error_text("fv_mesh_build_elements: unmarked face with one cell (missing boundary marker)");
-    else if (flags & kBadSelf) fv_internal_set_error_text("fv_mesh_build_elements: an element lists one face twice");
-    else if (flags & kBadForeign) fv_internal_set_error_text("fv_mesh_build_elements: a marked face is shared by two elements");
+    if (flags & kBadElement) fv_internal_set_error_text("fv_mesh_build: invalid element (kind, node count or dimension)");
+    else if (flags & kBadNode) fv_internal_set_error_text("fv_mesh_build: element node id out of range");
+    else if (flags & kBadOpenFace) fv_internal_set_error_text("fv_mesh_build: unmarked face with one cell (missing boundary marker)");
+    else if (flags & kBadSelf) fv_internal_set_error_text("fv_mesh_build: an element lists one face twice");
+    else if (flags & kBadForeign) fv_internal_set_error_text("fv_mesh_build: a marked face is shared by two elements");
     else return FV_OK;
     return FV_ERR_INVALID;
 }
@@ -594,6 +662,87 @@ fv_status read_back(const fv_mesh *m, int dim, int64_t n_nodes, const double *no
         h->cell_volume[c] = cell[c].w;
     }
     *host_out = h;
+    return FV_OK;
+}
+
+
+// Everything after the faces exist (cells listed, face_cells, unoriented face
+// geometry): cell geometry, orientation, the cell -> face lists of the
+// assembly kernels, gradient coefficients and the optional host copy.
+// m->gcf_ptr / m->gcf_face hold the cells' faces in mesh order (L entries).
+fv_status finish(Scratch &sc, fv_mesh *m, int64_t L, int *d_flags, int64_t n_nodes, const double *nodes,
+                 const int32_t *fnp, const int32_t *fnodes, const int32_t *face_patch, fv_host_mesh **host_out) {
+    cudaStream_t st = sc.st;
+    const int dim = m->dim;
+    const int64_t N = m->n_cells, F = m->n_faces, n_int = F - m->n_bfaces;
+    cudaError_t e = cudaSuccess;
+    fv_note_launch();
+    if (dim == 2)
+        k_cell_geom<2><<<blocks(N), kB, 0, st>>>(N, m->gcf_ptr, m->gcf_face, m->face_area, m->face_normal,
+                                                 m->face_center, m->cell);
+    else
+        k_cell_geom<3><<<blocks(N), kB, 0, st>>>(N, m->gcf_ptr, m->gcf_face, m->face_area, m->face_normal,
+                                                 m->face_center, m->cell);
+    fv_note_launch();
+    if (dim == 2)
+        k_orient<2><<<blocks(F), kB, 0, st>>>(F, m->face_cells, m->cell, m->face_center, m->face_normal);
+    else
+        k_orient<3><<<blocks(F), kB, 0, st>>>(F, m->face_cells, m->cell, m->face_center, m->face_normal);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && F > n_int)
+        e = cudaMemcpyAsync(m->bface_center, m->face_center + n_int, sizeof(double4) * (F - n_int),
+                            cudaMemcpyDeviceToDevice, st);
+
+    // cell -> faces lists of the assembly kernels
+    int32_t *cnt = sc.get<int32_t>((size_t)N + 1);
+    int *d_maxf = d_flags + 1;
+    if (e == cudaSuccess) e = sc.err;
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_ptr, sizeof(int32_t) * (N + 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt + N, 0, sizeof(int32_t), st);
+    if (e == cudaSuccess) {
+        fv_note_launch();
+        k_cf_count<<<blocks(N), kB, 0, st>>>(N, m->gcf_ptr, m->gcf_face, m->face_cells, cnt, d_maxf, d_flags);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = scan(sc, cnt, m->cf_ptr, N + 1, false);
+    int32_t ncf = 0;
+    int h_flags[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ncf, m->cf_ptr + N, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(e, "fv_mesh_build (geometry)");
+    if (flag_status(h_flags[0]) != FV_OK) return FV_ERR_INVALID;
+    const int maxf = h_flags[1];
+    if (maxf > 16) {
+        fv_internal_set_error_text("fv_mesh_build: a cell with more than 16 faces");
+        return FV_ERR_UNSUPPORTED;
+    }
+    m->maxf = maxf;
+    m->padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
+    e = cudaMalloc(&m->cf_face, sizeof(int32_t) * (ncf ? ncf : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_other, sizeof(int32_t) * (ncf ? ncf : 1));
+    if (e == cudaSuccess && m->padf) e = cudaMalloc(&m->cf_pad, sizeof(int2) * N * m->padf);
+    if (e == cudaSuccess) {
+        fv_note_launch();
+        k_cf_fill<<<blocks(N), kB, 0, st>>>(N, m->gcf_ptr, m->gcf_face, m->face_cells, m->cf_ptr, m->cf_face,
+                                            m->cf_other, m->padf, m->cf_pad);
+        e = cudaGetLastError();
+    }
+
+    // gradient coefficients (compute.rs:155-203) over the mesh-order cell faces
+    int *d_gbad = d_flags + 2;
+    if (e == cudaSuccess) e = cudaMalloc(&m->gcoef, sizeof(double4) * (L ? L : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->gdiag, sizeof(double4) * N);
+    if (e == cudaSuccess) e = fv_mesh_launch_grad_coeffs(m, d_gbad, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(e, "fv_mesh_build (cell faces)");
+    if (h_flags[2]) {  // Mesh::compute returns Error::SingularMatrix
+        fv_internal_set_error_text("fv_mesh_build: singular gradient matrix of a cell");
+        return FV_ERR_INVALID;
+    }
+    if (host_out)
+        return read_back(m, dim, n_nodes, nodes, fnp, fnodes, face_patch, m->gcf_ptr, m->gcf_face, st, host_out);
     return FV_OK;
 }
 
@@ -772,72 +921,115 @@ extern "C" fv_status fv_mesh_build_elements(int32_t dim, int64_t n_nodes, const 
                                                      fnodes, m->face_area, m->face_normal, m->face_center);
         fv_note_launch();
         k_cell_faces<<<blocks(M), kB, 0, st>>>(M, L, perm, gid1, fid, m->gcf_face);
-        fv_note_launch();
-        if (dim == 2)
-            k_cell_geom<2><<<blocks(n_elems), kB, 0, st>>>(n_elems, efp, m->gcf_face, m->face_area, m->face_normal,
-                                                           m->face_center, m->cell);
-        else
-            k_cell_geom<3><<<blocks(n_elems), kB, 0, st>>>(n_elems, efp, m->gcf_face, m->face_area, m->face_normal,
-                                                           m->face_center, m->cell);
-        fv_note_launch();
-        if (dim == 2)
-            k_orient<2><<<blocks(F), kB, 0, st>>>(F, m->face_cells, m->cell, m->face_center, m->face_normal);
-        else
-            k_orient<3><<<blocks(F), kB, 0, st>>>(F, m->face_cells, m->cell, m->face_center, m->face_normal);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess && F > n_int)
-        e = cudaMemcpyAsync(m->bface_center, m->face_center + n_int, sizeof(double4) * (F - n_int),
-                            cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return give_up(fail(e, "fv_mesh_build_elements (faces)"));
+    const fv_status fs = finish(sc, m, L, d_flags, n_nodes, nodes, fnp, fnodes, face_patch, host_out);
+    if (fs != FV_OK) return give_up(fs);
+    *out = m;
+    return FV_OK;
+}
 
-    // cell -> faces lists of the assembly kernels
-    int32_t *cnt = sc.get<int32_t>((size_t)n_elems + 1);
-    int *d_maxf = d_flags + 1;
+// Mesh::compute on the device for explicit faces and cells (the layout of the
+// crate's own mesh files): owner / neighbour as add_cell assigns them, then
+// the same geometry, orientation, cell-face lists and gradient coefficients.
+extern "C" fv_status fv_mesh_build_faces(int32_t dim, int64_t n_nodes, const double *nodes, int64_t n_faces,
+                                         const int32_t *face_node_ptr, const int32_t *face_nodes,
+                                         const int32_t *face_patch, int64_t n_cells, const int32_t *cell_face_ptr,
+                                         const int32_t *cell_faces, void *stream, fv_mesh **out,
+                                         fv_host_mesh **host_out) {
+    if (!out || (dim != 2 && dim != 3) || n_nodes <= 0 || n_faces <= 0 || n_cells <= 0 || !nodes ||
+        !face_node_ptr || !face_nodes || !face_patch || !cell_face_ptr || !cell_faces || n_nodes >= 0x7fffffffLL ||
+        n_faces >= 0x7fffffffLL || n_cells >= 0x7fffffffLL || face_node_ptr[0] != 0 || cell_face_ptr[0] != 0)
+        return FV_ERR_INVALID;
+    *out = nullptr;
+    if (host_out) *host_out = nullptr;
+    // index ranges are checked here: the kernels below index with them
+    int64_t n_tagged = 0;
+    for (int64_t f = 0; f < n_faces; ++f) {
+        const int len = face_node_ptr[f + 1] - face_node_ptr[f];
+        if (len < 2 || len > 64 || (dim == 2 && len != 2)) return FV_ERR_INVALID;
+        for (int q = 0; q < len; ++q) {
+            const int32_t id = face_nodes[face_node_ptr[f] + q];
+            if (id < 0 || id >= n_nodes) return FV_ERR_INVALID;
+        }
+        if (face_patch[f] >= 0) {
+            ++n_tagged;
+        } else if (n_tagged) {
+            fv_internal_set_error_text("fv_mesh_build_faces: tagged faces must be the tail of the face list");
+            return FV_ERR_UNSUPPORTED;
+        }
+    }
+    for (int64_t c = 0; c < n_cells; ++c) {
+        const int len = cell_face_ptr[c + 1] - cell_face_ptr[c];
+        if (len < 2 || len > 64) return FV_ERR_INVALID;
+        for (int q = 0; q < len; ++q) {
+            const int32_t f = cell_faces[cell_face_ptr[c] + q];
+            if (f < 0 || f >= n_faces) return FV_ERR_INVALID;
+        }
+    }
+    const int64_t F = n_faces, N = n_cells, fnn = face_node_ptr[F], L = cell_face_ptr[N];
+    cudaStream_t st = fv_stream(stream);
+    Scratch sc(st);
+    double *d_nodes = nullptr;
+    int32_t *fnp = nullptr, *fnodes = nullptr, *patch = nullptr;
+    cudaError_t e = to_device(sc, d_nodes, nodes, (size_t)(n_nodes * dim));
+    if (e == cudaSuccess) e = to_device(sc, fnp, face_node_ptr, (size_t)F + 1);
+    if (e == cudaSuccess) e = to_device(sc, fnodes, face_nodes, (size_t)fnn);
+    if (e == cudaSuccess) e = to_device(sc, patch, face_patch, (size_t)F);
+    int32_t *first = sc.get<int32_t>((size_t)F), *second = sc.get<int32_t>((size_t)F);
+    int32_t *rec_cell = sc.get<int32_t>((size_t)L);
+    int *d_flags = sc.get<int>(4);
     if (e == cudaSuccess) e = sc.err;
-    if (e == cudaSuccess) e = cudaMalloc(&m->cf_ptr, sizeof(int32_t) * (n_elems + 1));
-    if (e == cudaSuccess) e = cudaMemsetAsync(cnt + n_elems, 0, sizeof(int32_t), st);
+    fv_mesh *m = new fv_mesh();
+    auto give_up = [&](fv_status s) {
+        fv_mesh_destroy(m);
+        return s;
+    };
+    m->dim = dim;
+    m->n_cells = N;
+    m->n_faces = F;
+    m->n_bfaces = n_tagged;
+    if (e == cudaSuccess) e = cudaMalloc(&m->gcf_ptr, sizeof(int32_t) * (N + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->gcf_face, sizeof(int32_t) * (L ? L : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_cells, sizeof(int2) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_area, sizeof(double) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_normal, sizeof(double4) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_center, sizeof(double4) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->cell, sizeof(double4) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&m->bface_center, sizeof(double4) * (n_tagged ? n_tagged : 1));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->gcf_ptr, cell_face_ptr, sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && L)
+        e = cudaMemcpyAsync(m->gcf_face, cell_faces, sizeof(int32_t) * L, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st);
     if (e == cudaSuccess) {
         fv_note_launch();
-        k_cf_count<<<blocks(n_elems), kB, 0, st>>>(n_elems, efp, m->gcf_face, m->face_cells, cnt, d_maxf, d_flags);
+        k_fill_i32<<<blocks(F), kB, 0, st>>>(F, INT32_MAX, first);
+        fv_note_launch();
+        k_fill_i32<<<blocks(F), kB, 0, st>>>(F, INT32_MAX, second);
+        fv_note_launch();
+        k_first_listing<<<blocks(N), kB, 0, st>>>(N, m->gcf_ptr, m->gcf_face, rec_cell, first);
+        fv_note_launch();
+        k_second_listing<<<blocks(L), kB, 0, st>>>(L, m->gcf_face, first, second);
+        fv_note_launch();
+        k_listed_cells<<<blocks(F), kB, 0, st>>>(F, first, second, rec_cell, patch, m->face_cells, d_flags);
+        fv_note_launch();
+        if (dim == 2)
+            k_face_geom_list<2><<<blocks(F), kB, 0, st>>>(F, fnp, fnodes, d_nodes, m->face_area, m->face_normal,
+                                                          m->face_center);
+        else
+            k_face_geom_list<3><<<blocks(F), kB, 0, st>>>(F, fnp, fnodes, d_nodes, m->face_area, m->face_normal,
+                                                          m->face_center);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = scan(sc, cnt, m->cf_ptr, n_elems + 1, false);
-    int32_t ncf = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&ncf, m->cf_ptr + n_elems, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    int h_flags[4] = {0, 0, 0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return give_up(fail(e, "fv_mesh_build_elements (geometry)"));
+    if (e != cudaSuccess) return give_up(fail(e, "fv_mesh_build_faces"));
     if (flag_status(h_flags[0]) != FV_OK) return give_up(FV_ERR_INVALID);
-    const int maxf = h_flags[1];
-    if (maxf > 16) return give_up(FV_ERR_UNSUPPORTED);
-    m->maxf = maxf;
-    m->padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
-    e = cudaMalloc(&m->cf_face, sizeof(int32_t) * (ncf ? ncf : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&m->cf_other, sizeof(int32_t) * (ncf ? ncf : 1));
-    if (e == cudaSuccess && m->padf) e = cudaMalloc(&m->cf_pad, sizeof(int2) * n_elems * m->padf);
-    if (e == cudaSuccess) {
-        fv_note_launch();
-        k_cf_fill<<<blocks(n_elems), kB, 0, st>>>(n_elems, efp, m->gcf_face, m->face_cells, m->cf_ptr, m->cf_face,
-                                                  m->cf_other, m->padf, m->cf_pad);
-        e = cudaGetLastError();
-    }
-
-    // gradient coefficients (compute.rs:155-203) over the mesh-order cell faces
-    int *d_gbad = d_flags + 2;
-    if (e == cudaSuccess) e = cudaMalloc(&m->gcoef, sizeof(double4) * (L ? L : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&m->gdiag, sizeof(double4) * n_elems);
-    if (e == cudaSuccess) e = fv_mesh_launch_grad_coeffs(m, d_gbad, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return give_up(fail(e, "fv_mesh_build_elements (cell faces)"));
-    if (h_flags[2]) {  // Mesh::compute returns Error::SingularMatrix
-        fv_internal_set_error_text("fv_mesh_build_elements: singular gradient matrix of a cell");
-        return give_up(FV_ERR_INVALID);
-    }
-    if (host_out) {
-        const fv_status s = read_back(m, dim, n_nodes, nodes, fnp, fnodes, face_patch, efp, m->gcf_face, st, host_out);
-        if (s != FV_OK) return give_up(s);
-    }
+    const fv_status fs = finish(sc, m, L, d_flags, n_nodes, nodes, fnp, fnodes, patch, host_out);
+    if (fs != FV_OK) return give_up(fs);
     *out = m;
     return FV_OK;
 }

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cerrno>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -27,6 +28,8 @@
 #include <cstring>
 #include <new>
 #include <vector>
+
+void fv_internal_set_error_text(const char *what);  // fv_assembly.cu
 
 #define FV_RETURN_IF(expr)            \
     do {                              \
@@ -273,11 +276,30 @@ static void cell_geometry(int dim, const int32_t *cf, int len, const double *far
     for (int d = 0; d < dim; ++d) center[d] = ctr[d] / vol;
 }
 
-struct Builder {
-    int dim = 0;
-    int64_t n_nodes = 0;
-    const double *nodes = nullptr;
-};
+// Mesh::compute (compute.rs:12-131) on a host mesh whose topology is set:
+// face data, then cell data, then orientation.
+void compute_geometry(fv_host_mesh *m) {
+    const int dim = m->dim;
+    const int64_t F = m->n_faces, N = m->n_cells;
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f)
+        face_geometry(dim, m->nodes, m->face_nodes + m->face_node_ptr[f], m->face_node_ptr[f + 1] - m->face_node_ptr[f],
+                      m->face_area + f, m->face_normal + f * dim, m->face_center + f * dim);
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < N; ++c)
+        cell_geometry(dim, m->cell_faces + m->cell_face_ptr[c], m->cell_face_ptr[c + 1] - m->cell_face_ptr[c],
+                      m->face_area, m->face_normal, m->face_center, m->cell_center + c * dim, m->cell_volume + c);
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f) {
+        const double *ip = m->cell_center + (int64_t)m->face_owner[f] * dim;
+        double *nv = m->face_normal + f * dim;
+        const double *fc = m->face_center + f * dim;
+        double s = 0.0;
+        for (int d = 0; d < dim; ++d) s += nv[d] * (fc[d] - ip[d]);
+        if (s < 0.0)
+            for (int d = 0; d < dim; ++d) nv[d] *= -1.0;
+    }
+}
 
 }  // namespace
 
@@ -460,27 +482,7 @@ extern "C" fv_status fv_host_mesh_from_elements(int32_t dim, int64_t n_nodes, co
                 return FV_ERR_INVALID;
             }
 
-        // Mesh::compute: face data, then cell data, then orientation.
-#pragma omp parallel for schedule(static)
-        for (int64_t f = 0; f < F; ++f)
-            face_geometry(dim, m->nodes, m->face_nodes + m->face_node_ptr[f],
-                          m->face_node_ptr[f + 1] - m->face_node_ptr[f], m->face_area + f,
-                          m->face_normal + f * dim, m->face_center + f * dim);
-#pragma omp parallel for schedule(static)
-        for (int64_t c = 0; c < n_elems; ++c)
-            cell_geometry(dim, m->cell_faces + m->cell_face_ptr[c], m->cell_face_ptr[c + 1] - m->cell_face_ptr[c],
-                          m->face_area, m->face_normal, m->face_center, m->cell_center + c * dim,
-                          m->cell_volume + c);
-#pragma omp parallel for schedule(static)
-        for (int64_t f = 0; f < F; ++f) {
-            const double *ip = m->cell_center + (int64_t)m->face_owner[f] * dim;
-            double *nv = m->face_normal + f * dim;
-            const double *fc = m->face_center + f * dim;
-            double s = 0.0;
-            for (int d = 0; d < dim; ++d) s += nv[d] * (fc[d] - ip[d]);
-            if (s < 0.0)
-                for (int d = 0; d < dim; ++d) nv[d] *= -1.0;
-        }
+        compute_geometry(m);
         *out = m;
         return FV_OK;
     } catch (const std::bad_alloc &) {
@@ -629,6 +631,12 @@ fv_status cube_elements(int32_t n, double jitter, uint64_t seed, Elements &el) {
         int32_t fn[24];
         int fs[8];
         for (int64_t q = 0; q < ne; ++q) {
+            const int64_t hex = q / 6;  // only hexes touching a side hold boundary faces
+            const int64_t hi = hex % n, hj = (hex / n) % n, hk = hex / ((int64_t)n * n);
+            if (hi > 0 && hi < n - 1 && hj > 0 && hj < n - 1 && hk > 0 && hk < n - 1) {
+                q += 5;
+                continue;
+            }
             vtk_faces(10, en.data() + q * 4, fn, fs);
             for (int l = 0; l < 4; ++l) {
                 const int32_t *f = fn + fs[l];
@@ -841,4 +849,441 @@ extern "C" fv_status fv_mesh_build_su2(const char *path, int32_t dim, void *stre
     Elements el;
     FV_RETURN_IF(su2_elements(path, dim, el));
     return to_device(el, stream, out, host_out);
+}
+
+// ---------------------------------------------------------------- explicit faces
+// add_face / add_cell (mod.rs:451-529) for explicit face and cell lists: the
+// first cell listing a face owns it, the second becomes its neighbour unless
+// the face carries a boundary tag; then Mesh::compute.  The tagged faces must
+// be the tail of the face list (the layout every mesh read from SU2 has).
+extern "C" fv_status fv_host_mesh_from_faces(int32_t dim, int64_t n_nodes, const double *nodes, int64_t n_faces,
+                                             const int32_t *face_node_ptr, const int32_t *face_nodes,
+                                             const int32_t *face_patch, int64_t n_cells,
+                                             const int32_t *cell_face_ptr, const int32_t *cell_faces,
+                                             fv_host_mesh **out) {
+    if (!out || (dim != 2 && dim != 3) || n_nodes <= 0 || n_faces <= 0 || n_cells <= 0 || !nodes ||
+        !face_node_ptr || !face_nodes || !face_patch || !cell_face_ptr || !cell_faces || n_nodes >= 0x7fffffffLL ||
+        n_faces >= 0x7fffffffLL || n_cells >= 0x7fffffffLL || face_node_ptr[0] != 0 || cell_face_ptr[0] != 0)
+        return FV_ERR_INVALID;
+    *out = nullptr;
+    int64_t n_tagged = 0;
+    for (int64_t f = 0; f < n_faces; ++f) {
+        const int len = face_node_ptr[f + 1] - face_node_ptr[f];
+        if (len < 2 || len > 64 || (dim == 2 && len != 2)) return FV_ERR_INVALID;
+        for (int q = 0; q < len; ++q) {
+            const int32_t id = face_nodes[face_node_ptr[f] + q];
+            if (id < 0 || id >= n_nodes) return FV_ERR_INVALID;
+        }
+        if (face_patch[f] >= 0) {
+            ++n_tagged;
+        } else if (n_tagged) {
+            fv_internal_set_error_text("fv_host_mesh_from_faces: tagged faces must be the tail of the face list");
+            return FV_ERR_UNSUPPORTED;
+        }
+    }
+    for (int64_t c = 0; c < n_cells; ++c) {
+        const int len = cell_face_ptr[c + 1] - cell_face_ptr[c];
+        if (len < 2 || len > 64) return FV_ERR_INVALID;
+        for (int q = 0; q < len; ++q) {
+            const int32_t f = cell_faces[cell_face_ptr[c] + q];
+            if (f < 0 || f >= n_faces) return FV_ERR_INVALID;
+        }
+    }
+    try {
+        fv_host_mesh *m = (fv_host_mesh *)std::calloc(1, sizeof(fv_host_mesh));
+        if (!m) return FV_ERR_ALLOC;
+        const int64_t F = n_faces, N = n_cells, fnn = face_node_ptr[F], ncf = cell_face_ptr[N];
+        m->dim = dim;
+        m->n_nodes = n_nodes;
+        m->n_faces = F;
+        m->n_cells = N;
+        m->n_boundary_faces = n_tagged;
+        m->nodes = (double *)std::malloc(sizeof(double) * n_nodes * dim);
+        m->face_node_ptr = (int32_t *)std::malloc(sizeof(int32_t) * (F + 1));
+        m->face_nodes = (int32_t *)std::malloc(sizeof(int32_t) * fnn);
+        m->face_patch = (int32_t *)std::malloc(sizeof(int32_t) * F);
+        m->cell_face_ptr = (int32_t *)std::malloc(sizeof(int32_t) * (N + 1));
+        m->cell_faces = (int32_t *)std::malloc(sizeof(int32_t) * ncf);
+        m->face_owner = (int32_t *)std::malloc(sizeof(int32_t) * F);
+        m->face_neighbor = (int32_t *)std::malloc(sizeof(int32_t) * F);
+        m->face_area = (double *)std::malloc(sizeof(double) * F);
+        m->face_normal = (double *)std::malloc(sizeof(double) * F * dim);
+        m->face_center = (double *)std::malloc(sizeof(double) * F * dim);
+        m->cell_center = (double *)std::malloc(sizeof(double) * N * dim);
+        m->cell_volume = (double *)std::malloc(sizeof(double) * N);
+        if (!m->nodes || !m->face_node_ptr || !m->face_nodes || !m->face_patch || !m->cell_face_ptr ||
+            !m->cell_faces || !m->face_owner || !m->face_neighbor || !m->face_area || !m->face_normal ||
+            !m->face_center || !m->cell_center || !m->cell_volume) {
+            fv_host_mesh_free(m);
+            return FV_ERR_ALLOC;
+        }
+        std::memcpy(m->nodes, nodes, sizeof(double) * n_nodes * dim);
+        std::memcpy(m->face_node_ptr, face_node_ptr, sizeof(int32_t) * (F + 1));
+        std::memcpy(m->face_nodes, face_nodes, sizeof(int32_t) * fnn);
+        std::memcpy(m->face_patch, face_patch, sizeof(int32_t) * F);
+        std::memcpy(m->cell_face_ptr, cell_face_ptr, sizeof(int32_t) * (N + 1));
+        std::memcpy(m->cell_faces, cell_faces, sizeof(int32_t) * ncf);
+        for (int64_t f = 0; f < F; ++f) m->face_owner[f] = m->face_neighbor[f] = -1;
+        for (int64_t c = 0; c < N; ++c)
+            for (int32_t k = cell_face_ptr[c]; k < cell_face_ptr[c + 1]; ++k) {
+                const int32_t f = cell_faces[k];
+                if (m->face_owner[f] < 0)
+                    m->face_owner[f] = (int32_t)c;
+                else if (m->face_patch[f] < 0 && m->face_neighbor[f] < 0)
+                    m->face_neighbor[f] = (int32_t)c;
+            }
+        for (int64_t f = 0; f < F; ++f)
+            if (m->face_owner[f] < 0 || (m->face_patch[f] < 0 && m->face_neighbor[f] < 0) ||
+                m->face_neighbor[f] == m->face_owner[f]) {
+                fv_internal_set_error_text(
+                    "fv_host_mesh_from_faces: a face no cell lists, an untagged face with one cell, or a cell listing "
+                    "a face twice");
+                fv_host_mesh_free(m);
+                return FV_ERR_INVALID;
+            }
+        compute_geometry(m);
+        *out = m;
+        return FV_OK;
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
+}
+
+// ---------------------------------------------------------------- .msh
+// The crate's own mesh format, Mesh::write / Mesh::read (io.rs:10-225):
+//   NDIME=<dim>
+//   NPATCH=<k>, then "<name> <id> <first face> <faces>" per patch
+//   NNODES=<n>, then the coordinates, separated by one space
+//   NFACES=<n>, then "<len> <nodes...> <tag|-> <global id> <-|owner rank>"
+//   NCELLS=<n>, then "<len> <faces...> <global id> <-|owner rank>"
+// Numbers print as Rust's Display does: integers in decimal, doubles as the
+// shortest digits that read back to the same value, never in exponent form.
+namespace {
+
+struct Topology {
+    int32_t dim = 0;
+    std::vector<double> nodes;
+    std::vector<int32_t> fptr{0}, fnodes, fpatch, cptr{0}, cfaces;
+};
+
+// Rust's `{}` for f64: shortest round-trip digits, positional notation.
+std::string rust_f64(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v < 0 ? "-inf" : "inf";
+    if (v == 0.0) return std::signbit(v) ? "-0" : "0";
+    char buf[64];
+    int p = 1;
+    for (; p <= 17; ++p) {
+        snprintf(buf, sizeof(buf), "%.*e", p - 1, v);
+        if (strtod(buf, nullptr) == v) break;
+    }
+    // buf = [-]d[.ddd]e[+-]xx
+    std::string s(buf), digits;
+    const bool neg = s[0] == '-';
+    size_t i = neg ? 1 : 0;
+    for (; i < s.size() && s[i] != 'e'; ++i)
+        if (s[i] != '.') digits += s[i];
+    const int e10 = atoi(s.c_str() + i + 1);
+    while (digits.size() > 1 && digits.back() == '0') digits.pop_back();
+    const int nd = (int)digits.size();
+    std::string out = neg ? "-" : "";
+    if (e10 < 0) {
+        out += "0.";
+        out.append((size_t)(-e10 - 1), '0');
+        out += digits;
+    } else if (e10 >= nd - 1) {
+        out += digits;
+        out.append((size_t)(e10 - (nd - 1)), '0');
+    } else {
+        out += digits.substr(0, (size_t)e10 + 1);
+        out += ".";
+        out += digits.substr((size_t)e10 + 1);
+    }
+    return out;
+}
+
+bool parse_i64(const std::string &t, long long &v) {
+    if (t.empty()) return false;
+    char *end = nullptr;
+    errno = 0;
+    v = strtoll(t.c_str(), &end, 10);
+    return errno == 0 && end && *end == '\0' && !isspace((unsigned char)t[0]);
+}
+
+std::vector<std::string> split_spaces(const std::string &l) {  // str::split(" "): empty pieces kept
+    std::vector<std::string> t;
+    size_t a = 0;
+    while (true) {
+        const size_t b = l.find(' ', a);
+        t.push_back(l.substr(a, b == std::string::npos ? std::string::npos : b - a));
+        if (b == std::string::npos) break;
+        a = b + 1;
+    }
+    return t;
+}
+
+std::string trim(const std::string &l) {
+    size_t a = 0, b = l.size();
+    while (a < b && isspace((unsigned char)l[a])) ++a;
+    while (b > a && isspace((unsigned char)l[b - 1])) --b;
+    return l.substr(a, b - a);
+}
+
+fv_status msh_parse(const char *path, int32_t dim, Topology &t) {
+    if (!path) return FV_ERR_INVALID;
+    FILE *fp = fopen(path, "r");
+    if (!fp) {
+        fv_internal_set_error_text("read_msh: cannot open the file");
+        return FV_ERR_INVALID;
+    }
+    auto bad = [&](long long line, const char *what) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "read_msh: line %lld: %s", line, what);
+        fv_internal_set_error_text(msg);
+        return FV_ERR_INVALID;
+    };
+    std::string section = "none", line;
+    long long nodes_left = 0, faces_left = 0, cells_left = 0, patches_left = 0, line_id = 0;
+    int d = dim;
+    fv_status st = FV_OK;
+    char buf[1 << 16];
+    std::string cur;
+    bool eof = false;
+    while (st == FV_OK && !eof) {
+        cur.clear();
+        while (true) {
+            if (!fgets(buf, sizeof(buf), fp)) {
+                eof = true;
+                break;
+            }
+            cur += buf;
+            if (!cur.empty() && cur.back() == '\n') break;
+        }
+        if (eof && cur.empty()) break;
+        ++line_id;
+        const std::string ls = trim(cur);
+        if (ls.empty()) continue;
+        if (ls[0] == 'N') {
+            const size_t eq = ls.find('=');
+            if (eq == std::string::npos) {
+                st = bad(line_id, "section header without '='");
+                break;
+            }
+            section = ls.substr(0, eq);
+            std::string rest = ls.substr(eq + 1);
+            const size_t eq2 = rest.find('=');
+            if (eq2 != std::string::npos) rest = rest.substr(0, eq2);
+            long long val = 0;
+            if (!parse_i64(rest, val) || val < 0) {
+                st = bad(line_id, "section size is not a number");
+                break;
+            }
+            if (section == "NDIME") {
+                if (d == 0) d = (int)val;
+                if (val != d || (d != 2 && d != 3)) {
+                    fv_internal_set_error_text("read_msh: NDIME differs from the requested dimension");
+                    st = FV_ERR_INVALID;
+                    break;
+                }
+                t.dim = d;
+            } else if (section == "NNODES") {
+                nodes_left = val;
+            } else if (section == "NFACES") {
+                faces_left = val;
+            } else if (section == "NCELLS") {
+                cells_left = val;
+            } else if (section == "NPATCH") {
+                patches_left = val;
+            }
+            continue;
+        }
+        if (section == "none") continue;
+        if (section == "NNODES") {
+            if (nodes_left == 0) continue;
+            if (t.dim == 0) {
+                st = bad(line_id, "nodes before NDIME");
+                break;
+            }
+            double x[3] = {0.0, 0.0, 0.0};
+            const auto tok = split_spaces(ls);
+            for (size_t i = 0; i < tok.size() && (int)i < t.dim; ++i) {
+                const std::string v = trim(tok[i]);
+                char *end = nullptr;
+                x[i] = strtod(v.c_str(), &end);
+                if (v.empty() || !end || *end != '\0') {
+                    st = bad(line_id, "bad coordinate");
+                    break;
+                }
+            }
+            for (int i = 0; i < t.dim; ++i) t.nodes.push_back(x[i]);
+            --nodes_left;
+        } else if (section == "NFACES" || section == "NCELLS") {
+            const bool faces = section == "NFACES";
+            if ((faces ? faces_left : cells_left) == 0) continue;
+            const auto tok = split_spaces(ls);
+            long long size = 0;
+            if (tok.empty() || !parse_i64(tok[0], size) || size < 0 || size > 64 ||
+                (long long)tok.size() < 1 + size + (faces ? 3 : 2)) {
+                st = bad(line_id, faces ? "bad face line" : "bad cell line");
+                break;
+            }
+            for (long long i = 0; i < size; ++i) {
+                long long v = 0;
+                if (!parse_i64(tok[1 + i], v) || v < 0 || v > 0x7fffffffLL) {
+                    st = bad(line_id, "bad index");
+                    break;
+                }
+                (faces ? t.fnodes : t.cfaces).push_back((int32_t)v);
+            }
+            if (st != FV_OK) break;
+            size_t k = (size_t)(1 + size);
+            if (faces) {
+                long long tag = -1;
+                if (tok[k] != "-" && (!parse_i64(tok[k], tag) || tag < 0 || tag > 65535)) {
+                    st = bad(line_id, "bad boundary tag");
+                    break;
+                }
+                t.fpatch.push_back((int32_t)tag);
+                ++k;
+            }
+            long long gid = 0;
+            if (!parse_i64(tok[k], gid) || gid < 0 || gid > 0xffffffffLL) {
+                st = bad(line_id, "bad global id");
+                break;
+            }
+            if (tok[k + 1] != "-") {  // Ownership::Remote: a ghost of a decomposed mesh
+                fv_internal_set_error_text("read_msh: remote (ghost) faces or cells are not supported");
+                st = FV_ERR_UNSUPPORTED;
+                break;
+            }
+            if (faces) {
+                t.fptr.push_back((int32_t)t.fnodes.size());
+                --faces_left;
+            } else {
+                t.cptr.push_back((int32_t)t.cfaces.size());
+                --cells_left;
+            }
+        } else if (section == "NPATCH") {
+            if (patches_left == 0) continue;
+            const auto tok = split_spaces(ls);
+            long long bid = 0, fstart = 0, len = 0;
+            if (tok.size() < 4 || !parse_i64(tok[1], bid) || !parse_i64(tok[2], fstart) || !parse_i64(tok[3], len)) {
+                st = bad(line_id, "bad patch line");
+                break;
+            }
+            --patches_left;
+        }
+    }
+    fclose(fp);
+    if (st != FV_OK) return st;
+    if (t.dim == 0 || t.nodes.empty() || t.fpatch.empty() || t.cptr.size() < 2) {
+        fv_internal_set_error_text("read_msh: missing NDIME, nodes, faces or cells");
+        return FV_ERR_INVALID;
+    }
+    return FV_OK;
+}
+
+fv_status topology_to_host(const Topology &t, fv_host_mesh **out) {
+    return fv_host_mesh_from_faces(t.dim, (int64_t)(t.nodes.size() / t.dim), t.nodes.data(), (int64_t)t.fpatch.size(),
+                                   t.fptr.data(), t.fnodes.data(), t.fpatch.data(), (int64_t)t.cptr.size() - 1,
+                                   t.cptr.data(), t.cfaces.data(), out);
+}
+
+}  // namespace
+
+extern "C" fv_status fv_host_mesh_read_msh(const char *path, int32_t dim, fv_host_mesh **out) {
+    if (!path || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    try {
+        Topology t;
+        FV_RETURN_IF(msh_parse(path, dim, t));
+        return topology_to_host(t, out);
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
+}
+
+extern "C" fv_status fv_mesh_build_msh(const char *path, int32_t dim, void *stream, fv_mesh **out,
+                                       fv_host_mesh **host_out) {
+    if (!path || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    try {
+        Topology t;
+        FV_RETURN_IF(msh_parse(path, dim, t));
+        return fv_mesh_build_faces(t.dim, (int64_t)(t.nodes.size() / t.dim), t.nodes.data(), (int64_t)t.fpatch.size(),
+                                   t.fptr.data(), t.fnodes.data(), t.fpatch.data(), (int64_t)t.cptr.size() - 1,
+                                   t.cptr.data(), t.cfaces.data(), stream, out, host_out);
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
+}
+
+extern "C" fv_status fv_host_mesh_write_msh(const fv_host_mesh *m, const char *path, const char *const *patch_names,
+                                            int32_t n_patch_names) {
+    if (!m || !path) return FV_ERR_INVALID;
+    FILE *fp = fopen(path, "w");
+    if (!fp) return FV_ERR_INVALID;
+    try {
+        const int dim = m->dim;
+        // patches: the tagged faces grouped by tag, in face order
+        std::vector<int32_t> ids;
+        std::vector<int64_t> first, count;
+        for (int64_t f = 0; f < m->n_faces; ++f) {
+            const int32_t p = m->face_patch[f];
+            if (p < 0) continue;
+            if (ids.empty() || ids.back() != p) {
+                ids.push_back(p);
+                first.push_back(f);
+                count.push_back(0);
+            }
+            ++count.back();
+        }
+        std::string out;
+        out.reserve(1 << 20);
+        auto flush = [&]() {
+            fwrite(out.data(), 1, out.size(), fp);
+            out.clear();
+        };
+        out += "NDIME=" + std::to_string(dim) + "\n";
+        out += "NPATCH=" + std::to_string(ids.size()) + "\n";
+        for (size_t i = 0; i < ids.size(); ++i) {
+            std::string name = (patch_names && ids[i] < n_patch_names && patch_names[ids[i]])
+                                   ? std::string(patch_names[ids[i]])
+                                   : "patch_" + std::to_string(ids[i]);
+            out += name + " " + std::to_string(ids[i]) + " " + std::to_string(first[i]) + " " +
+                   std::to_string(count[i]) + "\n";
+        }
+        out += "NNODES=" + std::to_string(m->n_nodes) + "\n";
+        for (int64_t n = 0; n < m->n_nodes; ++n) {
+            for (int d = 0; d < dim; ++d) {
+                if (d) out += ' ';
+                out += rust_f64(m->nodes[n * dim + d]);
+            }
+            out += '\n';
+            if (out.size() > (1 << 20)) flush();
+        }
+        out += "NFACES=" + std::to_string(m->n_faces) + "\n";
+        for (int64_t f = 0; f < m->n_faces; ++f) {
+            out += std::to_string(m->face_node_ptr[f + 1] - m->face_node_ptr[f]);
+            for (int32_t k = m->face_node_ptr[f]; k < m->face_node_ptr[f + 1]; ++k)
+                out += " " + std::to_string(m->face_nodes[k]);
+            out += m->face_patch[f] >= 0 ? " " + std::to_string(m->face_patch[f]) : std::string(" -");
+            out += " " + std::to_string(f) + " -\n";
+            if (out.size() > (1 << 20)) flush();
+        }
+        out += "NCELLS=" + std::to_string(m->n_cells) + "\n";
+        for (int64_t c = 0; c < m->n_cells; ++c) {
+            out += std::to_string(m->cell_face_ptr[c + 1] - m->cell_face_ptr[c]);
+            for (int32_t k = m->cell_face_ptr[c]; k < m->cell_face_ptr[c + 1]; ++k)
+                out += " " + std::to_string(m->cell_faces[k]);
+            out += " " + std::to_string(c) + " -\n";
+            if (out.size() > (1 << 20)) flush();
+        }
+        flush();
+        const bool ok = fclose(fp) == 0;
+        return ok ? FV_OK : FV_ERR_INVALID;
+    } catch (const std::bad_alloc &) {
+        fclose(fp);
+        return FV_ERR_ALLOC;
+    }
 }

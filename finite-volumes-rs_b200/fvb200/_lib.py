@@ -119,6 +119,11 @@ _SIGS = {
     "fv_mesh_upload": [P(MeshDesc), vp, P(vp)],
     "fv_mesh_build_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_build_su2": [C.c_char_p, C.c_int32, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_build_msh": [C.c_char_p, C.c_int32, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_build_faces": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, vp, P(vp), P(P(HostMesh_))],
+    "fv_host_mesh_from_faces": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, P(P(HostMesh_))],
+    "fv_host_mesh_read_msh": [C.c_char_p, C.c_int32, P(P(HostMesh_))],
+    "fv_host_mesh_write_msh": [P(HostMesh_), C.c_char_p, P(C.c_char_p), C.c_int32],
     "fv_mesh_build_square": [C.c_int32, C.c_double, C.c_uint64, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_build_cube": [C.c_int32, C.c_double, C.c_uint64, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_destroy": [vp],

@@ -127,6 +127,43 @@ class Mesh:
         return cls(out)
 
     @classmethod
+    def from_faces(cls, dim, nodes, face_node_ptr, face_nodes, face_patch, cell_face_ptr, cell_faces,
+                   on_device: bool = False, stream=None) -> "Mesh":
+        """Explicit faces and cells (add_face / add_cell, core/mesh/mod.rs:451-529) + Mesh::compute.
+        face_patch: boundary tag per face, -1 untagged; tagged faces last."""
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64).reshape(-1)
+        fp = np.ascontiguousarray(face_node_ptr, dtype=np.int32)
+        fn = np.ascontiguousarray(face_nodes, dtype=np.int32)
+        pa = np.ascontiguousarray(face_patch, dtype=np.int32)
+        cp = np.ascontiguousarray(cell_face_ptr, dtype=np.int32)
+        cf = np.ascontiguousarray(cell_faces, dtype=np.int32)
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        I = lambda a: P(a, C.c_int32)  # noqa: E731
+        args = (dim, len(nodes) // dim, P(nodes, C.c_double), len(pa), I(fp), I(fn), I(pa), len(cp) - 1, I(cp), I(cf))
+        if on_device:
+            return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_faces(*args, st, h, o),
+                                        "Mesh.from_faces(on_device)", stream)
+        out = C.POINTER(HostMesh_)()
+        check(lib().fv_host_mesh_from_faces(*args, C.byref(out)), "Mesh.from_faces")
+        return cls(out)
+
+    @classmethod
+    def read(cls, path, dim: int = 0, on_device: bool = False, stream=None) -> "Mesh":
+        """Mesh::read (core/mesh/io.rs:68-225): the crate's own .msh format; dim 0 = NDIME of the file."""
+        if on_device:
+            return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_msh(str(path).encode(), int(dim), st, h, o),
+                                        "Mesh.read(on_device)", stream)
+        out = C.POINTER(HostMesh_)()
+        check(lib().fv_host_mesh_read_msh(str(path).encode(), int(dim), C.byref(out)), "Mesh.read")
+        return cls(out)
+
+    def write(self, path, patch_names=None) -> None:
+        """Mesh::write (core/mesh/io.rs:10-66); patch_names[p] names boundary tag p ("patch_<p>" otherwise)."""
+        names = list(patch_names or [])
+        arr = (C.c_char_p * max(len(names), 1))(*[str(x).encode() for x in names])
+        check(lib().fv_host_mesh_write_msh(self._h, str(path).encode(), arr, len(names)), "Mesh.write")
+
+    @classmethod
     def square(cls, n: int, jitter: float = 0.0, seed: int = 0, on_device: bool = False, stream=None) -> "Mesh":
         if on_device:
             return cls._built_on_device(lambda st, h, o: lib().fv_mesh_build_square(n, jitter, seed, st, h, o),

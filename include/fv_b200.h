@@ -105,6 +105,23 @@ fv_status fv_host_mesh_generate_cube(int32_t n, double jitter, uint64_t seed, fv
 
 void fv_host_mesh_free(fv_host_mesh *m);
 
+/* add_face / add_cell + Mesh::compute on the host for explicit faces and cells
+ * (see fv_mesh_build_faces). */
+fv_status fv_host_mesh_from_faces(int32_t dim, int64_t n_nodes, const double *nodes, int64_t n_faces,
+                                  const int32_t *face_node_ptr, const int32_t *face_nodes,
+                                  const int32_t *face_patch, int64_t n_cells, const int32_t *cell_face_ptr,
+                                  const int32_t *cell_faces, fv_host_mesh **out);
+/* Mesh::read / Mesh::write (io.rs:10-225), the crate's own ".msh" format:
+ *   NDIME=<dim>, NPATCH=<k> + "<name> <id> <first face> <faces>",
+ *   NNODES=<n> + coordinates, NFACES=<n> + "<len> <nodes> <tag|-> <gid> -",
+ *   NCELLS=<n> + "<len> <faces> <gid> -".
+ * The writer prints doubles as Rust's Display does (shortest digits that read
+ * back exactly, positional) and names patch p patch_names[p] (NULL or short:
+ * "patch_<p>"). */
+fv_status fv_host_mesh_read_msh(const char *path, int32_t dim, fv_host_mesh **out);
+fv_status fv_host_mesh_write_msh(const fv_host_mesh *m, const char *path, const char *const *patch_names,
+                                 int32_t n_patch_names);
+
 /* Seeded synthetic fields on a host mesh.
  *   cell diffusivity kappa_c = kappa0 * exp(sigma * z), z ~ N(0,1)
  *   face diffusivity: linear interpolation weights of faceinterp/linear.rs:25-42
@@ -231,6 +248,21 @@ fv_status fv_mesh_build_elements(int32_t dim, int64_t n_nodes, const double *nod
                                  int64_t n_bfaces, const int32_t *bface_node_ptr,
                                  const int32_t *bface_nodes, const int32_t *bface_marker,
                                  void *stream, fv_mesh **out, fv_host_mesh **host_out);
+/* Mesh::compute on the device for explicit faces and cells (add_face /
+ * add_cell, mod.rs:451-529: the first cell listing a face owns it, the second
+ * is its neighbour unless the face is tagged).  face_patch: tag per face, -1
+ * untagged; tagged faces must be the tail of the face list.  Same outputs as
+ * fv_host_mesh_from_faces. */
+fv_status fv_mesh_build_faces(int32_t dim, int64_t n_nodes, const double *nodes, int64_t n_faces,
+                              const int32_t *face_node_ptr, const int32_t *face_nodes,
+                              const int32_t *face_patch, int64_t n_cells, const int32_t *cell_face_ptr,
+                              const int32_t *cell_faces, void *stream, fv_mesh **out,
+                              fv_host_mesh **host_out);
+/* The crate's own mesh file (Mesh::read, io.rs:68-225; ".msh"): on the device,
+ * or on the host (fv_host_mesh_read_msh).  dim 0 takes NDIME from the file.
+ * Remote (ghost) faces or cells of a decomposed mesh: FV_ERR_UNSUPPORTED. */
+fv_status fv_mesh_build_msh(const char *path, int32_t dim, void *stream, fv_mesh **out,
+                            fv_host_mesh **host_out);
 /* The same from an SU2 file (the parser of fv_host_mesh_read_su2) and from the
  * synthetic generators (fv_host_mesh_generate_square / _cube). */
 fv_status fv_mesh_build_su2(const char *path, int32_t dim, void *stream, fv_mesh **out,

@@ -109,7 +109,13 @@ def _face_data(dim, nodes, fn):
 def build(dim, nodes, elements, boundaries):
     """Mesh::read_su2 + Mesh::compute for a small element list."""
     face_nodes, fbnd, elem_faces = compute_vtk_faces(elements, boundaries)
-    F, N = len(face_nodes), len(elements)
+    return build_topology(dim, nodes, face_nodes, fbnd, elem_faces)
+
+
+def build_topology(dim, nodes, face_nodes, fbnd, elem_faces):
+    """add_face / add_cell (mod.rs:451-529) + Mesh::compute for explicit faces
+    (fbnd: tag or None per face) and cells (lists of faces)."""
+    F = len(face_nodes)
     owner, neigh = [-1] * F, [-1] * F
     for c, ef in enumerate(elem_faces):
         for f in ef:
@@ -255,3 +261,112 @@ def grad_coeffs(dim, cell_face_ptr, cell_faces, face_owner, face_neighbor, face_
             own = [own[i] - w[i] for i in range(dim)]
         gdg.append(own)
     return gco, gdg
+
+
+# ------------------------------------------------------------------ .msh
+# Mesh::write / Mesh::read (core/mesh/io.rs:10-225), the crate's own format.
+
+def rust_f64(x):
+    """Rust's Display for f64: the shortest digits that read back to x (Python's
+    repr finds the same digits), written out without an exponent."""
+    if x != x:
+        return "NaN"
+    if x == math.inf:
+        return "inf"
+    if x == -math.inf:
+        return "-inf"
+    if x == 0.0:
+        return "-0" if math.copysign(1.0, x) < 0 else "0"
+    r = repr(float(x))
+    sign = "-" if r.startswith("-") else ""
+    r = r.lstrip("-")
+    mant, exp = (r.split("e") + ["0"])[:2]
+    ip, fp = (mant.split(".") + [""])[:2]
+    digits, point = ip + fp, len(ip) + int(exp)
+    while len(digits) > 1 and digits[0] == "0":
+        digits, point = digits[1:], point - 1
+    digits = digits.rstrip("0") or "0"
+    if point <= 0:
+        body = "0." + "0" * (-point) + digits
+    elif point >= len(digits):
+        body = digits + "0" * (point - len(digits))
+    else:
+        body = digits[:point] + "." + digits[point:]
+    return sign + body
+
+
+def write_msh(dim, nodes, face_nodes, face_patch, cell_faces, names=None):
+    """Text of Mesh::write for a serial mesh (every face and cell owned, global
+    id = index); boundary faces grouped by tag in face order are the patches."""
+    patches = []
+    for f, p in enumerate(face_patch):
+        if p is None or p < 0:
+            continue
+        if not patches or patches[-1][0] != p:
+            patches.append([p, f, 0])
+        patches[-1][2] += 1
+    names = list(names or [])
+    out = [f"NDIME={dim}", f"NPATCH={len(patches)}"]
+    for p, first, cnt in patches:
+        nm = names[p] if p < len(names) else f"patch_{p}"
+        out.append(f"{nm} {p} {first} {cnt}")
+    out.append(f"NNODES={len(nodes)}")
+    out += [" ".join(rust_f64(float(v)) for v in n[:dim]) for n in nodes]
+    out.append(f"NFACES={len(face_nodes)}")
+    for f, fn in enumerate(face_nodes):
+        tag = face_patch[f]
+        tag = "-" if tag is None or tag < 0 else str(int(tag))
+        out.append(" ".join([str(len(fn))] + [str(int(v)) for v in fn] + [tag, str(f), "-"]))
+    out.append(f"NCELLS={len(cell_faces)}")
+    for c, cf in enumerate(cell_faces):
+        out.append(" ".join([str(len(cf))] + [str(int(v)) for v in cf] + [str(c), "-"]))
+    return "\n".join(out) + "\n"
+
+
+def read_msh(text, dim=0):
+    """Mesh::read: (dim, nodes, face_nodes, face_tags, cell_faces); ValueError on
+    a malformed line, NotImplementedError on remote (ghost) entries."""
+    section = "none"
+    left = {"NNODES": 0, "NFACES": 0, "NCELLS": 0, "NPATCH": 0}
+    nodes, face_nodes, tags, cells = [], [], [], []
+    for line in text.splitlines():
+        ls = line.strip()
+        if not ls:
+            continue
+        if ls[0] == "N":
+            parts = ls.split("=")
+            if len(parts) < 2:
+                raise ValueError(ls)
+            section, val = parts[0], int(parts[1])
+            if section == "NDIME":
+                dim = dim or val
+                if val != dim:
+                    raise ValueError("NDIME")
+            elif section in left:
+                left[section] = val
+            continue
+        if section not in left or left[section] == 0:
+            continue
+        tok = ls.split(" ")
+        if section == "NNODES":
+            x = [0.0] * dim
+            for i, t in enumerate(tok[:dim]):
+                x[i] = float(t.strip())
+            nodes.append(x)
+        elif section in ("NFACES", "NCELLS"):
+            size = int(tok[0])
+            if size > 64:
+                raise ValueError("size")
+            idx = [int(v) for v in tok[1:1 + size]]
+            rest = tok[1 + size:]
+            if section == "NFACES":
+                tags.append(None if rest[0] == "-" else int(rest[0]))
+                rest = rest[1:]
+                face_nodes.append(idx)
+            else:
+                cells.append(idx)
+            int(rest[0])
+            if rest[1] != "-":
+                raise NotImplementedError("remote entries")
+        left[section] -= 1
+    return dim, nodes, face_nodes, tags, cells

@@ -198,3 +198,42 @@ def test_bad_input_is_rejected_as_on_the_host(fv):
             with pytest.raises(FvError) as ei:
                 fv.Mesh.from_elements(dim, nodes, k, eptr, e, bp, bnn, bmm, on_device=on_device)
             assert "FV_ERR_INVALID" in str(ei.value), (name, on_device)
+
+
+def test_msh_file_and_explicit_faces_on_device(fv, tmp_path):
+    """Mesh::read of the crate's own format, and explicit faces/cells: device build == host build."""
+    rng = np.random.default_rng(10)
+    meshes = [fv.Mesh.square(9, 0.2, 5), fv.Mesh.cube(4, 0.15, 6),
+              fv.Mesh.from_elements(*_arrays(2, *_mixed_2d(6, rng))), fv.Mesh.from_elements(*_arrays(3, *_hex_3d(3, rng)))]
+    for k, m in enumerate(meshes):
+        path = tmp_path / f"m{k}.msh"
+        m.write(path)
+        host = fv.Mesh.read(path)
+        dev = fv.Mesh.read(path, on_device=True)
+        _same_mesh(host, m)
+        _same_mesh(dev, m)
+        dev2 = fv.Mesh.from_faces(m.dim, m.nodes, m.face_node_ptr, m.face_nodes, m.face_patch, m.cell_face_ptr,
+                                  m.cell_faces, on_device=True)
+        _same_mesh(dev2, m)
+
+
+def test_msh_errors_on_device(fv, tmp_path):
+    from fvb200._lib import FvError
+    m = fv.Mesh.square(3, 0.0, 0)
+    path = tmp_path / "g.msh"
+    m.write(path)
+    lines = path.read_text().splitlines()
+    ci = lines.index(f"NCELLS={m.n_cells}") + 1
+    fi = lines.index(f"NFACES={m.n_faces}") + 1
+    cases = {"remote": ("\n".join(lines[:ci] + [lines[ci][:-1] + "1"] + lines[ci + 1:]), "FV_ERR_UNSUPPORTED"),
+             "node": ("\n".join(lines[:fi] + ["2 0 999 - 0 -"] + lines[fi + 1:]), "FV_ERR_INVALID"),
+             # an interior face that no cell lists any more: its cell now lists face 0 twice
+             "open": ("\n".join(lines[:ci] + [" ".join([lines[ci].split(" ")[0], "0", "0"] + lines[ci].split(" ")[3:])]
+                                + lines[ci + 1:]), "FV_ERR_INVALID")}
+    for name, (text, want) in cases.items():
+        p = tmp_path / f"{name}.msh"
+        p.write_text(text)
+        for on_device in (False, True):
+            with pytest.raises(FvError) as ei:
+                fv.Mesh.read(p, on_device=on_device)
+            assert want in str(ei.value), (name, on_device)
