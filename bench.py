@@ -161,6 +161,8 @@ class Clocks:
 def sweep_schedule(P):
     """Which sweep schedule the preconditioner uses, with its box-tile plan."""
     act, st = P.schedule()
+    if act == 3:
+        return {"kind": "level chunks, next chunk prefetched"}
     if act != 2:
         return {"kind": "level chunks"}
     return {"kind": "box tiles", "box_edge_cells": float(st[0]), "boxes": int(st[1]),
@@ -515,7 +517,7 @@ def batch_arm(args, rank, world, local_rank):
     build()
     import fvb200 as fv
     from fvb200._lib import lib
-    from fvb200.batch import BatchCG, MeshBatch, autotune_tile
+    from fvb200.batch import BatchCG, MeshBatch, autotune_schedule, autotune_tile
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
     t0 = time.time()
@@ -531,6 +533,7 @@ def batch_arm(args, rank, world, local_rank):
     P = fv.IncompleteCholesky.from_matrix(A, 0)
     x = fv.DistributedVector.from_size(mb.n_cells)
     tile, tile_times = autotune_tile(A, mb.cell_offsets, P, b, x)
+    sched, sched_times = autotune_schedule(P, b, x)
     solver = BatchCG(A, mb.cell_offsets, tile)
     # both precisions reach the same FP64 target |b - A x| / |b| <= 1e-10 per problem
     opts_by = {"mixed": dict(precision="mixed", outer_tolerance=BATCH_OUTER_TOL, inner_relative_tolerance=1e-2,
@@ -632,7 +635,8 @@ def batch_arm(args, rank, world, local_rank):
                 choice=choice, trial=trial, other=other, t_other=t_other,
                 other_it_max=int(np.max(out_other["iterations"])),
                 nnz=A.shape()[2], tile=tile, tile_times=tile_times, errs=errs, plain_solves=plain_solves,
-                sample=len(sample), sides=sides, levels=P.levels()[2:], schedule=sweep_schedule(P))
+                sample=len(sample), sides=sides, levels=P.levels()[2:], schedule=sweep_schedule(P),
+                sched_times=sched_times)
 
 
 BATCH_OUTER_TOL = 1e-10
@@ -756,6 +760,7 @@ def main_batch(args, rank, world, local_rank):
         "launched_iterations": int(out["launched_iterations"]), "levels_fwd_bwd": list(res["levels"]),
         "sweep_schedule": res["schedule"],
         "autotune_tile_s": {str(k): round(v, 4) for k, v in res["tile_times"].items()},
+        "autotune_sweep_schedule_ms": {str(k): round(v, 3) for k, v in res["sched_times"].items()},
         "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "mesh_build_s": round(res["t_mesh"], 2),
     }
     if rank == 0:

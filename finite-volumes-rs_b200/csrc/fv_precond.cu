@@ -84,7 +84,8 @@ struct fv_precond {
     double *tmp = nullptr;        // forward-sweep output, kept at sentinel between applies
     unsigned *done = nullptr;     // factorisation flags
     unsigned epoch = 0;
-    int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned)
+    int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned);
+                                  // 3: level chunks, next chunk prefetched
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
@@ -567,6 +568,101 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
     leave(&ctrl[0], &ctrl[1]);
 }
 
+// k_sweep with the next chunk's static data loaded before the current chunk
+// waits: each warp holds two tickets, so twice the rows' independent loads
+// (order -> row bounds -> entries, rhs, 1/diagonal) are in flight while the
+// frontier waits for values.  Tickets are taken and processed in increasing
+// order per warp, so the lowest unfinished ticket is always some warp's
+// current chunk and its dependencies (earlier tickets) are finished.
+template <typename T, int MAXL>
+struct SweepRow {
+    int i, m;
+    bool live;
+    int c[MAXL];
+    T v[MAXL];
+    T s, d;
+};
+
+template <typename T, bool UNIT, int MAXL>
+__device__ __forceinline__ void sweep_stage(SweepRow<T, MAXL> &r, int64_t chunk, int64_t n,
+                                            const int32_t *__restrict__ order, const int32_t *__restrict__ ptr,
+                                            const int32_t *__restrict__ col, const T *__restrict__ val,
+                                            const T *__restrict__ dinv, const T *rhs, const fv_row_skip &rs) {
+    const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+    r.live = idx < n;
+    if (!r.live) return;
+    r.i = __ldg(&order[idx]);
+    if (rs.group && rs.done[(int64_t)__ldg(&rs.group[r.i]) * rs.stride]) {
+        r.live = false;
+        return;
+    }
+    const int k0 = __ldg(&ptr[r.i]);
+    r.m = __ldg(&ptr[r.i + 1]) - k0;
+#pragma unroll
+    for (int q = 0; q < MAXL; ++q)
+        if (q < r.m) {
+            r.c[q] = __ldg(&col[k0 + q]);
+            r.v[q] = __ldg(&val[k0 + q]);
+        }
+    r.s = rhs[r.i];
+    r.d = UNIT ? T(1) : __ldg(&dinv[r.i]);
+}
+
+template <typename T, bool UNIT, int MAXL>
+__global__ void __launch_bounds__(256) k_sweep_pf(int64_t n, const int32_t *__restrict__ order,
+                                                  const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                                                  const T *__restrict__ val, const T *__restrict__ dinv,
+                                                  const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
+                                                  int *err, const int *skip, fv_row_skip rs) {
+    if (skip && *(volatile const int *)skip) return;
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    bool have = take_chunk(&ctrl[0], nchunks, chunk);
+    SweepRow<T, MAXL> a, b;
+    if (have) sweep_stage<T, UNIT, MAXL>(a, chunk, n, order, ptr, col, val, dinv, rhs, rs);
+    while (have) {
+        int64_t next;
+        const bool have_next = take_chunk(&ctrl[0], nchunks, next);
+        if (have_next) sweep_stage<T, UNIT, MAXL>(b, next, n, order, ptr, col, val, dinv, rhs, rs);
+        if (a.live) {
+            T xv[MAXL];
+            unsigned pending = 0;
+#pragma unroll
+            for (int q = 0; q < MAXL; ++q)
+                if (q < a.m && !fv_slot_ready(&x[a.c[q]], xv[q])) pending |= 1u << q;
+            if (pending) {
+                const unsigned long long t0 = fv_globaltimer();
+                for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                    for (int q = 0; q < MAXL; ++q)
+                        if ((pending >> q) & 1u)
+                            if (fv_slot_ready(&x[a.c[q]], xv[q])) pending &= ~(1u << q);
+                    if (pending && (it & 255u) == 0) {
+                        if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
+                            if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+#pragma unroll
+                            for (int q = 0; q < MAXL; ++q)
+                                if ((pending >> q) & 1u) xv[q] = T(NAN);
+                            pending = 0;
+                        }
+                    }
+                }
+            }
+            T s = a.s;
+#pragma unroll
+            for (int q = 0; q < MAXL; ++q)
+                if (q < a.m) s = s - a.v[q] * xv[q];
+            const T r = UNIT ? s : a.d * s;
+            fv_publish(&x[a.i], r);
+            if (rhs_reset) fv_reset_slot(&rhs_reset[a.i]);
+            if (next_reset) fv_reset_slot(&next_reset[a.i]);
+        }
+        a = b;
+        have = have_next;
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
 // Rows longer than 32 entries on the swept side: one dependency at a time.
 template <typename T, bool UNIT>
 __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__restrict__ order,
@@ -599,8 +695,15 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
 template <typename T, bool UNIT>
 static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
                          const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
-                         T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs = {}) {
-    if (maxl <= 4)
+                         T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs = {},
+                         bool prefetch = false) {
+    if (prefetch && maxl <= 4)
+        fv_note_launch(), k_sweep_pf<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                   next_reset, ctrl, err, skip, rs);
+    else if (prefetch && maxl <= 8)
+        fv_note_launch(), k_sweep_pf<T, UNIT, 8><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
+                                                                   next_reset, ctrl, err, skip, rs);
+    else if (maxl <= 4)
         fv_note_launch(), k_sweep<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
                                                                 next_reset, ctrl, err, skip, rs);
     else if (maxl <= 8)
@@ -894,15 +997,16 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
+    const bool pf = P->schedule == 3;
     if (P->kind == 2)
         launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr, r,
-                                   P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
+                                   P->tmp, nullptr, z, P->ctrl, P->err, skip, rs, pf);
     else
         launch_sweep<double, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv, r,
-                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs);
+                                    P->tmp, nullptr, z, P->ctrl, P->err, skip, rs, pf);
     FV_CUDA_TRY(cudaGetLastError());
     launch_sweep<double, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv, P->tmp,
-                                z, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs);
+                                z, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs, pf);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
@@ -959,26 +1063,27 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
     const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
+    const bool pf = P->schedule == 3;
     if (P->kind == 2)
         launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
-                                  P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
+                                  P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs, pf);
     else
         launch_sweep<float, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, P->dinv32, r,
-                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs);
+                                   P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs, pf);
     FV_CUDA_TRY(cudaGetLastError());
     launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
-                               P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs);
+                               P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs, pf);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
 
 extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
-    if (!P || request < -1 || request > 2) return FV_ERR_INVALID;
+    if (!P || request < -1 || request > 3) return FV_ERR_INVALID;
     fv_symbolic *s = P->sym;
     if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
     if (request == 2 && !s->tiled) return FV_ERR_UNSUPPORTED;
-    if (request >= 0) P->schedule = request == 2 ? 2 : 1;
-    if (active) *active = use_tiles(P) ? 2 : 1;
+    if (request >= 0) P->schedule = request <= 1 ? 1 : request;
+    if (active) *active = use_tiles(P) ? 2 : (P->schedule == 3 ? 3 : 1);
     if (stats) {
         stats[0] = s->t_edge;
         stats[1] = s->t_nb[0];

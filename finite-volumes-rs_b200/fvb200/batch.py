@@ -147,3 +147,25 @@ def autotune_tile(A, row_offsets, P, b, x, candidates=(256, 512, 1024, 2048), it
         if dt < best_t:
             best, best_t = tile, dt
     return best, timings
+
+
+def autotune_schedule(P, b, x, candidates=(1, 3), reps=3, stream=None):
+    """Pick the faster sweep schedule for this preconditioner (level chunks, or
+    level chunks with the next chunk prefetched: the same bits either way) by
+    timing a few applies of each; returns (chosen, {schedule: ms per apply})."""
+    import torch
+    times = {}
+    for sch in candidates:
+        P.schedule(sch)
+        P.precondition(x, b, stream=stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            P.precondition(x, b, stream=stream)
+        ev[1].record()
+        torch.cuda.synchronize()
+        times[sch] = ev[0].elapsed_time(ev[1]) / reps
+    best = min(times, key=times.get)
+    P.schedule(best)
+    return best, times

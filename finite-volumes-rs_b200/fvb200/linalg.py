@@ -278,9 +278,10 @@ class Preconditioner:
 
     def schedule(self, request: int = -1):
         """Sweep schedule: request -1 = query, 0 or 1 = level chunks (default),
-        2 = box tiles (matrices assembled on a mesh).  Returns (active, stats)
-        with active 1 (level chunks) or 2 (box tiles) and stats = (box edge in
-        cell sizes, boxes, lane use fwd/bwd, ring share fwd/bwd)."""
+        2 = box tiles (matrices assembled on a mesh), 3 = level chunks with
+        the next chunk prefetched.  Returns (active, stats) with active 1, 2
+        or 3 and stats = (box edge in cell sizes, boxes, lane use fwd/bwd,
+        ring share fwd/bwd)."""
         act = C.c_int32()
         st = np.zeros(6)
         check(lib().fv_precond_schedule(self.handle, int(request), C.byref(act),

@@ -331,8 +331,9 @@ fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bw
                             int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream);
 /* Sweep schedule of P.  request: -1 query only; 0 or 1 level chunks (the
  * default); 2 box tiles, available when the matrix was assembled on a mesh
- * whose box order exists (FV_ERR_UNSUPPORTED otherwise).  *active receives
- * 1 (level chunks) or 2 (box tiles).  stats (optional, 6 doubles): box edge
+ * whose box order exists (FV_ERR_UNSUPPORTED otherwise); 3 level chunks with
+ * each warp loading its next chunk's rows before waiting on the current one.
+ * *active receives 1, 2 or 3.  stats (optional, 6 doubles): box edge
  * in mean cell sizes, number of boxes, lane use of the forward / backward
  * steps, share of dependencies read from shared memory forward / backward
  * (zeros without a tiling).  Both schedules give the same bits. */

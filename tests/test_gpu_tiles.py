@@ -1,4 +1,5 @@
-"""Box-tiled sweeps on the GPU: the same bits as the level-ordered sweeps.
+"""Box-tiled sweeps, and level chunks with the next chunk prefetched, on the
+GPU: the same bits as the level-ordered sweeps.
 
 A matrix assembled on a mesh gets a box tiling at factorisation; the tiled
 sweeps must reproduce the level-chunk sweeps (and so the oracle) bit for bit,
@@ -35,6 +36,12 @@ def test_tiled_apply_equals_level_apply_and_oracle(fv, orc, kind):
     ptr, cols, vals, _ = oracle_system(orc, case)
     want = orc.Precond("ilu" if kind == "3d" else "ic", ptr, cols, vals).apply(r.numpy())
     assert np.array_equal(z_tiles.numpy(), want)
+    # level chunks with the next chunk prefetched: same bits
+    assert P.schedule(3)[0] == 3
+    z_pf = fv.DistributedVector.from_size(A.nrows())
+    for _ in range(3):
+        P.precondition(z_pf, r)
+    assert np.array_equal(z_pf.numpy(), want)
     # repeated applies keep the sentinel protocol intact
     P.schedule(2)
     for _ in range(3):
@@ -48,14 +55,15 @@ def test_tiled_solve_equals_level_solve(fv):
     P = fv.IncompleteLowerUpper.from_matrix(A, 0)
     opts = fv.LinearSolverOptions(1e-10, 1e-10, 2000)
     out = {}
-    for req in (2, 1):
+    for req in (2, 3, 1):
         P.schedule(req)
         x = fv.DistributedVector.from_size(A.nrows())
         info = fv.bi_conjugate_gradient_stab(x, A, b, P, None, opts)
         out[req] = (x.numpy(), info.iterations, info.history)
-    assert out[2][1] == out[1][1]
-    assert np.array_equal(out[2][0], out[1][0])
-    assert out[2][2] == out[1][2]
+    for req in (2, 3):
+        assert out[req][1] == out[1][1]
+        assert np.array_equal(out[req][0], out[1][0])
+        assert out[req][2] == out[1][2]
 
 
 def test_tiled_fp32_batch_equals_level_batch(fv):
@@ -70,10 +78,11 @@ def test_tiled_fp32_batch_equals_level_batch(fv):
     P = fv.IncompleteCholesky.from_matrix(A, 0)
     assert P.schedule(2)[0] == 2
     res = {}
-    for req in (2, 1):
+    for req in (2, 3, 1):
         P.schedule(req)
         x = fv.DistributedVector.from_size(mb.n_cells)
         o = BatchCG(A, mb.cell_offsets, 256).solve(P, b, x, precision="mixed", outer_tolerance=1e-10)
         res[req] = (x.numpy(), list(o["iterations"]))
-    assert res[2][1] == res[1][1]
-    assert np.array_equal(res[2][0], res[1][0])
+    for req in (2, 3):
+        assert res[req][1] == res[1][1]
+        assert np.array_equal(res[req][0], res[1][0])
