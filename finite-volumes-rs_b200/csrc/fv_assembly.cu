@@ -787,6 +787,7 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     m->n_bfaces = Fb;
     m->maxf = maxf;
     m->padf = padf;
+    m->ncf = ncf;
     cudaStream_t st = fv_stream(stream);
     cudaError_t e = cudaSuccess;
     e = cudaMalloc(&m->face_cells, sizeof(int2) * F);

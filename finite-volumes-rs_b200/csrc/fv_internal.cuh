@@ -62,6 +62,7 @@ struct fv_mesh {
     int32_t *cf_other = nullptr;       // the other cell, -1 for boundary faces
     int2 *cf_pad = nullptr;            // (cf_face, cf_other) at cell * padf + slot, padded with (0, -2)
     int padf = 0;                      // 4 or 8 (0: no padded copy, cells with more than 8 faces)
+    int64_t ncf = 0;                   // entries of cf_face / cf_other
     // Corrected scheme / gradients (present when uploaded with normals and cell_faces)
     double4 *face_normal = nullptr;    // per face (x, y, z|0, 0)
     double4 *face_center = nullptr;    // per face, all faces

@@ -718,6 +718,7 @@ fv_status finish(Scratch &sc, fv_mesh *m, int64_t L, int *d_flags, int64_t n_nod
         return FV_ERR_UNSUPPORTED;
     }
     m->maxf = maxf;
+    m->ncf = ncf;
     m->padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
     e = cudaMalloc(&m->cf_face, sizeof(int32_t) * (ncf ? ncf : 1));
     if (e == cudaSuccess) e = cudaMalloc(&m->cf_other, sizeof(int32_t) * (ncf ? ncf : 1));
@@ -1030,6 +1031,174 @@ extern "C" fv_status fv_mesh_build_faces(int32_t dim, int64_t n_nodes, const dou
     if (flag_status(h_flags[0]) != FV_OK) return give_up(FV_ERR_INVALID);
     const fv_status fs = finish(sc, m, L, d_flags, n_nodes, nodes, fnp, fnodes, patch, host_out);
     if (fs != FV_OK) return give_up(fs);
+    *out = m;
+    return FV_OK;
+}
+
+// ---------------------------------------------------------------- union of meshes
+// One mesh from several resident meshes, laid out as a batch of independent
+// problems: the interior faces of every part first (in part order), then the
+// boundary faces of every part; cells in part order.  Each part keeps its
+// faces' relative order, and interior faces stay ahead of boundary faces, so
+// every cell's ascending face list maps to an ascending list: assembly and
+// factorisation of the union give each part's own system on the diagonal,
+// exactly as the same union uploaded from host arrays.  Gradient data is not
+// carried over (the union has none, like a host upload without normals).
+namespace {
+
+struct CatPtrs {
+    const int2 *const *face_cells;
+    const double *const *face_area;
+    const double4 *const *bface_center;
+    const double4 *const *cell;
+    const int32_t *const *cf_ptr;
+    const int32_t *const *cf_face;
+    const int32_t *const *cf_other;
+    const int64_t *co, *io, *bo, *cfo, *fi;  // cell / interior-face / boundary-face / cf-entry offsets, interior faces
+};
+
+__device__ __forceinline__ int part_of(const int64_t *off, int P, int64_t x) {  // largest p with off[p] <= x
+    int lo = 0, hi = P - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int32_t union_face(const CatPtrs &q, int64_t TI, int p, int32_t f) {
+    return (int32_t)(f < q.fi[p] ? q.io[p] + f : TI + q.bo[p] + (f - q.fi[p]));
+}
+
+__global__ void k_cat_faces(int64_t F, int64_t TI, int P, CatPtrs q, int2 *__restrict__ fc, double *__restrict__ area,
+                            double4 *__restrict__ bfc) {
+    const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= F) return;
+    int p;
+    int64_t f;
+    if (u < TI) {
+        p = part_of(q.io, P, u);
+        f = u - q.io[p];
+    } else {
+        p = part_of(q.bo, P, u - TI);
+        f = q.fi[p] + (u - TI - q.bo[p]);
+    }
+    const int2 on = q.face_cells[p][f];
+    fc[u] = make_int2(on.x + (int32_t)q.co[p], on.y >= 0 ? on.y + (int32_t)q.co[p] : on.y);
+    area[u] = q.face_area[p][f];
+    if (u >= TI) bfc[u - TI] = q.bface_center[p][f - q.fi[p]];
+}
+
+__global__ void k_cat_cells(int64_t N, int64_t TI, int P, CatPtrs q, int padf, double4 *__restrict__ cell,
+                            int32_t *__restrict__ cf_ptr, int32_t *__restrict__ cf_face,
+                            int32_t *__restrict__ cf_other, int2 *__restrict__ cf_pad) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    const int p = part_of(q.co, P, c);
+    const int64_t cl = c - q.co[p];
+    cell[c] = q.cell[p][cl];
+    const int32_t k0 = q.cf_ptr[p][cl], k1 = q.cf_ptr[p][cl + 1];
+    const int64_t base = q.cfo[p];
+    cf_ptr[c] = (int32_t)(base + k0);
+    if (c == N - 1) cf_ptr[N] = (int32_t)q.cfo[P];
+    for (int32_t k = k0; k < k1; ++k) {
+        const int32_t raw = q.cf_face[p][k];
+        const int32_t f = union_face(q, TI, p, raw & 0x7fffffff) | (raw & (int32_t)0x80000000);
+        const int32_t o = q.cf_other[p][k];
+        const int32_t other = o >= 0 ? o + (int32_t)q.co[p] : o;
+        cf_face[base + k] = f;
+        cf_other[base + k] = other;
+        if (padf && k - k0 < padf) cf_pad[c * padf + (k - k0)] = make_int2(f, other);
+    }
+    for (int s = k1 - k0; s < padf; ++s) cf_pad[c * padf + s] = make_int2(0, -2);
+}
+
+}  // namespace
+
+extern "C" fv_status fv_mesh_concat(const fv_mesh *const *parts, int32_t n_parts, void *stream, fv_mesh **out) {
+    if (!parts || n_parts <= 0 || !out) return FV_ERR_INVALID;
+    *out = nullptr;
+    const int P = n_parts;
+    const int dim = parts[0] ? parts[0]->dim : 0;
+    std::vector<int64_t> co(P + 1, 0), io(P + 1, 0), bo(P + 1, 0), cfo(P + 1, 0), fi(P, 0);
+    int maxf = 0;
+    for (int p = 0; p < P; ++p) {
+        const fv_mesh *m = parts[p];
+        if (!m || m->dim != dim || !m->cf_ptr || m->n_cells <= 0) return FV_ERR_INVALID;
+        fi[p] = m->n_faces - m->n_bfaces;
+        co[p + 1] = co[p] + m->n_cells;
+        io[p + 1] = io[p] + fi[p];
+        bo[p + 1] = bo[p] + m->n_bfaces;
+        cfo[p + 1] = cfo[p] + m->ncf;
+        maxf = std::max(maxf, m->maxf);
+    }
+    const int64_t N = co[P], TI = io[P], TB = bo[P], F = TI + TB, NCF = cfo[P];
+    if (N >= 0x7fffffffLL || F >= 0x7fffffffLL || NCF >= 0x7fffffffLL) return FV_ERR_UNSUPPORTED;
+    cudaStream_t st = fv_stream(stream);
+    std::vector<const void *> ptrs((size_t)7 * P);
+    for (int p = 0; p < P; ++p) {
+        ptrs[0 * P + p] = parts[p]->face_cells;
+        ptrs[1 * P + p] = parts[p]->face_area;
+        ptrs[2 * P + p] = parts[p]->bface_center;
+        ptrs[3 * P + p] = parts[p]->cell;
+        ptrs[4 * P + p] = parts[p]->cf_ptr;
+        ptrs[5 * P + p] = parts[p]->cf_face;
+        ptrs[6 * P + p] = parts[p]->cf_other;
+    }
+    std::vector<int64_t> offs;
+    offs.reserve((size_t)5 * (P + 1));
+    for (auto *v : {&co, &io, &bo, &cfo}) offs.insert(offs.end(), v->begin(), v->end());
+    offs.insert(offs.end(), fi.begin(), fi.end());
+    Scratch sc(st);
+    const void **d_ptrs = nullptr;
+    int64_t *d_offs = nullptr;
+    cudaError_t e = to_device(sc, d_ptrs, ptrs.data(), ptrs.size());
+    if (e == cudaSuccess) e = to_device(sc, d_offs, offs.data(), offs.size());
+    fv_mesh *m = new fv_mesh();
+    m->dim = dim;
+    m->n_cells = N;
+    m->n_faces = F;
+    m->n_bfaces = TB;
+    m->maxf = maxf;
+    m->padf = maxf <= 4 ? 4 : (maxf <= 8 ? 8 : 0);
+    m->ncf = NCF;
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_cells, sizeof(int2) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->face_area, sizeof(double) * F);
+    if (e == cudaSuccess) e = cudaMalloc(&m->bface_center, sizeof(double4) * (TB ? TB : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cell, sizeof(double4) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_ptr, sizeof(int32_t) * (N + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_face, sizeof(int32_t) * (NCF ? NCF : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&m->cf_other, sizeof(int32_t) * (NCF ? NCF : 1));
+    if (e == cudaSuccess && m->padf) e = cudaMalloc(&m->cf_pad, sizeof(int2) * N * m->padf);
+    if (e == cudaSuccess) {
+        CatPtrs q;
+        q.face_cells = reinterpret_cast<const int2 *const *>(d_ptrs + 0 * P);
+        q.face_area = reinterpret_cast<const double *const *>(d_ptrs + 1 * P);
+        q.bface_center = reinterpret_cast<const double4 *const *>(d_ptrs + 2 * P);
+        q.cell = reinterpret_cast<const double4 *const *>(d_ptrs + 3 * P);
+        q.cf_ptr = reinterpret_cast<const int32_t *const *>(d_ptrs + 4 * P);
+        q.cf_face = reinterpret_cast<const int32_t *const *>(d_ptrs + 5 * P);
+        q.cf_other = reinterpret_cast<const int32_t *const *>(d_ptrs + 6 * P);
+        q.co = d_offs;
+        q.io = d_offs + (P + 1);
+        q.bo = d_offs + 2 * (P + 1);
+        q.cfo = d_offs + 3 * (P + 1);
+        q.fi = d_offs + 4 * (P + 1);
+        fv_note_launch();
+        k_cat_faces<<<blocks(F), kB, 0, st>>>(F, TI, P, q, m->face_cells, m->face_area, m->bface_center);
+        fv_note_launch();
+        k_cat_cells<<<blocks(N), kB, 0, st>>>(N, TI, P, q, m->padf, m->cell, m->cf_ptr, m->cf_face, m->cf_other,
+                                              m->cf_pad);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging vectors go out of scope
+    if (e != cudaSuccess) {
+        fv_mesh_destroy(m);
+        return fail(e, "fv_mesh_concat");
+    }
     *out = m;
     return FV_OK;
 }

@@ -27,6 +27,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cub/cub.cuh>
+
 #include "fv_internal.cuh"
 
 struct fv_symbolic {
@@ -39,7 +41,8 @@ struct fv_symbolic {
     int32_t max_row = 0;                         // longest row of the pattern
     int32_t max_lower = 0, max_upper = 0;        // longest strict-lower / strict-upper row
     bool symmetric_pattern = false;
-    std::vector<int32_t> h_fwd_level, h_bwd_level;
+    std::vector<int32_t> h_fwd_level, h_bwd_level;   // host copies (filled on demand for device-built schedules)
+    int32_t *d_fwd_level = nullptr, *d_bwd_level = nullptr;  // device-built schedules only
     // box tiling of the two sweeps ([0] forward over L, [1] backward over U);
     // absent (tiled = false) for matrices without mesh geometry or without an
     // acyclic box order
@@ -65,6 +68,8 @@ void fv_symbolic_free(fv_symbolic *s) {
     cudaFree(s->fwd_order);
     cudaFree(s->bwd_order);
     cudaFree(s->l_tpos);
+    cudaFree(s->d_fwd_level);
+    cudaFree(s->d_bwd_level);
     for (int d = 0; d < 2; ++d) {
         cudaFree(s->t_box_step[d]);
         cudaFree(s->t_slot_row[d]);
@@ -237,6 +242,8 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     return FV_OK;
 }
 
+static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st);
+
 // Box tiles of the two sweeps, planned on first request when the matrix was
 // assembled on a mesh (cell centres known); s->tiled says whether a plan exists.
 static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
@@ -259,6 +266,7 @@ static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
     FV_CUDA_TRY(cudaStreamSynchronize(st));
     fv_tile_plan tp[2];
     if (s->max_lower > FV_TILE_MAXL || s->max_upper > FV_TILE_MAXL) return FV_OK;
+    FV_TRY(ensure_host_levels(s, st));
     if (!fv_build_tile_plans(n, A->mesh->dim, (const double *)cells.data(), lp.data(), lc.data(), up.data(),
                              uc.data(), s->h_fwd_level.data(), s->h_bwd_level.data(), fo.data(), bo.data(),
                              FV_TILE_RING, tp[0], tp[1]))
@@ -318,9 +326,31 @@ static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
     return FV_OK;
 }
 
+static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symbolic **out);
+
+// The device analysis serves every pattern without IC(k) fill entries; the
+// host one keeps the fill entries' special place in the backward sweep.
 fv_status fv_get_symbolic(fv_csr *A, cudaStream_t st, fv_symbolic **out) {
-    if (!A->sym) FV_TRY(build_symbolic(A, st, &A->sym));
+    if (!A->sym) {
+        if (A->fill_mask.empty())
+            FV_TRY(build_symbolic_device(A, st, &A->sym));
+        else
+            FV_TRY(build_symbolic(A, st, &A->sym));
+    }
     *out = A->sym;
+    return FV_OK;
+}
+
+// Host copies of the level of every row (box-tile planning, fv_precond_levels).
+static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st) {
+    if (!s->h_fwd_level.empty() || s->n == 0 || !s->d_fwd_level) return FV_OK;
+    s->h_fwd_level.resize((size_t)s->n);
+    s->h_bwd_level.resize((size_t)s->n);
+    FV_CUDA_TRY(cudaMemcpyAsync(s->h_fwd_level.data(), s->d_fwd_level, sizeof(int32_t) * s->n,
+                                cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(s->h_bwd_level.data(), s->d_bwd_level, sizeof(int32_t) * s->n,
+                                cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
     return FV_OK;
 }
 
@@ -977,6 +1007,272 @@ static fv_status tiled_apply(fv_precond *P, const T *r, T *z, T *tmp, cudaStream
     return FV_OK;
 }
 
+static int sweep_grid(int64_t n);
+
+// ------------------------------------------------------------------ symbolic on the device
+// The same analysis as build_symbolic: strict lower / upper parts, the level
+// of every row (longest dependency chain), rows ordered by level (ascending
+// row within a level), and the transpose map of IC.  Levels come from a
+// sync-free sweep in natural row order (reverse order for the upper part):
+// a row's dependencies are lower (higher) rows, so they sit in earlier
+// chunks or earlier lanes of the same chunk.
+namespace {
+
+enum : int { kSymUnsorted = 1, kSymNoDiag = 2, kSymRange = 4, kSymAsym = 8 };
+
+__global__ void k_sym_count(int64_t n, const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                            int32_t *__restrict__ cl, int32_t *__restrict__ cu, int *flags, int *maxes) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int nl = 0, nu = 0, len = 0, bad = 0;
+    if (i < n) {
+        bool diag = false;
+        const int k0 = ptr[i], k1 = ptr[i + 1];
+        len = k1 - k0;
+        for (int k = k0; k < k1; ++k) {
+            const int c = col[k];
+            if (c < 0 || c >= n) bad |= kSymRange;
+            if (k > k0 && c <= col[k - 1]) bad |= kSymUnsorted;
+            if (c < i)
+                ++nl;
+            else if (c > i)
+                ++nu;
+            else
+                diag = true;
+        }
+        if (!diag) bad |= kSymNoDiag;
+        cl[i] = nl;
+        cu[i] = nu;
+    }
+    const int ml = __reduce_max_sync(0xffffffffu, nl), mu = __reduce_max_sync(0xffffffffu, nu);
+    const int mr = __reduce_max_sync(0xffffffffu, len), bo = __reduce_or_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&maxes[0], ml);
+        atomicMax(&maxes[1], mu);
+        atomicMax(&maxes[2], mr);
+        if (bo) atomicOr(flags, bo);
+    }
+}
+
+__global__ void k_sym_split(int64_t n, const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                            const int32_t *__restrict__ lp, const int32_t *__restrict__ up,
+                            int32_t *__restrict__ lc, int32_t *__restrict__ uc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int a = lp[i], b = up[i];
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+        const int c = col[k];
+        if (c < i) lc[a++] = c;
+        if (c > i) uc[b++] = c;
+    }
+}
+
+// level[i] = 1 + max level of the row's dependencies (0 without any); slots
+// start at all-ones (no level yet).  Bounded waits as in the sweeps.
+__global__ void __launch_bounds__(256) k_sym_levels(int64_t n, int upper, const int32_t *__restrict__ ptr,
+                                                    const int32_t *__restrict__ col, int32_t *level,
+                                                    unsigned *ctrl, int *err, int *nlev) {
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    int top = -1;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int64_t i = upper ? n - 1 - idx : idx;
+        int lev = 0;
+        for (int k = __ldg(&ptr[i]); k < __ldg(&ptr[i + 1]); ++k) {
+            const int32_t c = __ldg(&col[k]);
+            unsigned v = fv_ld_relaxed_u32(&level[c]);
+            if (v == 0xFFFFFFFFu) {
+                const unsigned long long t0 = fv_globaltimer();
+                for (unsigned it = 1; v == 0xFFFFFFFFu; ++it) {
+                    v = fv_ld_relaxed_u32(&level[c]);
+                    if (v == 0xFFFFFFFFu && (it & 255u) == 0 &&
+                        (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS)) {
+                        if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+                        v = 0;
+                    }
+                }
+            }
+            lev = max(lev, (int)v + 1);
+        }
+        asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(&level[i]), "r"((unsigned)lev) : "memory");
+        top = max(top, lev);
+    }
+    top = __reduce_max_sync(0xffffffffu, top);
+    if ((threadIdx.x & 31) == 0) atomicMax(nlev, top + 1);
+    leave(&ctrl[0], &ctrl[1]);
+}
+
+__global__ void k_sym_iota(int64_t n, int32_t *__restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (int32_t)i;
+}
+
+// L entry (i, j) -> position of (j, i) among U's entries; a missing mirror
+// entry marks the pattern unsymmetric.
+__global__ void k_sym_tpos(int64_t n, const int32_t *__restrict__ lp, const int32_t *__restrict__ lc,
+                           const int32_t *__restrict__ up, const int32_t *__restrict__ uc,
+                           int32_t *__restrict__ tpos, int *flags) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int bad = 0;
+    if (i < n) {
+        for (int k = lp[i]; k < lp[i + 1]; ++k) {
+            const int j = lc[k];
+            int lo = up[j], hi = up[j + 1];
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (uc[mid] < i)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (lo < up[j + 1] && uc[lo] == i)
+                tpos[k] = lo;
+            else
+                bad = kSymAsym;
+        }
+    }
+    if (__reduce_or_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, kSymAsym);
+}
+
+}  // namespace
+
+static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symbolic **out) {
+    const int64_t n = A->nrows;
+    if (n <= 0 || n >= 0x7fffffffLL || A->nnz >= 0x7fffffffLL) return FV_ERR_INVALID;
+    const unsigned G = (unsigned)((n + 255) / 256);
+    fv_symbolic *s = new fv_symbolic();
+    s->n = n;
+    int *dw = nullptr;  // [0] flags [1..3] max lower / upper / row [4] err [5,6] levels fwd / bwd
+    unsigned *ctrl = nullptr;
+    int32_t *cnt = nullptr, *keys = nullptr, *iota = nullptr;
+    void *tmp = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(dw);
+        cudaFree(ctrl);
+        cudaFree(cnt);
+        cudaFree(keys);
+        cudaFree(iota);
+        cudaFree(tmp);
+    };
+    auto fail = [&](cudaError_t e, const char *what) {
+        fv_internal_set_cuda_error(e, what);
+        cleanup();
+        fv_symbolic_free(s);
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    };
+    auto reject = [&](fv_status code) {
+        cleanup();
+        fv_symbolic_free(s);
+        return code;
+    };
+    cudaError_t e = cudaMalloc(&dw, sizeof(int) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&ctrl, sizeof(unsigned) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&cnt, sizeof(int32_t) * 2 * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->l_ptr, sizeof(int32_t) * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->u_ptr, sizeof(int32_t) * (n + 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(dw, 0, sizeof(int) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctrl, 0, sizeof(unsigned) * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(int32_t) * 2 * (n + 1), st);
+    if (e == cudaSuccess) {
+        fv_note_launch();
+        k_sym_count<<<G, 256, 0, st>>>(n, A->row_ptr, A->cols, cnt, cnt + (n + 1), dw, dw + 1);
+        e = cudaGetLastError();
+    }
+    size_t tb = 0, tb2 = 0;
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, s->l_ptr, (int)(n + 1), st);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb2, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, 32, st);
+    tb = std::max(tb, tb2);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, s->l_ptr, (int)(n + 1), st);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt + (n + 1), s->u_ptr, (int)(n + 1), st);
+    int h[8] = {0};
+    int32_t nl = 0, nu = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, dw, sizeof(int) * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nl, s->l_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nu, s->u_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(e, "symbolic (counts)");
+    if (h[0]) return reject(FV_ERR_INVALID);  // unsorted / duplicate columns, no diagonal (the reference panics)
+    s->nnz_l = nl;
+    s->nnz_u = nu;
+    s->max_lower = h[1];
+    s->max_upper = h[2];
+    s->max_row = h[3];
+    e = cudaMalloc(&s->l_col, sizeof(int32_t) * (nl ? nl : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->u_col, sizeof(int32_t) * (nu ? nu : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_fwd_level, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_bwd_level, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->fwd_order, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->bwd_order, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&keys, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&iota, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_fwd_level, 0xFF, sizeof(int32_t) * n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_bwd_level, 0xFF, sizeof(int32_t) * n, st);
+    if (e == cudaSuccess) {
+        fv_note_launch();
+        k_sym_split<<<G, 256, 0, st>>>(n, A->row_ptr, A->cols, s->l_ptr, s->u_ptr, s->l_col, s->u_col);
+        fv_note_launch();
+        k_sym_iota<<<G, 256, 0, st>>>(n, iota);
+        const int SG = sweep_grid(n);
+        fv_note_launch();
+        k_sym_levels<<<SG, 256, 0, st>>>(n, 0, s->l_ptr, s->l_col, s->d_fwd_level, ctrl, dw + 4, dw + 5);
+        fv_note_launch();
+        k_sym_levels<<<SG, 256, 0, st>>>(n, 1, s->u_ptr, s->u_col, s->d_bwd_level, ctrl + 2, dw + 4, dw + 6);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, dw, sizeof(int) * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(e, "symbolic (levels)");
+    if (h[4]) {
+        fv_internal_set_error_text("symbolic analysis: level sweep timed out");
+        return reject(FV_ERR_TIMEOUT);
+    }
+    s->n_fwd_levels = h[5];
+    s->n_bwd_levels = h[6];
+    // rows by level, ascending row within a level (the radix sort is stable)
+    for (int d = 0; d < 2 && e == cudaSuccess; ++d) {
+        const int32_t nlev = d == 0 ? s->n_fwd_levels : s->n_bwd_levels;
+        int bits = 1;
+        while (bits < 31 && (1 << bits) < nlev) ++bits;
+        size_t need = 0;
+        e = cub::DeviceRadixSort::SortPairs(nullptr, need, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, bits, st);
+        if (e == cudaSuccess && need > tb) {
+            cudaFree(tmp);
+            tmp = nullptr;
+            tb = need;
+            e = cudaMalloc(&tmp, tb);
+        }
+        if (e != cudaSuccess) break;
+        e = cub::DeviceRadixSort::SortPairs(tmp, tb, (const uint32_t *)(d == 0 ? s->d_fwd_level : s->d_bwd_level),
+                                            (uint32_t *)keys, iota, d == 0 ? s->fwd_order : s->bwd_order, (int)n, 0,
+                                            bits, st);
+    }
+    // transpose map (IC) when the pattern is structurally symmetric
+    if (e == cudaSuccess && nl == nu) {
+        e = cudaMalloc(&s->l_tpos, sizeof(int32_t) * (nl ? nl : 1));
+        if (e == cudaSuccess) {
+            fv_note_launch();
+            k_sym_tpos<<<G, 256, 0, st>>>(n, s->l_ptr, s->l_col, s->u_ptr, s->u_col, s->l_tpos, dw);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, dw, sizeof(int) * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(e, "symbolic (orders)");
+    s->symmetric_pattern = nl == nu && !(h[0] & kSymAsym);
+    if (!s->symmetric_pattern) {
+        cudaFree(s->l_tpos);
+        s->l_tpos = nullptr;
+    }
+    cleanup();
+    *out = s;
+    return FV_OK;
+}
+
 static int sweep_grid(int64_t n) {
     int64_t warps = (n + 31) / 32;
     int64_t blocks = (warps + 7) / 8;
@@ -1440,9 +1736,9 @@ extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_
 
 extern "C" fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,
                                        int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream) {
-    (void)stream;
     if (!P) return FV_ERR_INVALID;
-    const fv_symbolic *s = P->sym;
+    fv_symbolic *s = P->sym;
+    if (fwd_level || bwd_level) FV_TRY(ensure_host_levels(s, fv_stream(stream)));
     if (fwd_level) std::copy(s->h_fwd_level.begin(), s->h_fwd_level.end(), fwd_level);
     if (bwd_level) std::copy(s->h_bwd_level.begin(), s->h_bwd_level.end(), bwd_level);
     if (n_fwd_levels) *n_fwd_levels = s->n_fwd_levels;

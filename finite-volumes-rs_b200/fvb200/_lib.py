@@ -120,6 +120,7 @@ _SIGS = {
     "fv_mesh_build_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_build_su2": [C.c_char_p, C.c_int32, vp, P(vp), P(P(HostMesh_))],
     "fv_mesh_build_msh": [C.c_char_p, C.c_int32, vp, P(vp), P(P(HostMesh_))],
+    "fv_mesh_concat": [P(vp), C.c_int32, vp, P(vp)],
     "fv_mesh_build_faces": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, vp, P(vp), P(P(HostMesh_))],
     "fv_host_mesh_from_faces": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, P(P(HostMesh_))],
     "fv_host_mesh_read_msh": [C.c_char_p, C.c_int32, P(P(HostMesh_))],

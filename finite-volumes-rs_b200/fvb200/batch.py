@@ -11,6 +11,7 @@ per-problem scalars (fv_batch_cg).
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import time
 
 import numpy as np
@@ -36,18 +37,39 @@ class MeshBatch:
         self.n_cells = int(self.cell_offsets[-1])
         self.n_boundary_faces = int(self.bnd_offsets[-1])
         self.n_faces = int(self.int_offsets[-1]) + self.n_boundary_faces
-        co = self.cell_offsets
-        own_i = [m.face_owner[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
-        own_b = [m.face_owner[fi[p]:].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
-        nb_i = [m.face_neighbor[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(meshes)]
-        self.face_owner = np.concatenate(own_i + own_b).astype(np.int32)
-        self.face_neighbor = np.concatenate(nb_i + [np.full(fb[p], -1, np.int64) for p in range(len(meshes))]).astype(
-            np.int32)
-        self.face_area = self.face_field([m.face_area for m in meshes])
-        self.face_center = self.face_field([m.face_center for m in meshes])
-        self.cell_center = np.ascontiguousarray(np.concatenate([m.cell_center for m in meshes]))
-        self.cell_volume = np.ascontiguousarray(np.concatenate([m.cell_volume for m in meshes]))
+        self._fi, self._fb = fi, fb
         self._device = {}
+
+    # union arrays on the host, built on first use (a union whose parts are
+    # resident on the GPU is joined there by fv_mesh_concat without them)
+    @functools.cached_property
+    def face_owner(self):
+        co, fi = self.cell_offsets, self._fi
+        own_i = [m.face_owner[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(self.meshes)]
+        own_b = [m.face_owner[fi[p]:].astype(np.int64) + co[p] for p, m in enumerate(self.meshes)]
+        return np.concatenate(own_i + own_b).astype(np.int32)
+
+    @functools.cached_property
+    def face_neighbor(self):
+        co, fi, fb = self.cell_offsets, self._fi, self._fb
+        nb_i = [m.face_neighbor[: fi[p]].astype(np.int64) + co[p] for p, m in enumerate(self.meshes)]
+        return np.concatenate(nb_i + [np.full(fb[p], -1, np.int64) for p in range(self.n_problems)]).astype(np.int32)
+
+    @functools.cached_property
+    def face_area(self):
+        return self.face_field([m.face_area for m in self.meshes])
+
+    @functools.cached_property
+    def face_center(self):
+        return self.face_field([m.face_center for m in self.meshes])
+
+    @functools.cached_property
+    def cell_center(self):
+        return np.ascontiguousarray(np.concatenate([m.cell_center for m in self.meshes]))
+
+    @functools.cached_property
+    def cell_volume(self):
+        return np.ascontiguousarray(np.concatenate([m.cell_volume for m in self.meshes]))
 
     def face_field(self, per_problem):
         """Concatenate per-problem face arrays into the union face order."""
@@ -68,7 +90,14 @@ class MeshBatch:
         from .mesh import DeviceMesh
         dev = torch.cuda.current_device()
         if dev not in self._device:
-            self._device[dev] = DeviceMesh(self, stream)
+            parts = [getattr(m, "_device", {}).get(dev) for m in self.meshes]
+            if all(p is not None and p.handle for p in parts):  # every part resident: join on the device
+                arr = (C.c_void_p * len(parts))(*[p.handle.value for p in parts])
+                h = C.c_void_p()
+                check(lib().fv_mesh_concat(arr, len(parts), stream_handle(stream), C.byref(h)), "fv_mesh_concat")
+                self._device[dev] = DeviceMesh.adopt(self, h)
+            else:
+                self._device[dev] = DeviceMesh(self, stream)
         return self._device[dev]
 
     def __del__(self):

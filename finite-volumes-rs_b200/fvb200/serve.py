@@ -21,6 +21,7 @@ import collections
 import dataclasses
 import threading
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -69,10 +70,13 @@ def request_stream(rate: float, duration: float, seed: int, mix_3d: float = 0.5,
 
 
 class MeshCache:
-    """Host meshes per (kind, side); geometry jitter seeded by the size."""
+    """Meshes per (kind, side), built on the GPU (faces, geometry and the
+    resident fv_mesh on the device; the host arrays read back); geometry
+    jitter seeded by the size.  A wave joins its meshes on the device."""
 
-    def __init__(self, fv, capacity_cells: int = 60_000_000):
+    def __init__(self, fv, capacity_cells: int = 60_000_000, on_device: bool = True):
         self.fv = fv
+        self.on_device = on_device
         self.cap = capacity_cells
         self.d = collections.OrderedDict()
         self.cells = 0
@@ -84,7 +88,8 @@ class MeshCache:
             if key in self.d:
                 self.d.move_to_end(key)
                 return self.d[key]
-        m = self.fv.Mesh.square(side, 0.2, 17 + side) if kind == "2d" else self.fv.Mesh.cube(side, 0.15, 17 + side)
+        m = (self.fv.Mesh.square(side, 0.2, 17 + side, on_device=self.on_device) if kind == "2d"
+             else self.fv.Mesh.cube(side, 0.15, 17 + side, on_device=self.on_device))
         with self.lock:
             self.d[key] = m
             self.cells += m.n_cells
@@ -114,14 +119,11 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
     import torch
     kind = reqs[0].kind
     with torch.cuda.stream(stream):
-        meshes, kfs, fls, scs = [], [], [], []
-        for r in reqs:
-            m = cache.get(r.kind, r.side)
-            kf, fl, sc = request_fields(m, r)
-            meshes.append(m)
-            kfs.append(kf)
-            fls.append(fl)
-            scs.append(sc)
+        meshes = [cache.get(r.kind, r.side) for r in reqs]
+        # per-request fields on host threads (the generator releases the GIL)
+        with ThreadPoolExecutor(max_workers=min(8, len(reqs))) as ex:
+            fields = list(ex.map(lambda mr: request_fields(*mr), zip(meshes, reqs)))
+        kfs, fls, scs = (list(x) for x in zip(*fields))
         mb = MeshBatch(meshes)
         kf = mb.face_field(kfs)
         sc = mb.cell_field(scs)

@@ -263,6 +263,12 @@ fv_status fv_mesh_build_faces(int32_t dim, int64_t n_nodes, const double *nodes,
  * Remote (ghost) faces or cells of a decomposed mesh: FV_ERR_UNSUPPORTED. */
 fv_status fv_mesh_build_msh(const char *path, int32_t dim, void *stream, fv_mesh **out,
                             fv_host_mesh **host_out);
+/* One resident mesh from n_parts resident meshes, laid out as a batch of
+ * independent problems (batched and served solves): the interior faces of every part in part order,
+ * then the boundary faces of every part; cells in part order.  Equal to
+ * fv_mesh_upload of the same union built on the host, without its host
+ * pass; no gradient data.  The parts stay owned by the caller. */
+fv_status fv_mesh_concat(const fv_mesh *const *parts, int32_t n_parts, void *stream, fv_mesh **out);
 /* The same from an SU2 file (the parser of fv_host_mesh_read_su2) and from the
  * synthetic generators (fv_host_mesh_generate_square / _cube). */
 fv_status fv_mesh_build_su2(const char *path, int32_t dim, void *stream, fv_mesh **out,

@@ -165,3 +165,37 @@ def test_batch_bicgstab_fp64_and_mixed(fv, orc):
         assert np.linalg.norm(a64[r0:r1] - xo) <= 1e-10 * np.linalg.norm(xo)
         assert om["final_residual"][k] <= 1e-10
         assert np.linalg.norm(am[r0:r1] - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+def test_union_of_resident_meshes_equals_host_union(fv):
+    """Parts already on the GPU are joined there (fv_mesh_concat): the same system as the host-built union."""
+    sides = [6, 9, 4, 13]
+    host = _problems(fv, sides, seed0=300)
+    dev = []
+    for k, s in enumerate(sides):
+        m = fv.Mesh.square(s, 0.2, 300 + k, on_device=True)
+        dev.append((m, host[k][1], host[k][2]))
+    mbh, Ah, bh = _union_system(fv, host)
+    mbd, Ad, bd = _union_system(fv, dev)
+    for x, y in zip(Ah.to_csr(), Ad.to_csr()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(bh.numpy(), bd.numpy())
+    Ph = fv.IncompleteCholesky.from_matrix(Ah, 0)
+    Pd = fv.IncompleteCholesky.from_matrix(Ad, 0)
+    for x, y in zip(Ph.factors()[:3], Pd.factors()[:3]):
+        assert np.array_equal(x, y)
+    # a 3D union mixing device-built and uploaded parts
+    cubes = [fv.Mesh.cube(3, 0.1, 5, on_device=True), fv.Mesh.cube(4, 0.1, 6)]
+    cubes[1].device()
+    from fvb200.batch import MeshBatch
+    mb = MeshBatch(cubes)
+    flux = mb.face_field([np.linspace(-1, 1, m.n_faces) for m in cubes])
+    kap = mb.face_field([np.full(m.n_faces, 0.3) for m in cubes])
+    nb = mb.n_boundary_faces
+    eq = fv.convection(fv.Upwind(flux), flux) - fv.laplacian(fv.Orthogonal(), kap)
+    A1, b1 = fv.assemble(eq, (np.zeros(nb), np.ones(nb)), mb)
+    mb2 = MeshBatch([fv.Mesh.cube(3, 0.1, 5), fv.Mesh.cube(4, 0.1, 6)])
+    A2, b2 = fv.assemble(eq, (np.zeros(nb), np.ones(nb)), mb2)
+    for x, y in zip(A1.to_csr(), A2.to_csr()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(b1.numpy(), b2.numpy())

@@ -40,6 +40,31 @@ def test_ic0_rejects_nonsymmetric(fv):
     assert e.value.status == FV_ERR_NOT_SYMMETRIC
 
 
+def test_symbolic_analysis_rejects_bad_patterns(fv):
+    """The reference indexes [[i, i]] and walks sorted rows: a row without its diagonal, or with
+    unsorted / repeated columns, is FV_ERR_INVALID; IC(0) of a structurally unsymmetric pattern is
+    FV_ERR_NOT_SYMMETRIC."""
+    from fvb200._lib import FV_ERR_INVALID, FV_ERR_NOT_SYMMETRIC, FvError
+    for name, (ptr, cols) in {"unsorted": ([0, 2, 4], [1, 0, 0, 1]), "repeated": ([0, 2, 4], [0, 0, 0, 1])}.items():
+        with pytest.raises(FvError) as e:  # refused when the matrix is created
+            fv.DistributedMatrix.from_csr(np.array(ptr, np.int32), np.array(cols, np.int32), np.ones(len(cols)))
+        assert e.value.status == FV_ERR_INVALID, name
+    A = fv.DistributedMatrix.from_csr(np.array([0, 2, 3], np.int32), np.array([0, 1, 0], np.int32), np.ones(3))
+    for cls in (fv.IncompleteLowerUpper, fv.IncompleteCholesky):
+        with pytest.raises(FvError) as e:  # no diagonal in row 1: refused by the symbolic analysis
+            cls.from_matrix(A, 0)
+        assert e.value.status == FV_ERR_INVALID
+    A = fv.DistributedMatrix.from_csr(np.array([0, 2, 3], np.int32), np.array([0, 1, 1], np.int32),
+                                      np.array([4.0, 1.0, 4.0]))
+    with pytest.raises(FvError) as e:
+        fv.IncompleteCholesky.from_matrix(A, 0)
+    assert e.value.status == FV_ERR_NOT_SYMMETRIC
+    P = fv.IncompleteLowerUpper.from_matrix(A, 0)  # ILU(0) takes it
+    z = fv.DistributedVector.from_size(2)
+    P.precondition(z, fv.DistributedVector(np.array([1.0, 2.0])))
+    assert np.allclose(z.numpy(), np.linalg.solve([[4.0, 1.0], [0.0, 4.0]], [1.0, 2.0]), rtol=1e-15)
+
+
 def test_one_cell_mesh(fv, orc):
     nodes = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
     bp = np.array([0, 2, 4, 6], np.int32)
