@@ -1283,6 +1283,82 @@ static int sweep_grid(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 2));
 }
 
+// DiagonalPreconditioner (preconditioners/mod.rs:38-68): dinv[i] = 1.0 / a_ii
+// (Inverse for f64, linalg/mod.rs:48-52); z_i = dinv_i * r_i.  A row without its
+// diagonal is an error (the reference indexes [[i, i]] and panics).
+namespace {
+__global__ void k_diag_inverse(int64_t n, const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                               const double *__restrict__ val, double *__restrict__ dinv, int *err) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = ptr[i], hi = ptr[i + 1];
+    while (lo < hi) {  // columns ascending
+        const int mid = (lo + hi) >> 1;
+        if (col[mid] < i)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo < ptr[i + 1] && col[lo] == i)
+        dinv[i] = 1.0 / val[lo];
+    else
+        atomicOr(err, FV_DEV_SINGULAR);
+}
+
+template <typename T>
+__global__ void k_diag_apply(int64_t n, const T *__restrict__ dinv, const T *__restrict__ r, T *__restrict__ z,
+                             const int *skip, fv_row_skip rs) {
+    if (skip && *(volatile const int *)skip) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (rs.group && rs.done[(int64_t)rs.group[i] * rs.stride]) continue;
+        z[i] = dinv[i] * r[i];
+    }
+}
+
+static fv_status diag_compute(fv_precond *P, cudaStream_t st) {
+    const int64_t n = P->n;
+    FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+    fv_note_launch(), k_diag_inverse<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, P->A->row_ptr, P->A->cols,
+                                                                                  P->A->vals, P->dinv, P->err);
+    FV_CUDA_TRY(cudaGetLastError());
+    int bad = 0;
+    FV_CUDA_TRY(cudaMemcpyAsync(&bad, P->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    if (bad) {
+        FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+        fv_internal_set_error_text("DiagonalPreconditioner: a row without its diagonal entry");
+        return FV_ERR_INVALID;
+    }
+    return FV_OK;
+}
+
+static int diag_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+}  // namespace
+
+extern "C" fv_status fv_diag_factor(const fv_csr *A, void *stream, fv_precond **out) {
+    if (!A || !out || A->nrows <= 0) return FV_ERR_INVALID;
+    *out = nullptr;
+    cudaStream_t st = fv_stream(stream);
+    fv_precond *P = new fv_precond();
+    P->kind = 3;
+    P->n = A->nrows;
+    P->A = A;
+    cudaError_t e = cudaMalloc(&P->dinv, sizeof(double) * P->n);
+    if (e == cudaSuccess) e = cudaMalloc(&P->err, sizeof(int));
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "fv_diag_factor");
+        fv_precond_destroy(P);
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    const fv_status s = diag_compute(P, st);
+    if (s != FV_OK) {
+        fv_precond_destroy(P);
+        return s;
+    }
+    *out = P;
+    return FV_OK;
+}
+
 // z = M^-1 r.  r must not alias z.  The forward sweep writes P->tmp and
 // pre-fills z with the sentinel; the backward sweep consumes tmp (resetting it
 // to the sentinel for the next apply) and writes z.
@@ -1290,8 +1366,13 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
                                const fv_row_skip *rskip) {
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
-    const int G = sweep_grid(n);
     const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
+    if (P->kind == 3) {
+        fv_note_launch(), k_diag_apply<double><<<diag_grid(n), 256, 0, st>>>(n, P->dinv, r, z, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
+    const int G = sweep_grid(n);
     if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1334,6 +1415,13 @@ __global__ void k_to_f32(int64_t n, const double *__restrict__ a, float *__restr
 fv_status fv_precond_make_f32(fv_precond *P, cudaStream_t st) {
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
+    if (P->kind == 3) {
+        if (!P->dinv32) FV_CUDA_TRY(cudaMalloc(&P->dinv32, sizeof(float) * n));
+        fv_note_launch(), k_to_f32<<<148 * 8, 256, 0, st>>>(n, P->dinv, P->dinv32);
+        FV_CUDA_TRY(cudaGetLastError());
+        P->f32_version += 1;
+        return FV_OK;
+    }
     if (!P->l32) {
         FV_CUDA_TRY(cudaMalloc(&P->l32, sizeof(float) * (s->nnz_l ? s->nnz_l : 1)));
         FV_CUDA_TRY(cudaMalloc(&P->u32, sizeof(float) * (s->nnz_u ? s->nnz_u : 1)));
@@ -1355,9 +1443,15 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
                                    const fv_row_skip *rskip) {
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
+    const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
+    if (P->kind == 3) {
+        if (!P->dinv32) return FV_ERR_INVALID;
+        fv_note_launch(), k_diag_apply<float><<<diag_grid(n), 256, 0, st>>>(n, P->dinv32, r, z, skip, rs);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (!P->l32) return FV_ERR_INVALID;
     const int G = sweep_grid(n);
-    const fv_row_skip rs = rskip ? *rskip : fv_row_skip{};
     if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1375,6 +1469,11 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
 
 extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
     if (!P || request < -1 || request > 3) return FV_ERR_INVALID;
+    if (P->kind == 3) {  // no sweeps to schedule
+        if (active) *active = 1;
+        if (stats) std::fill(stats, stats + 6, 0.0);
+        return FV_OK;
+    }
     fv_symbolic *s = P->sym;
     if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
     if (request == 2 && !s->tiled) return FV_ERR_UNSUPPORTED;
@@ -1656,6 +1755,7 @@ extern "C" fv_status fv_precond_refactor(fv_precond *P, void *stream) {
     if (!P) return FV_ERR_INVALID;
     fv_precond *q = P;
     cudaStream_t st = fv_stream(stream);
+    if (P->kind == 3) return diag_compute(P, st);
     if (P->fill) {  // level k: new values of the original matrix into the fill pattern
         if (P->kind == 1) FV_TRY(check_symmetric(const_cast<fv_csr *>(P->orig), st));
         FV_TRY(scatter_fill(P, st));
@@ -1692,6 +1792,15 @@ extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_
     const fv_symbolic *s = P->sym;
     const int64_t n = P->n;
     if (n_dropped) *n_dropped = (int32_t)P->n_dropped;
+    if (P->kind == 3) {  // the reference's `diagonal`: 1 / a_ii on the diagonal
+        *nnz = n;
+        if (!row_ptr || !cols || !vals) return FV_OK;
+        FV_CUDA_TRY(cudaMemcpyAsync(vals, P->dinv, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int64_t i = 0; i <= n; ++i) row_ptr[i] = (int32_t)i;
+        for (int64_t i = 0; i < n; ++i) cols[i] = (int32_t)i;
+        return FV_OK;
+    }
     // IC: the reference's `l` (lower incl. diagonal); ILU: the reference's `lu` (dropped entries removed)
     const int64_t total = P->kind == 1 ? s->nnz_l + n : s->nnz_l + s->nnz_u + n - P->n_dropped;
     if (!row_ptr || !cols || !vals) {
@@ -1738,6 +1847,7 @@ extern "C" fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, 
                                        int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream) {
     if (!P) return FV_ERR_INVALID;
     fv_symbolic *s = P->sym;
+    if (!s) return FV_ERR_UNSUPPORTED;  // the diagonal preconditioner has no sweeps
     if (fwd_level || bwd_level) FV_TRY(ensure_host_levels(s, fv_stream(stream)));
     if (fwd_level) std::copy(s->h_fwd_level.begin(), s->h_fwd_level.end(), fwd_level);
     if (bwd_level) std::copy(s->h_bwd_level.begin(), s->h_bwd_level.end(), bwd_level);

@@ -3,12 +3,13 @@ hot path, behind the C ABI of include/fv_b200.h.
 
 The names mirror the reference crate (fvm::assembly::assemble,
 linalg::{DistributedMatrix, DistributedVector}, preconditioners::{
-IncompleteCholesky, IncompleteLowerUpper}, solvers::{conjugate_gradient,
+IncompleteCholesky, IncompleteLowerUpper, DiagonalPreconditioner}, solvers::{conjugate_gradient,
 bi_conjugate_gradient_stab, LinearSolverOptions, LinearSolverInfo}).
 """
 from ._lib import FvError, lib  # noqa: F401
 from .linalg import (  # noqa: F401
-    DistributedMatrix, DistributedVector, IdentityPreconditioner, IncompleteCholesky, IncompleteLowerUpper,
+    DiagonalPreconditioner, DistributedMatrix, DistributedVector, IdentityPreconditioner, IncompleteCholesky,
+    IncompleteLowerUpper,
     LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, compute_gradients,
     conjugate_gradient,
 )

@@ -139,6 +139,7 @@ _SIGS = {
     "fv_spmv_host": [vp, dp, dp, vp],
     "fv_ic0_factor": [vp, vp, P(vp)],
     "fv_ilu0_factor": [vp, vp, P(vp)],
+    "fv_diag_factor": [vp, vp, P(vp)],
     "fv_ic_factor": [vp, C.c_int32, vp, P(vp)],
     "fv_ilu_factor": [vp, C.c_int32, vp, P(vp)],
     "fv_precond_refactor": [vp, vp],

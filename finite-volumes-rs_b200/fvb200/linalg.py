@@ -329,6 +329,19 @@ class IncompleteLowerUpper(Preconditioner):
         return cls(h, matrix.nrows(), matrix)
 
 
+class DiagonalPreconditioner(Preconditioner):
+    """DiagonalPreconditioner (preconditioners/mod.rs:38-68): z = r / diag(A)."""
+
+    def __init__(self, handle, n, matrix):
+        self.handle, self.n, self._m = handle, n, matrix
+
+    @classmethod
+    def from_matrix(cls, matrix: DistributedMatrix, stream=None) -> "DiagonalPreconditioner":
+        h = C.c_void_p()
+        check(lib().fv_diag_factor(matrix.handle, stream_handle(stream), C.byref(h)), "DiagonalPreconditioner")
+        return cls(h, matrix.nrows(), matrix)
+
+
 class IdentityPreconditioner(Preconditioner):
     handle = C.c_void_p()
 

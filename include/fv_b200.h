@@ -311,6 +311,12 @@ fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double *y_host, vo
 /* IncompleteCholesky::from_matrix(A, 0) / IncompleteLowerUpper::from_matrix(A, 0). */
 fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out);
 fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out);
+/* DiagonalPreconditioner::from_matrix(A) (preconditioners/mod.rs:38-68):
+ * z_i = (1 / a_ii) r_i.  A row without its diagonal: FV_ERR_INVALID (the
+ * reference panics).  Usable wherever an fv_precond is taken (solvers,
+ * batched and distributed solves, fv_precond_apply / _refactor / _export);
+ * fv_precond_levels answers FV_ERR_UNSUPPORTED (no sweeps). */
+fv_status fv_diag_factor(const fv_csr *A, void *stream, fv_precond **out);
 /* IncompleteCholesky / IncompleteLowerUpper ::from_matrix(A, level) for any
  * level (incomplete_cholesky.rs:35-85,148-205; incomplete_lower_upper.rs:
  * 30-137,200-266): the reference's level-k patterns (depth-first walks over

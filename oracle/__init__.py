@@ -61,6 +61,7 @@ def lib():
             "or_fill_pattern": ([C.c_int, C.c_int, i64, ip, ip, ip, ip, P(C.c_ubyte)], i64),
             "or_ilu0_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
             "or_precond_apply": ([vp, dp, dp], None),
+            "or_diag_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
             "or_precond_free": ([vp], None),
             "or_precond_nnz": ([vp], i64),
             "or_precond_ndropped": ([vp], i64),
@@ -248,7 +249,7 @@ def fill_pattern(kind, level, ptr, cols):
 
 
 class Precond:
-    """IncompleteCholesky / IncompleteLowerUpper restated.  level >= 1: the
+    """IncompleteCholesky / IncompleteLowerUpper / DiagonalPreconditioner ("diag") restated.  level >= 1: the
     level-0 numerics on the level-k pattern with zeros at fill positions (IC
     sums a row's fill entries after its matrix entries in the backward sweep,
     as the reference's sp_t does)."""
@@ -267,7 +268,10 @@ class Precond:
                 fv_[pos] = vals_[a0:a1]
             ptr, cols, vals = fptr, fcol, fv_
         self._keep = (_i(ptr), _i(cols), _d(vals), fill)
-        if kind == "ic":
+        if kind == "diag":
+            self.h = lib().or_diag_create(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]),
+                                          C.byref(st))
+        elif kind == "ic":
             fl = fill.ctypes.data_as(P(C.c_ubyte)) if fill is not None else None
             self.h = lib().or_ic_create_fill(self.n, _pi(self._keep[0]), _pi(self._keep[1]), _pd(self._keep[2]),
                                              fl, C.byref(st))

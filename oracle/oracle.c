@@ -562,7 +562,7 @@ double or_dot(int64_t n, const double *a, const double *b) {
 
 /* ---------------------------------------------------------- preconditioners */
 typedef struct {
-    int kind;    /* 1 = IC, 2 = ILU */
+    int kind;    /* 1 = IC, 2 = ILU, 3 = diagonal */
     int64_t n;
     /* IC: l (lower incl. diag), sp_t (upper pattern), l_vt, inv_diag */
     csr_t l;
@@ -789,10 +789,35 @@ or_precond *or_ilu0_create(int64_t n, const int32_t *ptr, const int32_t *col, co
     return p;
 }
 
+/* DiagonalPreconditioner::from_matrix (preconditioners/mod.rs:44-60):
+ * diagonal[i] = matrix[[i, i]].inverse() = 1.0 / a_ii (linalg/mod.rs:48-52);
+ * NULL with *status = 1 when a row has no diagonal (the reference panics). */
+or_precond *or_diag_create(int64_t n, const int32_t *ptr, const int32_t *col, const double *val, int *status) {
+    *status = 0;
+    or_precond *p = (or_precond *)calloc(1, sizeof(or_precond));
+    p->kind = 3;
+    p->n = n;
+    p->inv_diag = (double *)malloc(sizeof(double) * (n ? n : 1));
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t k = csr_find(ptr, col, i, (int32_t)i);
+        if (k < 0) {
+            *status = 1;
+            or_precond_free(p);
+            return NULL;
+        }
+        p->inv_diag[i] = 1.0 / val[k];
+    }
+    return p;
+}
+
 /* Preconditioner::precondition: IC (incomplete_cholesky.rs:217-255),
- * ILU (incomplete_lower_upper.rs:287-329). */
+ * ILU (incomplete_lower_upper.rs:287-329), diagonal (preconditioners/mod.rs:63-67). */
 void or_precond_apply(const or_precond *p, const double *rhs, double *sol) {
     const int64_t n = p->n;
+    if (p->kind == 3) {
+        for (int64_t i = 0; i < n; ++i) sol[i] = p->inv_diag[i] * rhs[i];
+        return;
+    }
     if (p->kind == 1) {
         for (int64_t i = 0; i < n; ++i) {
             double si = rhs[i];

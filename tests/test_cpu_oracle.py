@@ -264,3 +264,15 @@ def test_host_builder_rejects_bad_node_ids(fv):
         with pytest.raises(FvError) as ei:
             fv.Mesh.from_elements(2, nodes, kinds, eptr, en, bptr, bn, bm)
         assert "FV_ERR_INVALID" in str(ei.value)
+
+
+def test_oracle_diagonal_preconditioner(fv, orc):
+    """DiagonalPreconditioner restated: z = (1 / a_ii) r; a missing diagonal is refused."""
+    case = diffusion_2d(fv, 6, seed=4)
+    ptr, cols, vals, _ = oracle_system(orc, case)
+    A = sp.csr_matrix((vals, cols, ptr))
+    r = np.random.default_rng(1).standard_normal(A.shape[0])
+    z = orc.Precond("diag", ptr, cols, vals).apply(r)
+    assert np.array_equal(z, (1.0 / A.diagonal()) * r)
+    bad = orc.Precond("diag", np.array([0, 2, 3]), np.array([0, 1, 0]), np.ones(3))
+    assert not bad.ok() and bad.status == 1
