@@ -165,8 +165,8 @@ class Server:
     """solve_fn(fv, cache, wave, stream) solves a wave in place (default: solve_wave);
     it is a parameter so the scheduling can be exercised without a GPU."""
 
-    def __init__(self, fv, workers: int = 3, budget_bytes: int | None = None, max_wave_cells: int = 16_000_000,
-                 max_wave_requests: int = 256, solve_fn=None, make_stream=None):
+    def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
+                 max_wave_requests: int = 512, solve_fn=None, make_stream=None):
         self.fv = fv
         self.cache = MeshCache(fv)
         self.workers = workers
