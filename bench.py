@@ -680,9 +680,13 @@ def serve_arm(args, rank, world, local_rank):
     stats = srv.run(reqs, time_limit=args.serve_time_limit)
     launches = lib().fv_launch_count() - L0
     clocks = clk.stop()
-    # plain FP64 per-request path on a sample of the same requests
-    rng = np.random.default_rng(5)
-    sample = [reqs[i] for i in rng.choice(len(reqs), size=min(args.plain_sample, len(reqs)), replace=False)]
+    # plain FP64 per-request path on a sample of the same requests, stratified by
+    # size: per kind, the requests at evenly spaced quantiles of the cell count
+    sample = []
+    for kind in ("2d", "3d"):
+        rk = sorted((r for r in reqs if r.kind == kind), key=lambda r: r.cells)
+        m = min(max(1, args.plain_sample // 2), len(rk))
+        sample += [rk[int((j + 0.5) * len(rk) / m)] for j in range(m)] if rk else []
     plain = []
     for r in sample:
         m = srv.cache.get(r.kind, r.side)
@@ -723,6 +727,7 @@ def serve_arm(args, rank, world, local_rank):
         "completed": stats["completed"], "waves": stats["waves"], "cells_per_s": round(stats["cells_per_s"], 1),
         "max_final_residual": stats["max_residual"],
         "plain_fp64_solves_per_s": round(plain_rate, 3),
+        "plain_sample": f"{len(sample)} requests at evenly spaced size quantiles per kind, one at a time, rtol 1e-8",
         "speedup_vs_plain_fp64": round(stats["solves_per_s"] / plain_rate, 2) if plain_rate > 0 else None,
         "gpu_launches": int(launches), "clocks": clocks, "mesh_build_s": round(t_mesh, 1),
     }
