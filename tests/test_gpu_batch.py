@@ -199,3 +199,34 @@ def test_union_of_resident_meshes_equals_host_union(fv):
     for x, y in zip(A1.to_csr(), A2.to_csr()):
         assert np.array_equal(x, y)
     assert np.array_equal(b1.numpy(), b2.numpy())
+
+
+def test_batch_with_diagonal_preconditioner(fv, orc):
+    """DiagonalPreconditioner in the batched CG (FP64 and mixed): per problem against the oracle's
+    plain CG with the same preconditioner (<=1e-10 rel, iterations +-2 in FP64), same alone and in a mix."""
+    from fvb200.batch import BatchCG
+    probs = _problems(fv, [7, 11, 5], seed0=500)
+    mb, A, b = _union_system(fv, probs)
+    P = fv.DiagonalPreconditioner.from_matrix(A)
+    x = fv.DistributedVector.from_size(mb.n_cells)
+    out = BatchCG(A, mb.cell_offsets, 256).solve(P, b, x, precision="fp64", relative_tolerance=1e-10,
+                                                 absolute_tolerance=1e-10, max_iterations=5000)
+    xs = x.numpy()
+    for k, (m, kf, sc) in enumerate(probs):
+        nb = m.n_boundary_faces
+        ptr, cols, vals, rhs = orc.assemble(m, -1.0, 0.0, -1.0, kappa=kf, source=sc, bndi=np.zeros(nb),
+                                            bnde=np.zeros(nb))
+        xo, io = orc.cg(ptr, cols, vals, orc.Precond("diag", ptr, cols, vals), rhs, rtol=1e-10, atol=1e-10,
+                        maxit=5000)
+        r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+        assert abs(int(out["iterations"][k]) - io["iterations"]) <= 2
+        assert np.linalg.norm(xs[r0:r1] - xo) <= 1e-10 * np.linalg.norm(xo)
+    x2 = fv.DistributedVector.from_size(mb.n_cells)
+    o2 = BatchCG(A, mb.cell_offsets, 256).solve(P, b, x2, precision="mixed", outer_tolerance=1e-10)
+    assert max(o2["final_residual"]) <= 1e-10
+    mb1, A1, b1 = _union_system(fv, [probs[1]])
+    P1 = fv.DiagonalPreconditioner.from_matrix(A1)
+    x1 = fv.DistributedVector.from_size(mb1.n_cells)
+    o1 = BatchCG(A1, mb1.cell_offsets, 256).solve(P1, b1, x1, precision="mixed", outer_tolerance=1e-10)
+    r0, r1 = mb.cell_offsets[1], mb.cell_offsets[2]
+    assert np.array_equal(x1.numpy(), x2.numpy()[r0:r1]) and int(o1["iterations"][0]) == int(o2["iterations"][1])
