@@ -50,6 +50,11 @@ WORKLOADS = {
     "batch1024_diffusion": dict(kind="batch"),
     # BASELINE served configuration (Poisson stream, continuous batching)
     "serve_mixed": dict(kind="serve"),
+    # the time loop of the crate's examples on the config-1 mesh: implicit Euler,
+    # per step value-only re-assembly, ILU(0) refactorisation, BiCGStab from
+    # the previous solution
+    "cube128_transient": dict(kind="transient", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
+                              dt=2e-3),
 }
 RTOL = 1e-8
 
@@ -489,6 +494,90 @@ def config_of(args, wl, N, nnz):
             "parallelism": f"replicas x{args.gpus}"}
 
 
+def transient_arm(args, rank, world, local_rank):
+    """Implicit-Euler time loop on the config-1 problem (what every example of
+    the crate runs): time(Euler(u, dt)) + convection(Upwind(F), F)
+    - laplacian(Orthogonal, kappa) - source(f), u0 = 0.  One step = value-only
+    re-assembly into the resident pattern, ILU(0) refactorisation, BiCGStab to
+    rtol 1e-8 from the previous solution.  Metric: time steps per second."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    from fvb200.build import build
+    build()
+    import fvb200 as fv
+    from fvb200._lib import lib
+    wl = WORKLOADS[args.workload]
+    prob = make_problem(fv, dict(wl, kind="3d"), seed=1000 + rank, on_device=True)
+    mesh = prob["mesh"]
+    dev = torch.device("cuda", local_rank)
+    T = {k: torch.as_tensor(prob[k], device=dev) for k in ("kappa", "flux", "source", "bndi", "bnde")}
+    bc = (T["bndi"], T["bnde"])
+    N = mesh.n_cells
+    u = torch.zeros(N, dtype=torch.float64, device=dev)
+    opts = fv.LinearSolverOptions(RTOL, RTOL, 10000)
+    stream = torch.cuda.current_stream()
+    A = P = None
+
+    def step():
+        nonlocal A, P, u
+        eq = (fv.time(fv.Euler(u, wl["dt"])) + fv.convection(fv.Upwind(T["flux"]), T["flux"])
+              - fv.laplacian(fv.Orthogonal(), T["kappa"]) - fv.source(T["source"]))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        if A is None:
+            A, b = fv.assemble(eq, bc, mesh)
+            ev[1].record(stream)
+            P = fv.IncompleteLowerUpper.from_matrix(A, 0)
+        else:
+            _, b = fv.assemble(eq, bc, mesh, lhs=A)
+            ev[1].record(stream)
+            P.refactor()
+        ev[2].record(stream)
+        x = fv.DistributedVector(u.clone())
+        info = fv.bi_conjugate_gradient_stab(x, A, b, P, None, opts)
+        ev[3].record(stream)
+        u = x.data
+        return info.iterations, ev
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clk = Clocks(local_rank)
+    clk.start()
+    L0 = lib().fv_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    its, phases = [], []
+    for _ in range(args.steps):
+        n_it, ev = step()
+        its.append(int(n_it))
+        phases.append(ev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = lib().fv_launch_count() - L0
+    elapsed = e0.elapsed_time(e1) / 1e3
+    ph = [[round(ev[0].elapsed_time(ev[1]), 2), round(ev[1].elapsed_time(ev[2]), 2), round(ev[2].elapsed_time(ev[3]), 2)]
+          for ev in phases]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    line = {
+        "metric": "implicit-Euler time steps/s (re-assembly + ILU(0) refactorisation + BiCGStab to rtol 1e-8)",
+        "value": round(args.steps * world / elapsed, 4), "unit": "time steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "cells": N, "dt": wl["dt"], "solver": "bicgstab+ilu0",
+                   "rtol": RTOL, "parallelism": f"replicas x{world}"},
+        "iterations": its, "step_phase_ms": ph, "phase_names": ["assemble", "refactor", "solve"],
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def batch_problems(fv, count, seed, rank):
     """BASELINE batched configuration: `count` 2D diffusion problems built as the
     256x256 case, sides log-uniform in [32, 512], per-problem sigma ~ U(0.5, 2),
@@ -807,8 +896,9 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    if WORKLOADS[args.workload]["kind"] in ("batch", "serve"):
-        (main_batch if WORKLOADS[args.workload]["kind"] == "batch" else serve_arm)(args, rank, world, local_rank)
+    if WORKLOADS[args.workload]["kind"] in ("batch", "serve", "transient"):
+        kind = WORKLOADS[args.workload]["kind"]
+        {"batch": main_batch, "serve": serve_arm, "transient": transient_arm}[kind](args, rank, world, local_rank)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
