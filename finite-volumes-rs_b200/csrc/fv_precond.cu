@@ -428,6 +428,116 @@ __global__ void __launch_bounds__(128) k_ilu0(int64_t n, const int32_t *__restri
     leave(&ctrl[0], &ctrl[1]);
 }
 
+// k_ilu0 for short rows (at most MAXR entries: tetrahedra, triangles): the
+// same arithmetic in the same order, with the loads rearranged so that one
+// level costs about one flag round trip: the row bounds of every U_k are
+// read before waiting, all flags are polled together, and then diag[k] and
+// every u_kj are loaded at once into registers before the elimination runs.
+template <int MAXR>
+__global__ void __launch_bounds__(128) k_ilu0s(int64_t n, const int32_t *__restrict__ order,
+                                               const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
+                                               const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
+                                               const int32_t *__restrict__ u_ptr, const int32_t *__restrict__ u_col,
+                                               double *l_val, double *u_val, double *diag, double *dinv,
+                                               unsigned *done, unsigned epoch, unsigned *ctrl, int *err) {
+    constexpr int MU = MAXR - 1;  // a strict-upper row holds at most MAXR - 1 entries
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int i = __ldg(&order[idx]);
+        const int l0 = __ldg(&l_ptr[i]), nl = __ldg(&l_ptr[i + 1]) - l0;
+        const int u0 = __ldg(&u_ptr[i]), nu = __ldg(&u_ptr[i + 1]) - u0;
+        const int m = nl + 1 + nu;
+        const int a0 = __ldg(&a_ptr[i]);
+        int c[MAXR];
+        double v[MAXR];
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+            if (q < m) {
+                v[q] = a_val[a0 + q];
+                c[q] = q < nl ? __ldg(&l_col[l0 + q]) : (q == nl ? i : __ldg(&u_col[u0 + q - nl - 1]));
+            }
+        // static parts of the rows k the elimination reads
+        int ub[MAXR], ul[MAXR], ucol[MAXR][MU];
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+            if (q < nl) {
+                ub[q] = __ldg(&u_ptr[c[q]]);
+                ul[q] = __ldg(&u_ptr[c[q] + 1]) - ub[q];
+            }
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+#pragma unroll
+            for (int t = 0; t < MU; ++t)
+                if (q < nl && t < ul[q]) ucol[q][t] = __ldg(&u_col[ub[q] + t]);
+        // every dependency's flag, polled together (bounded)
+        unsigned pending = 0;
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+            if (q < nl && fv_ld_acquire_u32(&done[c[q]]) != epoch) pending |= 1u << q;
+        if (pending) {
+            const unsigned long long t0 = fv_globaltimer();
+            for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                for (int q = 0; q < MAXR; ++q)
+                    if (((pending >> q) & 1u) && fv_ld_acquire_u32(&done[c[q]]) == epoch) pending &= ~(1u << q);
+                if (pending && (it & 255u) == 0 &&
+                    (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS)) {
+                    if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+                    pending = 0;
+                }
+            }
+        }
+        // the factored values of those rows, loaded together
+        double dk[MAXR], uv[MAXR][MU];
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+            if (q < nl) dk[q] = __ldcg(&diag[c[q]]);
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+#pragma unroll
+            for (int t = 0; t < MU; ++t)
+                if (q < nl && t < ul[q]) uv[q][t] = __ldcg(&u_val[ub[q] + t]);
+        // elimination in the order of k_ilu0
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q) {
+            if (q < nl) {
+                const double lukk = dk[q];
+                if (fabs(lukk) < 1e-16) atomicOr(err, FV_DEV_SINGULAR);
+                const double lukkinv = 1.0 / lukk;
+                v[q] = lukkinv * v[q];
+                const double lik = v[q];
+#pragma unroll
+                for (int t = 0; t < MU; ++t) {
+                    if (t < ul[q]) {
+                        const int j = ucol[q][t];
+                        const double term = lik * uv[q][t];
+#pragma unroll
+                        for (int p = q + 1; p < MAXR; ++p)
+                            if (p < m && c[p] == j) v[p] -= term;
+                    }
+                }
+            }
+        }
+        const double tol = fabs(v[nl]) * 1e-6;
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q)
+            if (q < m && q != nl && !(fabs(v[q]) > tol)) v[q] = 0.0;
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q) {
+            if (q < nl) l_val[l0 + q] = v[q];
+            if (q > nl && q < m) u_val[u0 + q - nl - 1] = v[q];
+        }
+        diag[i] = v[nl];
+        dinv[i] = 1.0 / v[nl];
+        __threadfence();
+        fv_st_release_u32(&done[i], epoch);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
 // IC(0) numeric, up-looking form of the reference's right-looking loop
 // (incomplete_cholesky.rs:87-135): every l_ij receives the same updates
 // l_ik*l_jk in ascending k and the same final scaling by 1/l_jj.
@@ -1585,7 +1695,11 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
     fv_note_launch(), k_ilu0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->u_ptr, \
                                   sym->u_col, P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch,        \
                                   P->ctrl + 4, P->err)
-        if (mr <= 8)
+        if (mr <= 6)
+            fv_note_launch(), k_ilu0s<6><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr,
+                                                             sym->l_col, sym->u_ptr, sym->u_col, P->l_val, P->u_val,
+                                                             P->diag, P->dinv, P->done, P->epoch, P->ctrl + 4, P->err);
+        else if (mr <= 8)
             FV_ILU(8);
         else if (mr <= 16)
             FV_ILU(16);
