@@ -590,6 +590,107 @@ __global__ void __launch_bounds__(128) k_ic0(int64_t n, const int32_t *__restric
     leave(&ctrl[0], &ctrl[1]);
 }
 
+// k_ic0 for short rows, rearranged like k_ilu0s: row j's lower bounds and
+// columns before the wait, all flags polled together, dinv[j] and row j's
+// lower values loaded at once; the arithmetic and its order are k_ic0's.
+template <int MAXR>
+__global__ void __launch_bounds__(128) k_ic0s(int64_t n, const int32_t *__restrict__ order,
+                                              const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
+                                              const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
+                                              const int32_t *__restrict__ l_tpos, double *l_val, double *u_val,
+                                              double *diag, double *dinv, unsigned *done, unsigned epoch,
+                                              unsigned *ctrl, int *err) {
+    constexpr int ML = MAXR - 1;  // a strict-lower row holds at most MAXR - 1 entries
+    const int64_t nchunks = (n + 31) / 32;
+    int64_t chunk;
+    while (take_chunk(&ctrl[0], nchunks, chunk)) {
+        const int64_t idx = chunk * 32 + (threadIdx.x & 31);
+        if (idx >= n) continue;
+        const int i = __ldg(&order[idx]);
+        const int l0 = __ldg(&l_ptr[i]), nl = __ldg(&l_ptr[i + 1]) - l0;
+        const int a0 = __ldg(&a_ptr[i]);
+        int c[ML];
+        double v[ML];
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl) {
+                c[q] = __ldg(&l_col[l0 + q]);
+                v[q] = a_val[a0 + q];
+            }
+        double vd = a_val[a0 + nl];
+        int lb[ML], ln[ML], lc[ML][ML];
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl) {
+                lb[q] = __ldg(&l_ptr[c[q]]);
+                ln[q] = __ldg(&l_ptr[c[q] + 1]) - lb[q];
+            }
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+#pragma unroll
+            for (int t = 0; t < ML; ++t)
+                if (q < nl && t < ln[q]) lc[q][t] = __ldg(&l_col[lb[q] + t]);
+        unsigned pending = 0;
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl && fv_ld_acquire_u32(&done[c[q]]) != epoch) pending |= 1u << q;
+        if (pending) {
+            const unsigned long long t0 = fv_globaltimer();
+            for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                for (int q = 0; q < ML; ++q)
+                    if (((pending >> q) & 1u) && fv_ld_acquire_u32(&done[c[q]]) == epoch) pending &= ~(1u << q);
+                if (pending && (it & 255u) == 0 &&
+                    (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS)) {
+                    if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+                    pending = 0;
+                }
+            }
+        }
+        double dj[ML], lv[ML][ML];
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl) dj[q] = __ldcg(&dinv[c[q]]);
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+#pragma unroll
+            for (int t = 0; t < ML; ++t)
+                if (q < nl && t < ln[q]) lv[q][t] = __ldcg(&l_val[lb[q] + t]);
+        // k_ic0's merge: for each dependency j (ascending) the row's own k < j
+        // against row j's lower part, ascending k
+#pragma unroll
+        for (int q = 0; q < ML; ++q) {
+            if (q < nl) {
+#pragma unroll
+                for (int t = 0; t < ML; ++t) {
+                    if (t < ln[q]) {
+                        const int k = lc[q][t];
+#pragma unroll
+                        for (int p = 0; p < ML; ++p)
+                            if (p < q && c[p] == k) v[q] -= v[p] * lv[q][t];
+                    }
+                }
+                v[q] = dj[q] * v[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl) vd -= v[q] * v[q];
+        const double lii = sqrt(vd);
+#pragma unroll
+        for (int q = 0; q < ML; ++q)
+            if (q < nl) {
+                l_val[l0 + q] = v[q];
+                u_val[__ldg(&l_tpos[l0 + q])] = v[q];
+            }
+        diag[i] = lii;
+        dinv[i] = 1.0 / lii;
+        __threadfence();
+        fv_st_release_u32(&done[i], epoch);
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
 // |a_ij - a_ji| < 1e-14 for every stored pair (is_symmetric, dmatrix.rs:76-88)
 __global__ void k_check_symmetric(int64_t n, const int32_t *__restrict__ a_ptr, const double *__restrict__ a_val,
                                   const int32_t *__restrict__ l_ptr, const int32_t *__restrict__ l_col,
@@ -1257,13 +1358,9 @@ static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symb
     unsigned *ctrl = nullptr;
     int32_t *cnt = nullptr, *keys = nullptr, *iota = nullptr;
     void *tmp = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(dw);
-        cudaFree(ctrl);
-        cudaFree(cnt);
-        cudaFree(keys);
-        cudaFree(iota);
-        cudaFree(tmp);
+    auto cleanup = [&]() {  // scratch from the stream-ordered pool: no device-wide synchronisation
+        for (void *q : {(void *)dw, (void *)ctrl, (void *)cnt, (void *)keys, (void *)iota, tmp})
+            if (q) cudaFreeAsync(q, st);
     };
     auto fail = [&](cudaError_t e, const char *what) {
         fv_internal_set_cuda_error(e, what);
@@ -1276,9 +1373,9 @@ static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symb
         fv_symbolic_free(s);
         return code;
     };
-    cudaError_t e = cudaMalloc(&dw, sizeof(int) * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&ctrl, sizeof(unsigned) * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&cnt, sizeof(int32_t) * 2 * (n + 1));
+    cudaError_t e = fv_malloc_async(&dw, sizeof(int) * 8, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&ctrl, sizeof(unsigned) * 4, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&cnt, sizeof(int32_t) * 2 * (n + 1), st);
     if (e == cudaSuccess) e = cudaMalloc(&s->l_ptr, sizeof(int32_t) * (n + 1));
     if (e == cudaSuccess) e = cudaMalloc(&s->u_ptr, sizeof(int32_t) * (n + 1));
     if (e == cudaSuccess) e = cudaMemsetAsync(dw, 0, sizeof(int) * 8, st);
@@ -1295,7 +1392,7 @@ static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symb
         e = cub::DeviceRadixSort::SortPairs(nullptr, tb2, (const uint32_t *)nullptr, (uint32_t *)nullptr,
                                             (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, 32, st);
     tb = std::max(tb, tb2);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+    if (e == cudaSuccess) e = fv_malloc_async(&tmp, tb, st);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, s->l_ptr, (int)(n + 1), st);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt + (n + 1), s->u_ptr, (int)(n + 1), st);
     int h[8] = {0};
@@ -1317,8 +1414,8 @@ static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symb
     if (e == cudaSuccess) e = cudaMalloc(&s->d_bwd_level, sizeof(int32_t) * n);
     if (e == cudaSuccess) e = cudaMalloc(&s->fwd_order, sizeof(int32_t) * n);
     if (e == cudaSuccess) e = cudaMalloc(&s->bwd_order, sizeof(int32_t) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&keys, sizeof(int32_t) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&iota, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = fv_malloc_async(&keys, sizeof(int32_t) * n, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&iota, sizeof(int32_t) * n, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_fwd_level, 0xFF, sizeof(int32_t) * n, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_bwd_level, 0xFF, sizeof(int32_t) * n, st);
     if (e == cudaSuccess) {
@@ -1351,10 +1448,10 @@ static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symb
         e = cub::DeviceRadixSort::SortPairs(nullptr, need, (const uint32_t *)nullptr, (uint32_t *)nullptr,
                                             (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, bits, st);
         if (e == cudaSuccess && need > tb) {
-            cudaFree(tmp);
+            cudaFreeAsync(tmp, st);
             tmp = nullptr;
             tb = need;
-            e = cudaMalloc(&tmp, tb);
+            e = fv_malloc_async(&tmp, tb, st);
         }
         if (e != cudaSuccess) break;
         e = cub::DeviceRadixSort::SortPairs(tmp, tb, (const uint32_t *)(d == 0 ? s->d_fwd_level : s->d_bwd_level),
@@ -1710,7 +1807,11 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
 #define FV_IC(MR)                                                                                             \
     fv_note_launch(), k_ic0<MR><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr, sym->l_col, sym->l_tpos, \
                                  P->l_val, P->u_val, P->diag, P->dinv, P->done, P->epoch, P->ctrl + 4, P->err)
-        if (mr <= 8)
+        if (mr <= 6)
+            fv_note_launch(), k_ic0s<6><<<G, 128, 0, st>>>(n, sym->fwd_order, A->row_ptr, A->vals, sym->l_ptr,
+                                                            sym->l_col, sym->l_tpos, P->l_val, P->u_val, P->diag,
+                                                            P->dinv, P->done, P->epoch, P->ctrl + 4, P->err);
+        else if (mr <= 8)
             FV_IC(8);
         else if (mr <= 16)
             FV_IC(16);
