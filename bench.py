@@ -23,6 +23,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -35,20 +36,20 @@ sys.path.insert(0, str(ROOT / "finite-volumes-rs_b200"))
 METRIC = "solves/s and DOF-iters/s vs plain FP64 at rel err <=1e-8; p50/p99 solve latency"
 
 WORKLOADS = {
-    # BASELINE configuration "plain FP64 3D convection-diffusion", 128^3 hexes x 6 tets
+    # plain FP64 3D convection-diffusion, 128^3 hexes x 6 tets (the headline problem)
     "cube128_convdiff": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     # the CPU-runnable 2D case: 256x256 squares x 2 triangles, lognormal(0,1)
     "square256_diffusion": dict(kind="2d", n=256, jitter=0.2, sigma=1.0, solver="cg"),
     # smaller versions (profiling captures, smoke runs); cube64 still exceeds L2
-    # BASELINE mixed-precision configuration: the 3D case with FP32 BiCGStab + FP32 ILU(0)
+    # mixed precision: the 3D case with FP32 BiCGStab + FP32 ILU(0)
     # inside FP64 reliable updates, to |b - A x| / |b| <= 1e-10
     "cube128_convdiff_mixed": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
                                    solver="bicgstab", precision="mixed"),
     "cube64_convdiff": dict(kind="3d", n=64, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     "cube32_convdiff": dict(kind="3d", n=32, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
-    # BASELINE batched configuration: 1,024 2D diffusion problems, mixed precision
+    # batched: 1,024 2D diffusion problems of uneven sizes
     "batch1024_diffusion": dict(kind="batch"),
-    # BASELINE served configuration (Poisson stream, continuous batching)
+    # served: a Poisson stream of requests, continuous batching
     "serve_mixed": dict(kind="serve"),
     # the time loop of the crate's examples on the config-1 mesh: implicit Euler,
     # per step value-only re-assembly, ILU(0) refactorisation, BiCGStab from
@@ -126,8 +127,9 @@ class Clocks:
 
     def start(self):
         try:
-            out = ROOT / "gpurun_out"
-            out.mkdir(exist_ok=True)
+            # raw samples go to FV_BENCH_CLOCKS_DIR when set (kept for inspection), else a temporary folder
+            out = Path(os.environ.get("FV_BENCH_CLOCKS_DIR") or tempfile.mkdtemp(prefix="fv_clocks_"))
+            out.mkdir(parents=True, exist_ok=True)
             self.path = out / f"clocks_rank{self.index}{self.tag}.csv"
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -579,7 +581,7 @@ def transient_arm(args, rank, world, local_rank):
 
 
 def batch_problems(fv, count, seed, rank):
-    """BASELINE batched configuration: `count` 2D diffusion problems built as the
+    """The batched workload: `count` 2D diffusion problems built as the
     256x256 case, sides log-uniform in [32, 512], per-problem sigma ~ U(0.5, 2),
     seeds seed+k.  Meshes are generated on all host cores."""
     from concurrent.futures import ThreadPoolExecutor

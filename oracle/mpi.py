@@ -1,5 +1,5 @@
 """MPI-semantics oracle (block-Jacobi over P contiguous partitions, one OpenMP
-thread per rank) -- TEST / BASELINE INFRASTRUCTURE ONLY.  See oracle_mpi.c."""
+thread per rank) -- TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  See oracle_mpi.c."""
 from __future__ import annotations
 
 import ctypes as C

@@ -1,5 +1,5 @@
 /*
- * CPU oracle, MPI semantics -- TEST / BASELINE INFRASTRUCTURE ONLY.
+ * CPU oracle, MPI semantics -- TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
  *
  * Restates what the finite-volumes crate computes when it runs on P MPI
  * ranks, with one OpenMP thread standing for one rank:
