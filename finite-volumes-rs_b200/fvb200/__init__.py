@@ -13,6 +13,7 @@ from .linalg import (  # noqa: F401
     LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, compute_gradients,
     conjugate_gradient,
 )
+from .bcs import FaceConstraints  # noqa: F401
 from .mesh import DeviceMesh, Mesh  # noqa: F401
 from .terms import (  # noqa: F401
     Backward, Corrected, Euler, Orthogonal, Upwind, convection, divergence, laplacian, linear_source, source, time,

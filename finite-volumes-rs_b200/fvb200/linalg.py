@@ -133,12 +133,26 @@ class DistributedMatrix:
             pass
 
 
+def _bc_arrays(boundary_condition, mesh):
+    """(bndi, bnde) over the boundary faces from a FaceConstraints, a callable
+    face id -> (bndi, bnde), or the pair of arrays itself."""
+    if hasattr(boundary_condition, "as_bc"):
+        return boundary_condition.as_bc()
+    if callable(boundary_condition):
+        nb = mesh.n_boundary_faces
+        fb0 = mesh.n_faces - nb
+        pairs = [boundary_condition(fb0 + k) for k in range(nb)]
+        return (np.array([p[0] for p in pairs], dtype=np.float64),
+                np.array([p[1] for p in pairs], dtype=np.float64))
+    return boundary_condition
+
+
 def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None = None, stream=None):
     """assemble(equation, boundary_condition, mesh) -> (DistributedMatrix, DistributedVector).
 
-    boundary_condition: a callable face_id -> (bndi, bnde) as in the reference
-    (evaluated once per boundary face on the host), or a pair of arrays
-    (bndi, bnde) over the boundary faces.  Passing `lhs` from an earlier call
+    boundary_condition: a FaceConstraints, a callable face_id -> (bndi, bnde)
+    as in the reference (evaluated once per boundary face on the host), or a
+    pair of arrays (bndi, bnde) over the boundary faces.  Passing `lhs` from an earlier call
     on the same mesh refills its values in place (value-only re-assembly).
     """
     torch = _torch()
@@ -194,14 +208,7 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
     if "divergence" in equation.data:
         t.divergence_coef = equation.coefficient("divergence")
         t.divergence_flux = arr(equation.data["divergence"])
-    nb = mesh.n_boundary_faces
-    if callable(boundary_condition):
-        fb0 = mesh.n_faces - nb
-        pairs = [boundary_condition(fb0 + k) for k in range(nb)]
-        bndi = np.array([p[0] for p in pairs], dtype=np.float64)
-        bnde = np.array([p[1] for p in pairs], dtype=np.float64)
-    else:
-        bndi, bnde = boundary_condition
+    bndi, bnde = _bc_arrays(boundary_condition, mesh)
     bi = _dev_f64(bndi)
     be = _dev_f64(bnde)
     keep += [bi, be]
@@ -225,14 +232,7 @@ def compute_gradients(gradients: DistributedVector, values, boundary_condition, 
     pair of arrays over the boundary faces)."""
     dm = mesh.device(stream)
     v = _dev_f64(values)
-    nb = mesh.n_boundary_faces
-    if callable(boundary_condition):
-        fb0 = mesh.n_faces - nb
-        pairs = [boundary_condition(fb0 + k) for k in range(nb)]
-        bndi = np.array([p[0] for p in pairs], dtype=np.float64)
-        bnde = np.array([p[1] for p in pairs], dtype=np.float64)
-    else:
-        bndi, bnde = boundary_condition
+    bndi, bnde = _bc_arrays(boundary_condition, mesh)
     bi, be = _dev_f64(bndi), _dev_f64(bnde)
     if len(gradients) != mesh.n_cells * mesh.dim:
         raise ValueError("gradients must hold n_cells * dim values")

@@ -276,3 +276,20 @@ def test_oracle_diagonal_preconditioner(fv, orc):
     assert np.array_equal(z, (1.0 / A.diagonal()) * r)
     bad = orc.Precond("diag", np.array([0, 2, 3]), np.array([0, 1, 0]), np.ones(3))
     assert not bad.ok() and bad.status == 1
+
+
+def test_face_constraints(fv):
+    """FaceConstraints (fvm/bcs/mod.rs): indexed by face id from the first boundary face, (0, 0) by default,
+    set per face or for many faces at once; as_bc() is the (bndi, bnde) pair assemble takes."""
+    m = fv.Mesh.square(4, 0.0, 0)
+    fc = fv.FaceConstraints.from_mesh(m)
+    fb0 = m.n_faces - m.n_boundary_faces
+    assert fc[fb0] == (0.0, 0.0)
+    fc[fb0 + 1] = (1.0, 0.0)
+    bottom = [f for f in range(fb0, m.n_faces) if abs(m.face_center[f, 1]) < 1e-12]
+    fc[bottom] = (0.0, 2.5)
+    bi, be = fc.as_bc()
+    assert len(bi) == m.n_boundary_faces and bi[1] == 1.0
+    assert np.all(be[np.array(bottom) - fb0] == 2.5)
+    with pytest.raises(IndexError):
+        fc[0]

@@ -213,3 +213,20 @@ def test_diagonal_preconditioner_matches_oracle(fv, orc, kind):
     P2 = fv.DiagonalPreconditioner.from_matrix(A2)
     P2.precondition(z, fv.DistributedVector(r))
     assert np.array_equal(z.numpy(), orc.Precond("diag", ptr, cols, 2.0 * np.asarray(vals)).apply(r))
+
+
+def test_face_constraints_as_boundary_condition(fv, orc):
+    """A FaceConstraints passed to assemble gives the same system as its (bndi, bnde) arrays and the oracle."""
+    case = diffusion_2d(fv, 12, seed=21)
+    m = case["mesh"]
+    fc = fv.FaceConstraints.from_mesh(m)
+    fb0 = m.n_faces - m.n_boundary_faces
+    for f in range(fb0, m.n_faces):
+        fc[f] = (1.0, 0.0) if m.face_center[f, 0] > 0.999 else (0.0, float(m.face_center[f, 1]))
+    bi, be = fc.as_bc()
+    A, b = fv.assemble(equation(fv, case), fc, m)
+    ptr, cols, vals, rhs = orc.assemble(m, case["c_lap"], case["c_conv"], case["c_src"], kappa=case["kappa"],
+                                        flux=case["flux"], source=case["source"], bndi=bi, bnde=be)
+    gp, gc, gv = A.to_csr()
+    assert np.array_equal(gp, ptr) and np.array_equal(gc, cols) and np.array_equal(gv, vals)
+    assert np.array_equal(b.numpy(), rhs)
