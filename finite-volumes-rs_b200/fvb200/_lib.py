@@ -140,6 +140,9 @@ _SIGS = {
     "fv_ic0_factor": [vp, vp, P(vp)],
     "fv_ilu0_factor": [vp, vp, P(vp)],
     "fv_diag_factor": [vp, vp, P(vp)],
+    "fv_vec_dot": [i64, vp, vp, vp, P(C.c_double)],
+    "fv_vec_sum": [i64, vp, vp, P(C.c_double)],
+    "fv_vec_update": [i64, vp, vp, C.c_double, C.c_int32, vp],
     "fv_ic_factor": [vp, C.c_int32, vp, P(vp)],
     "fv_ilu_factor": [vp, C.c_int32, vp, P(vp)],
     "fv_precond_refactor": [vp, vp],

@@ -18,7 +18,7 @@ CSRC = PKG.parent / "csrc"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libfvb200.so"
 
-CUDA_SOURCES = ["fv_assembly.cu", "fv_precond.cu", "fv_solvers.cu", "fv_batch.cu", "fv_dist.cu", "fv_tiles.cu", "fv_fill.cu", "fv_meshbuild.cu"]
+CUDA_SOURCES = ["fv_assembly.cu", "fv_precond.cu", "fv_solvers.cu", "fv_batch.cu", "fv_dist.cu", "fv_tiles.cu", "fv_fill.cu", "fv_meshbuild.cu", "fv_vector.cu"]
 HOST_SOURCES = ["meshgen.cpp"]
 
 NVCC_FLAGS = [

@@ -64,6 +64,59 @@ class DistributedVector:
     def numpy(self) -> np.ndarray:
         return self.data.detach().cpu().numpy()
 
+    # DistributedVector operations (linalg/dvector.rs:46-160) on the device
+    def dot(self, rhs: "DistributedVector", stream=None) -> float:
+        if len(self) != len(rhs):
+            raise ValueError("dot: lengths differ (the reference asserts)")
+        return self.dot_smaller(rhs, stream)
+
+    def dot_smaller(self, rhs: "DistributedVector", stream=None) -> float:
+        out = C.c_double()
+        check(lib().fv_vec_dot(min(len(self), len(rhs)), self.ptr(), rhs.ptr(), stream_handle(stream),
+                               C.byref(out)), "dot")
+        return out.value
+
+    def sum(self, stream=None) -> float:
+        out = C.c_double()
+        check(lib().fv_vec_sum(len(self), self.ptr(), stream_handle(stream), C.byref(out)), "sum")
+        return out.value
+
+    def _update(self, other, a, op, n=None, stream=None):
+        x = other.ptr() if other is not None else None
+        check(lib().fv_vec_update(len(self) if n is None else n, self.ptr(), x, float(a), op,
+                                  stream_handle(stream)), "vector update")
+        return self
+
+    def __iadd__(self, rhs: "DistributedVector"):
+        if len(self) != len(rhs):
+            raise ValueError("+=: lengths differ")
+        return self._update(rhs, 0.0, 0)
+
+    def __isub__(self, rhs: "DistributedVector"):
+        if len(self) != len(rhs):
+            raise ValueError("-=: lengths differ")
+        return self._update(rhs, 0.0, 1)
+
+    def __imul__(self, a: float):
+        return self._update(None, a, 2)
+
+    def inv(self) -> "DistributedVector":
+        return self._update(None, 0.0, 3)
+
+    def set(self, rhs: "DistributedVector"):
+        if len(rhs) < len(self):
+            raise ValueError("set: source shorter than the vector")
+        return self._update(rhs, 0.0, 4)
+
+    def set_smaller(self, rhs: "DistributedVector"):
+        return self._update(rhs, 0.0, 4, n=min(len(self), len(rhs)))
+
+    def __getitem__(self, i):
+        return float(self.data[i].item())
+
+    def __setitem__(self, i, v):
+        self.data[i] = float(v)
+
     def ptr(self) -> C.c_void_p:
         return C.c_void_p(self.data.data_ptr())
 

@@ -308,6 +308,17 @@ fv_status fv_csr_destroy(fv_csr *A);
 fv_status fv_spmv(const fv_csr *A, const double *x, double *y, void *stream);
 fv_status fv_spmv_host(const fv_csr *A, const double *x_host, double *y_host, void *stream);
 
+/* DistributedVector operations (linalg/dvector.rs:46-160) on device vectors.
+ * fv_vec_dot: dot / dot_smaller (the caller passes the shorter length);
+ * fv_vec_sum: sum.  Both write the result to host *out after their stream
+ * finished; the sum order is fixed by n (strided per thread, a fixed tree,
+ * block partials in order), not the reference's serial order: results agree
+ * to rounding.  fv_vec_update, elementwise and exact: op 0 y += x, 1 y -= x,
+ * 2 y *= a, 3 y = 1/y (inv), 4 y = x (set / set_smaller with the shorter n). */
+fv_status fv_vec_dot(int64_t n, const double *x, const double *y, void *stream, double *out);
+fv_status fv_vec_sum(int64_t n, const double *x, void *stream, double *out);
+fv_status fv_vec_update(int64_t n, double *y, const double *x, double a, int32_t op, void *stream);
+
 /* IncompleteCholesky::from_matrix(A, 0) / IncompleteLowerUpper::from_matrix(A, 0). */
 fv_status fv_ic0_factor(const fv_csr *A, void *stream, fv_precond **out);
 fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **out);
