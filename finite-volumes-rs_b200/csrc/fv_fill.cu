@@ -13,7 +13,12 @@
 // The walk order matters for levels where a node can be reached by paths of
 // different lengths, so it is restated exactly: neighbours in ascending
 // order, last pushed popped first, a node marked on its first visit.
+//
+// Rows are independent, so the rows are split into contiguous ranges walked
+// by host threads, each with its own visited marks; the ranges are joined in
+// row order, which gives the same arrays as one sequential pass.
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "fv_internal.cuh"
@@ -22,90 +27,141 @@ namespace {
 
 enum Walk { kUpperThroughLower, kLowerThroughUpper, kBall };
 
-// Returns the walk's result set (unsorted); stamp/len/stack are scratch of
-// size n; gen is a value no earlier walk used (a fresh visited set).
-void walk(Walk w, int32_t i, int level, const int32_t *ptr, const int32_t *col, std::vector<int64_t> &stamp,
-          int64_t gen, std::vector<int32_t> &len, std::vector<int32_t> &stack, std::vector<int32_t> &out) {
-    out.clear();
-    stack.clear();
-    stack.push_back(i);
-    stamp[i] = gen;
-    len[i] = 0;
-    while (!stack.empty()) {
-        const int32_t k = stack.back();
-        stack.pop_back();
-        const int32_t lk = len[k];
-        for (int32_t t = ptr[k]; t < ptr[k + 1]; ++t) {
-            const int32_t j = col[t];
-            if (j == k) continue;
-            if (stamp[j] == gen) continue;
-            stamp[j] = gen;
-            if (w == kBall) {
-                if (lk < level) {
+struct Walker {
+    std::vector<uint32_t> mark;  // mark[j] == gen: j visited by the current walk
+    uint32_t gen = 0;
+    std::vector<int32_t> stack;  // (node, path length) pairs, last pushed on top
+
+    // Appends the walk's result set (unsorted) to out.
+    void walk(Walk w, int32_t i, int level, const int32_t *ptr, const int32_t *col, std::vector<int32_t> &out) {
+        ++gen;
+        stack.clear();
+        stack.push_back(i);
+        stack.push_back(0);
+        mark[i] = gen;
+        while (!stack.empty()) {
+            const int32_t lk = stack.back();
+            stack.pop_back();
+            const int32_t k = stack.back();
+            stack.pop_back();
+            for (int32_t t = ptr[k]; t < ptr[k + 1]; ++t) {
+                const int32_t j = col[t];
+                if (j == k) continue;
+                if (mark[j] == gen) continue;
+                mark[j] = gen;
+                const bool down = w == kBall || (w == kUpperThroughLower ? j < i : j > i);
+                if (down && lk < level) {
                     stack.push_back(j);
-                    len[j] = lk + 1;
-                    out.push_back(j);
-                }
-            } else if (w == kUpperThroughLower) {
-                if (j < i && lk < level) {
-                    stack.push_back(j);
-                    len[j] = lk + 1;
-                } else if (j > i) {
-                    out.push_back(j);
-                }
-            } else {
-                if (j > i && lk < level) {
-                    stack.push_back(j);
-                    len[j] = lk + 1;
-                } else if (j < i) {
+                    stack.push_back(lk + 1);
+                    if (w == kBall) out.push_back(j);
+                } else if (w == kUpperThroughLower ? j > i : w == kLowerThroughUpper && j < i) {
                     out.push_back(j);
                 }
             }
+        }
+    }
+};
+
+struct Part {
+    int64_t r0 = 0, r1 = 0;
+    std::vector<int32_t> len;   // entries per row
+    std::vector<int32_t> col;   // the rows' sorted patterns, concatenated
+    std::vector<int32_t> amap;  // A entry -> index into col
+    std::vector<uint8_t> fill;  // 1 for entries not in A (IC only)
+    bool ok = true;
+};
+
+void walk_rows(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col, Part &p) {
+    Walker wk;
+    wk.mark.assign((size_t)n, 0);
+    std::vector<int32_t> row;
+    p.len.resize((size_t)(p.r1 - p.r0));
+    p.amap.resize((size_t)(ptr[p.r1] - ptr[p.r0]));
+    for (int64_t i = p.r0; i < p.r1; ++i) {
+        row.clear();
+        if (kind == 2) {
+            wk.walk(kLowerThroughUpper, (int32_t)i, level, ptr, col, row);
+            row.push_back((int32_t)i);
+            wk.walk(kUpperThroughLower, (int32_t)i, level, ptr, col, row);
+        } else {
+            wk.walk(kBall, (int32_t)i, level, ptr, col, row);
+            row.insert(row.end(), col + ptr[i], col + ptr[i + 1]);
+        }
+        std::sort(row.begin(), row.end());
+        row.erase(std::unique(row.begin(), row.end()), row.end());
+        const size_t base = p.col.size();
+        if (kind == 1) p.fill.insert(p.fill.end(), row.size(), (uint8_t)1);
+        // the matrix's own entries must be part of the pattern
+        size_t q = 0;
+        for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) {
+            while (q < row.size() && row[q] < col[t]) ++q;
+            if (q == row.size() || row[q] != col[t]) {
+                p.ok = false;
+                return;
+            }
+            p.amap[(size_t)(t - ptr[p.r0])] = (int32_t)(base + q);
+            if (kind == 1) p.fill[base + q] = 0;
+        }
+        p.col.insert(p.col.end(), row.begin(), row.end());
+        p.len[(size_t)(i - p.r0)] = (int32_t)row.size();
+        if ((int64_t)p.col.size() > 0x7fffffffLL - 64) {
+            p.ok = false;
+            return;
         }
     }
 }
 
 }  // namespace
 
+/* fill is filled for IC (kind 1) only: 1 for pattern entries that are not
+ * entries of A.  Returns false when A's own entries are not all in the
+ * pattern (a pattern without its diagonal) or the pattern would not fit
+ * 32-bit offsets. */
 bool fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
                      std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
                      std::vector<uint8_t> &fill) {
-    std::vector<int64_t> stamp((size_t)n, -1);
-    std::vector<int32_t> len((size_t)n, 0), stack, a, b, row;
+    // one range per thread, at least 256 rows each, at most 16 threads (each
+    // holds 4 bytes of visited marks per row of A)
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>({(int64_t)hw, 16, n / 256}));
+    std::vector<Part> parts((size_t)nt);
+    for (int64_t p = 0; p < nt; ++p) {
+        parts[(size_t)p].r0 = n * p / nt;
+        parts[(size_t)p].r1 = n * (p + 1) / nt;
+    }
+    {
+        std::vector<std::thread> th;
+        for (int64_t p = 1; p < nt; ++p)
+            th.emplace_back(walk_rows, kind, level, n, ptr, col, std::ref(parts[(size_t)p]));
+        walk_rows(kind, level, n, ptr, col, parts[0]);
+        for (auto &t : th) t.join();
+    }
+    int64_t total = 0;
+    std::vector<int64_t> base((size_t)nt);
+    for (int64_t p = 0; p < nt; ++p) {
+        if (!parts[(size_t)p].ok) return false;
+        base[(size_t)p] = total;
+        total += (int64_t)parts[(size_t)p].col.size();
+        if (total > 0x7fffffffLL - 64) return false;
+    }
     fptr.assign((size_t)n + 1, 0);
-    fcol.clear();
-    fill.clear();
-    amap.assign((size_t)ptr[n], 0);
-    for (int64_t i = 0; i < n; ++i) {
-        row.clear();
-        if (kind == 2) {
-            walk(kLowerThroughUpper, (int32_t)i, level, ptr, col, stamp, 2 * i, len, stack, a);
-            walk(kUpperThroughLower, (int32_t)i, level, ptr, col, stamp, 2 * i + 1, len, stack, b);
-            row.insert(row.end(), a.begin(), a.end());
-            row.push_back((int32_t)i);
-            row.insert(row.end(), b.begin(), b.end());
-        } else {
-            walk(kBall, (int32_t)i, level, ptr, col, stamp, 2 * i, len, stack, a);
-            row.insert(row.end(), a.begin(), a.end());
-            for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) row.push_back(col[t]);
-        }
-        std::sort(row.begin(), row.end());
-        row.erase(std::unique(row.begin(), row.end()), row.end());
-        // the matrix's own entries must be part of the pattern
-        size_t q = 0;
-        for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) {
-            while (q < row.size() && row[q] < col[t]) ++q;
-            if (q == row.size() || row[q] != col[t]) return false;
-            amap[t] = (int32_t)(fcol.size() + q);
-        }
-        for (size_t u = 0; u < row.size(); ++u) {
-            fcol.push_back(row[u]);
-            bool in_a = false;
-            for (int32_t t = ptr[i]; t < ptr[i + 1] && !in_a; ++t) in_a = col[t] == row[u];
-            fill.push_back(in_a ? 0 : 1);
-        }
-        fptr[i + 1] = (int32_t)fcol.size();
-        if ((int64_t)fcol.size() > 0x7fffffffLL - 64) return false;
+    fcol.resize((size_t)total);
+    amap.resize((size_t)ptr[n]);
+    fill.resize(kind == 1 ? (size_t)total : 0);
+    auto join = [&](int64_t p) {
+        const Part &q = parts[(size_t)p];
+        const int32_t b = (int32_t)base[(size_t)p];
+        int32_t acc = b;
+        for (int64_t i = q.r0; i < q.r1; ++i) fptr[(size_t)i + 1] = acc += q.len[(size_t)(i - q.r0)];
+        std::copy(q.col.begin(), q.col.end(), fcol.begin() + b);
+        if (kind == 1) std::copy(q.fill.begin(), q.fill.end(), fill.begin() + b);
+        for (size_t t = 0; t < q.amap.size(); ++t) amap[(size_t)ptr[q.r0] + t] = b + q.amap[t];
+    };
+    {
+        std::vector<std::thread> th;
+        for (int64_t p = 1; p < nt; ++p) th.emplace_back(join, p);
+        join(0);
+        for (auto &t : th) t.join();
     }
     return true;
 }
