@@ -68,7 +68,7 @@ struct Part {
     std::vector<int32_t> col;   // the rows' sorted patterns, concatenated
     std::vector<int32_t> amap;  // A entry -> index into col
     std::vector<uint8_t> fill;  // 1 for entries not in A (IC only)
-    bool ok = true;
+    fv_status status = FV_OK;
 };
 
 void walk_rows(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col, Part &p) {
@@ -96,7 +96,7 @@ void walk_rows(int kind, int level, int64_t n, const int32_t *ptr, const int32_t
         for (int32_t t = ptr[i]; t < ptr[i + 1]; ++t) {
             while (q < row.size() && row[q] < col[t]) ++q;
             if (q == row.size() || row[q] != col[t]) {
-                p.ok = false;
+                p.status = FV_ERR_UNSUPPORTED;
                 return;
             }
             p.amap[(size_t)(t - ptr[p.r0])] = (int32_t)(base + q);
@@ -105,63 +105,78 @@ void walk_rows(int kind, int level, int64_t n, const int32_t *ptr, const int32_t
         p.col.insert(p.col.end(), row.begin(), row.end());
         p.len[(size_t)(i - p.r0)] = (int32_t)row.size();
         if ((int64_t)p.col.size() > 0x7fffffffLL - 64) {
-            p.ok = false;
+            p.status = FV_ERR_UNSUPPORTED;
             return;
         }
     }
 }
 
+void walk_rows_caught(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col, Part &p) {
+    try {
+        walk_rows(kind, level, n, ptr, col, p);
+    } catch (...) {  // std::bad_alloc: no exception may leave a thread
+        p.status = FV_ERR_ALLOC;
+    }
+}
+
+// Runs f(0) .. f(nt - 1), one thread each where a thread can be started and
+// on the calling thread otherwise.
+template <typename F>
+void run_parts(int64_t nt, F f) {
+    std::vector<std::thread> th;
+    try {
+        th.reserve((size_t)nt);
+        for (int64_t p = 1; p < nt; ++p) th.emplace_back(f, p);
+    } catch (...) {
+    }
+    f(0);
+    for (int64_t p = (int64_t)th.size() + 1; p < nt; ++p) f(p);
+    for (auto &t : th) t.join();
+}
+
 }  // namespace
 
 /* fill is filled for IC (kind 1) only: 1 for pattern entries that are not
- * entries of A.  Returns false when A's own entries are not all in the
+ * entries of A.  FV_ERR_UNSUPPORTED when A's own entries are not all in the
  * pattern (a pattern without its diagonal) or the pattern would not fit
- * 32-bit offsets. */
-bool fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
-                     std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
-                     std::vector<uint8_t> &fill) {
-    // one range per thread, at least 256 rows each, at most 16 threads (each
-    // holds 4 bytes of visited marks per row of A)
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>({(int64_t)hw, 16, n / 256}));
-    std::vector<Part> parts((size_t)nt);
-    for (int64_t p = 0; p < nt; ++p) {
-        parts[(size_t)p].r0 = n * p / nt;
-        parts[(size_t)p].r1 = n * (p + 1) / nt;
+ * 32-bit offsets; FV_ERR_ALLOC when host memory runs out. */
+fv_status fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
+                          std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
+                          std::vector<uint8_t> &fill) {
+    try {
+        // one range per thread, at least 256 rows each, at most 16 threads
+        // (each holds 4 bytes of visited marks per row of A)
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int64_t nt = std::max<int64_t>(1, std::min<int64_t>({(int64_t)hw, 16, n / 256}));
+        std::vector<Part> parts((size_t)nt);
+        for (int64_t p = 0; p < nt; ++p) {
+            parts[(size_t)p].r0 = n * p / nt;
+            parts[(size_t)p].r1 = n * (p + 1) / nt;
+        }
+        run_parts(nt, [&](int64_t p) { walk_rows_caught(kind, level, n, ptr, col, parts[(size_t)p]); });
+        int64_t total = 0;
+        std::vector<int64_t> base((size_t)nt);
+        for (int64_t p = 0; p < nt; ++p) {
+            if (parts[(size_t)p].status != FV_OK) return parts[(size_t)p].status;
+            base[(size_t)p] = total;
+            total += (int64_t)parts[(size_t)p].col.size();
+            if (total > 0x7fffffffLL - 64) return FV_ERR_UNSUPPORTED;
+        }
+        fptr.assign((size_t)n + 1, 0);
+        fcol.resize((size_t)total);
+        amap.resize((size_t)ptr[n]);
+        fill.resize(kind == 1 ? (size_t)total : 0);
+        run_parts(nt, [&](int64_t p) {
+            const Part &q = parts[(size_t)p];
+            const int32_t b = (int32_t)base[(size_t)p];
+            int32_t acc = b;
+            for (int64_t i = q.r0; i < q.r1; ++i) fptr[(size_t)i + 1] = acc += q.len[(size_t)(i - q.r0)];
+            std::copy(q.col.begin(), q.col.end(), fcol.begin() + b);
+            if (kind == 1) std::copy(q.fill.begin(), q.fill.end(), fill.begin() + b);
+            for (size_t t = 0; t < q.amap.size(); ++t) amap[(size_t)ptr[q.r0] + t] = b + q.amap[t];
+        });
+        return FV_OK;
+    } catch (...) {
+        return FV_ERR_ALLOC;
     }
-    {
-        std::vector<std::thread> th;
-        for (int64_t p = 1; p < nt; ++p)
-            th.emplace_back(walk_rows, kind, level, n, ptr, col, std::ref(parts[(size_t)p]));
-        walk_rows(kind, level, n, ptr, col, parts[0]);
-        for (auto &t : th) t.join();
-    }
-    int64_t total = 0;
-    std::vector<int64_t> base((size_t)nt);
-    for (int64_t p = 0; p < nt; ++p) {
-        if (!parts[(size_t)p].ok) return false;
-        base[(size_t)p] = total;
-        total += (int64_t)parts[(size_t)p].col.size();
-        if (total > 0x7fffffffLL - 64) return false;
-    }
-    fptr.assign((size_t)n + 1, 0);
-    fcol.resize((size_t)total);
-    amap.resize((size_t)ptr[n]);
-    fill.resize(kind == 1 ? (size_t)total : 0);
-    auto join = [&](int64_t p) {
-        const Part &q = parts[(size_t)p];
-        const int32_t b = (int32_t)base[(size_t)p];
-        int32_t acc = b;
-        for (int64_t i = q.r0; i < q.r1; ++i) fptr[(size_t)i + 1] = acc += q.len[(size_t)(i - q.r0)];
-        std::copy(q.col.begin(), q.col.end(), fcol.begin() + b);
-        if (kind == 1) std::copy(q.fill.begin(), q.fill.end(), fill.begin() + b);
-        for (size_t t = 0; t < q.amap.size(); ++t) amap[(size_t)ptr[q.r0] + t] = b + q.amap[t];
-    };
-    {
-        std::vector<std::thread> th;
-        for (int64_t p = 1; p < nt; ++p) th.emplace_back(join, p);
-        join(0);
-        for (auto &t : th) t.join();
-    }
-    return true;
 }

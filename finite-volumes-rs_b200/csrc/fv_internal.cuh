@@ -90,9 +90,9 @@ struct fv_symbolic;  // triangular split + level schedules of a pattern (fv_prec
 //                 (incomplete_lower_upper.rs:30-137)
 //   kind 1 (IC):  row i = entries of A ∪ the level-ball of i
 //                 (incomplete_cholesky.rs:35-85, 148-192); fill[k] marks fill
-bool fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
-                     std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
-                     std::vector<uint8_t> &fill);
+fv_status fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, const int32_t *col,
+                          std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
+                          std::vector<uint8_t> &fill);
 
 // Box tiling of one sweep direction (fv_tiles.cu): boxes in dispatch order,
 // each a run of steps (rows of one level, at most 32); trow lists the rows in

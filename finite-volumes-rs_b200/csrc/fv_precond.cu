@@ -24,6 +24,7 @@
 // unchanged, which is what skipping them does in the reference.
 #include <algorithm>
 #include <cmath>
+#include <new>
 #include <type_traits>
 #include <vector>
 
@@ -1884,14 +1885,20 @@ static fv_status fill_factor(const fv_csr *Ac, int kind, int level, cudaStream_t
     if (A->nrows != A->ncols) return FV_ERR_INVALID;
     if (kind == 1) FV_TRY(check_symmetric(A, st));
     const int64_t n = A->nrows, nnz = A->nnz;
-    std::vector<int32_t> ptr((size_t)n + 1), col((size_t)(nnz ? nnz : 1));
+    std::vector<int32_t> ptr, col, fptr, fcol, amap;
+    std::vector<uint8_t> fill;
+    try {
+        ptr.resize((size_t)n + 1);
+        col.resize((size_t)(nnz ? nnz : 1));
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
     FV_CUDA_TRY(cudaMemcpyAsync(ptr.data(), A->row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
     if (nnz) FV_CUDA_TRY(cudaMemcpyAsync(col.data(), A->cols, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
     FV_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<int32_t> fptr, fcol, amap;
-    std::vector<uint8_t> fill;
-    if (!fv_fill_pattern(kind, level, n, ptr.data(), col.data(), fptr, fcol, amap, fill)) return FV_ERR_UNSUPPORTED;
-    fv_csr *F = new fv_csr();
+    FV_TRY(fv_fill_pattern(kind, level, n, ptr.data(), col.data(), fptr, fcol, amap, fill));
+    fv_csr *F = new (std::nothrow) fv_csr();
+    if (!F) return FV_ERR_ALLOC;
     F->nrows = F->ncols = n;
     F->nnz = (int64_t)fcol.size();
     if (kind == 1) F->fill_mask = std::move(fill);
