@@ -715,7 +715,7 @@ extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
     return FV_OK;
 }
 
-extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh **out) {
+static fv_status mesh_upload_impl(const fv_mesh_desc *d, void *stream, fv_mesh **out) {
     if (!d || !out || (d->dim != 2 && d->dim != 3) || d->n_cells <= 0 || d->n_faces <= 0 || d->n_boundary_faces < 0 ||
         d->n_boundary_faces > d->n_faces || !d->face_owner || !d->face_neighbor || !d->face_area ||
         !d->cell_center || !d->cell_volume || (d->n_boundary_faces > 0 && !d->face_center) ||
@@ -859,6 +859,10 @@ extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh
     }
     *out = m;
     return FV_OK;
+}
+
+extern "C" fv_status fv_mesh_upload(const fv_mesh_desc *d, void *stream, fv_mesh **out) {
+    return fv_host_guard([&] { return mesh_upload_impl(d, stream, out); });
 }
 
 extern "C" fv_status fv_compute_gradients(fv_mesh *m, const double *values, const fv_bc_desc *bc, double *grad,

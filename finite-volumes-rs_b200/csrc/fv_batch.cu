@@ -654,8 +654,8 @@ extern "C" fv_status fv_batch_destroy(fv_batch *B) {
     return FV_OK;
 }
 
-extern "C" fv_status fv_batch_create(const fv_csr *A, int32_t n_problems, const int64_t *row_offsets,
-                                     int32_t tile_rows, void *stream, fv_batch **out) {
+static fv_status batch_create_impl(const fv_csr *A, int32_t n_problems, const int64_t *row_offsets,
+                                   int32_t tile_rows, void *stream, fv_batch **out) {
     if (!A || !out || n_problems <= 0 || !row_offsets || A->nrows != A->ncols) return FV_ERR_INVALID;
     if (row_offsets[0] != 0 || row_offsets[n_problems] != A->nrows) return FV_ERR_INVALID;
     if (tile_rows <= 0) tile_rows = 1024;
@@ -713,6 +713,11 @@ extern "C" fv_status fv_batch_create(const fv_csr *A, int32_t n_problems, const 
     }
     *out = B;
     return FV_OK;
+}
+
+extern "C" fv_status fv_batch_create(const fv_csr *A, int32_t n_problems, const int64_t *row_offsets,
+                                     int32_t tile_rows, void *stream, fv_batch **out) {
+    return fv_host_guard([&] { return batch_create_impl(A, n_problems, row_offsets, tile_rows, stream, out); });
 }
 
 namespace {
@@ -978,10 +983,10 @@ fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, do
 
 extern "C" fv_status fv_batch_cg(fv_batch *B, fv_precond *P, const double *b, double *x,
                                  const fv_batch_options *opt, fv_batch_info *info, void *stream) {
-    return batch_solve(false, B, P, b, x, opt, info, fv_stream(stream));
+    return fv_host_guard([&] { return batch_solve(false, B, P, b, x, opt, info, fv_stream(stream)); });
 }
 
 extern "C" fv_status fv_batch_bicgstab(fv_batch *B, fv_precond *P, const double *b, double *x,
                                        const fv_batch_options *opt, fv_batch_info *info, void *stream) {
-    return batch_solve(true, B, P, b, x, opt, info, fv_stream(stream));
+    return fv_host_guard([&] { return batch_solve(true, B, P, b, x, opt, info, fv_stream(stream)); });
 }

@@ -10,6 +10,8 @@
 
 #include <vector>
 
+#include <new>
+
 #include "fv_b200.h"
 
 #define FV_CUDA_TRY(expr)                                  \
@@ -29,6 +31,22 @@
 
 void fv_internal_set_cuda_error(cudaError_t e, const char *what);
 void fv_internal_set_error_text(const char *what);
+
+// Runs f() so that no C++ exception crosses the C ABI: a failed host
+// allocation (std::bad_alloc from a std::vector) returns FV_ERR_ALLOC, any
+// other exception (a size the host containers reject) FV_ERR_INVALID.
+template <typename F>
+inline fv_status fv_host_guard(F &&f) noexcept {
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        fv_internal_set_error_text("host memory allocation failed");
+        return FV_ERR_ALLOC;
+    } catch (...) {
+        fv_internal_set_error_text("host container size rejected");
+        return FV_ERR_INVALID;
+    }
+}
 // Counts kernel launches made by this library (fv_launch_count).
 // cudaMallocAsync from the device's default pool, which is first told to keep
 // freed memory (release threshold = max): without that the pool hands memory

@@ -1118,7 +1118,7 @@ __global__ void k_cat_cells(int64_t N, int64_t TI, int P, CatPtrs q, int padf, d
 
 }  // namespace
 
-extern "C" fv_status fv_mesh_concat(const fv_mesh *const *parts, int32_t n_parts, void *stream, fv_mesh **out) {
+static fv_status mesh_concat_impl(const fv_mesh *const *parts, int32_t n_parts, void *stream, fv_mesh **out) {
     if (!parts || n_parts <= 0 || !out) return FV_ERR_INVALID;
     *out = nullptr;
     const int P = n_parts;
@@ -1201,4 +1201,8 @@ extern "C" fv_status fv_mesh_concat(const fv_mesh *const *parts, int32_t n_parts
     }
     *out = m;
     return FV_OK;
+}
+
+extern "C" fv_status fv_mesh_concat(const fv_mesh *const *parts, int32_t n_parts, void *stream, fv_mesh **out) {
+    return fv_host_guard([&] { return mesh_concat_impl(parts, n_parts, stream, out); });
 }

@@ -114,7 +114,7 @@ struct fv_precond {
 };
 
 // ------------------------------------------------------------------ symbolic
-static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **out) {
+static fv_status build_symbolic_impl(const fv_csr *A, cudaStream_t st, fv_symbolic **out) {
     const int64_t n = A->nrows, nnz = A->nnz;
     std::vector<int32_t> ptr((size_t)n + 1), col((size_t)(nnz ? nnz : 1));
     FV_CUDA_TRY(cudaMemcpyAsync(ptr.data(), A->row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
@@ -243,11 +243,15 @@ static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **
     return FV_OK;
 }
 
+static fv_status build_symbolic(const fv_csr *A, cudaStream_t st, fv_symbolic **out) {
+    return fv_host_guard([&] { return build_symbolic_impl(A, st, out); });
+}
+
 static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st);
 
 // Box tiles of the two sweeps, planned on first request when the matrix was
 // assembled on a mesh (cell centres known); s->tiled says whether a plan exists.
-static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
+static fv_status build_tiles_impl(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
     if (s->tiles_tried) return FV_OK;
     s->tiles_tried = true;
     const int64_t n = s->n;
@@ -327,6 +331,10 @@ static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
     return FV_OK;
 }
 
+static fv_status build_tiles(fv_symbolic *s, const fv_csr *A, cudaStream_t st) {
+    return fv_host_guard([&] { return build_tiles_impl(s, A, st); });
+}
+
 static fv_status build_symbolic_device(const fv_csr *A, cudaStream_t st, fv_symbolic **out);
 
 // The device analysis serves every pattern without IC(k) fill entries; the
@@ -343,7 +351,7 @@ fv_status fv_get_symbolic(fv_csr *A, cudaStream_t st, fv_symbolic **out) {
 }
 
 // Host copies of the level of every row (box-tile planning, fv_precond_levels).
-static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st) {
+static fv_status ensure_host_levels_impl(fv_symbolic *s, cudaStream_t st) {
     if (!s->h_fwd_level.empty() || s->n == 0 || !s->d_fwd_level) return FV_OK;
     s->h_fwd_level.resize((size_t)s->n);
     s->h_bwd_level.resize((size_t)s->n);
@@ -353,6 +361,10 @@ static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st) {
                                 cudaMemcpyDeviceToHost, st));
     FV_CUDA_TRY(cudaStreamSynchronize(st));
     return FV_OK;
+}
+
+static fv_status ensure_host_levels(fv_symbolic *s, cudaStream_t st) {
+    return fv_host_guard([&] { return ensure_host_levels_impl(s, st); });
 }
 
 // ------------------------------------------------------------------ kernels
@@ -2007,8 +2019,8 @@ extern "C" fv_status fv_precond_apply_host(fv_precond *P, const double *r_host, 
     return s;
 }
 
-extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr, int32_t *cols,
-                                       double *vals, int32_t *n_dropped, void *stream) {
+static fv_status precond_export_impl(const fv_precond *P, int64_t *nnz, int32_t *row_ptr, int32_t *cols,
+                                      double *vals, int32_t *n_dropped, void *stream) {
     if (!P || !nnz) return FV_ERR_INVALID;
     cudaStream_t st = fv_stream(stream);
     const fv_symbolic *s = P->sym;
@@ -2063,6 +2075,11 @@ extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_
     row_ptr[n] = (int32_t)o;
     *nnz = o;
     return FV_OK;
+}
+
+extern "C" fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr, int32_t *cols,
+                                       double *vals, int32_t *n_dropped, void *stream) {
+    return fv_host_guard([&] { return precond_export_impl(P, nnz, row_ptr, cols, vals, n_dropped, stream); });
 }
 
 extern "C" fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,

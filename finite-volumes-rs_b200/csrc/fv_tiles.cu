@@ -327,9 +327,9 @@ bool fv_build_tile_plans(int64_t n, int dim, const double *cell, const int32_t *
 // fv_ilu0_factor build for a matrix assembled on a mesh, from host arrays.
 // sizes[0..2] receive (boxes, steps, entries of the swept side); the arrays
 // may be NULL to query the sizes first.
-extern "C" fv_status fv_tile_plan_host(int64_t n, int32_t dim, const double *cell, const int32_t *row_ptr,
-                                       const int32_t *cols, int32_t direction, int64_t *sizes, int32_t *box_step,
-                                       int32_t *sptr, int32_t *trow, int32_t *dsrc, double *stats) {
+static fv_status tile_plan_host_impl(int64_t n, int32_t dim, const double *cell, const int32_t *row_ptr,
+                                     const int32_t *cols, int32_t direction, int64_t *sizes, int32_t *box_step,
+                                     int32_t *sptr, int32_t *trow, int32_t *dsrc, double *stats) {
     if (n <= 0 || !cell || !row_ptr || !cols || !sizes || (direction != 0 && direction != 1)) return FV_ERR_INVALID;
     std::vector<int32_t> lp((size_t)n + 1), up((size_t)n + 1), lc, uc;
     for (int64_t i = 0; i < n; ++i) {
@@ -390,4 +390,12 @@ extern "C" fv_status fv_tile_plan_host(int64_t n, int32_t dim, const double *cel
         stats[3] = P.est;
     }
     return FV_OK;
+}
+
+extern "C" fv_status fv_tile_plan_host(int64_t n, int32_t dim, const double *cell, const int32_t *row_ptr,
+                                       const int32_t *cols, int32_t direction, int64_t *sizes, int32_t *box_step,
+                                       int32_t *sptr, int32_t *trow, int32_t *dsrc, double *stats) {
+    return fv_host_guard([&] {
+        return tile_plan_host_impl(n, dim, cell, row_ptr, cols, direction, sizes, box_step, sptr, trow, dsrc, stats);
+    });
 }
