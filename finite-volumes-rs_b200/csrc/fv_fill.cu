@@ -18,6 +18,7 @@
 // by host threads, each with its own visited marks; the ranges are joined in
 // row order, which gives the same arrays as one sequential pass.
 #include <algorithm>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -179,4 +180,29 @@ fv_status fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, co
     } catch (...) {
         return FV_ERR_ALLOC;
     }
+}
+
+extern "C" fv_status fv_fill_pattern_host(int32_t kind, int32_t level, int64_t n, const int32_t *row_ptr,
+                                          const int32_t *cols, int64_t *nnz, int32_t *fptr, int32_t *fcol,
+                                          int32_t *amap, uint8_t *fill) {
+    if ((kind != 1 && kind != 2) || level < 0 || n < 0 || n > 0x7fffffffLL || !row_ptr || !nnz) return FV_ERR_INVALID;
+    if (row_ptr[0] != 0 || (row_ptr[n] > 0 && !cols)) return FV_ERR_INVALID;
+    for (int64_t i = 0; i < n; ++i) {
+        if (row_ptr[i + 1] < row_ptr[i]) return FV_ERR_INVALID;
+        for (int32_t t = row_ptr[i]; t < row_ptr[i + 1]; ++t)
+            if (cols[t] < 0 || cols[t] >= n || (t > row_ptr[i] && cols[t] <= cols[t - 1])) return FV_ERR_INVALID;
+    }
+    return fv_host_guard([&]() -> fv_status {
+        std::vector<int32_t> p, c, a;
+        std::vector<uint8_t> f;
+        FV_TRY(fv_fill_pattern(kind, level, n, row_ptr, cols, p, c, a, f));
+        *nnz = (int64_t)c.size();
+        if (!fcol) return FV_OK;
+        if (!fptr) return FV_ERR_INVALID;
+        std::memcpy(fptr, p.data(), sizeof(int32_t) * (size_t)(n + 1));
+        if (!c.empty()) std::memcpy(fcol, c.data(), sizeof(int32_t) * c.size());
+        if (amap && !a.empty()) std::memcpy(amap, a.data(), sizeof(int32_t) * a.size());
+        if (fill && kind == 1 && !f.empty()) std::memcpy(fill, f.data(), f.size());
+        return FV_OK;
+    });
 }

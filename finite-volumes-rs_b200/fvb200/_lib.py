@@ -153,6 +153,7 @@ _SIGS = {
     "fv_precond_destroy": [vp],
     "fv_precond_schedule": [vp, C.c_int32, P(C.c_int32), dp],
     "fv_tile_plan_host": [i64, C.c_int32, dp, ip, ip, C.c_int32, P(i64), ip, ip, ip, ip, dp],
+    "fv_fill_pattern_host": [C.c_int32, C.c_int32, i64, ip, ip, P(i64), ip, ip, ip, P(C.c_uint8)],
     "fv_cg": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
     "fv_bicgstab": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
     "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],

@@ -359,9 +359,36 @@ class Preconditioner:
             pass
 
 
+def _fill_pattern(kind: int, level: int, row_ptr, cols):
+    """Host level-k factor pattern (fv_fill_pattern_host): (fptr, fcol, amap, fill)."""
+    ip = C.POINTER(C.c_int32)
+    ptr = np.ascontiguousarray(row_ptr, np.int32)
+    col = np.ascontiguousarray(cols, np.int32)
+    n = len(ptr) - 1
+    nnz = C.c_int64()
+    check(lib().fv_fill_pattern_host(kind, int(level), n, ptr.ctypes.data_as(ip), col.ctypes.data_as(ip),
+                                     C.byref(nnz), None, None, None, None), "fill pattern")
+    fptr = np.zeros(n + 1, np.int32)
+    fcol = np.zeros(max(nnz.value, 1), np.int32)
+    amap = np.zeros(max(len(col), 1), np.int32)
+    fill = np.zeros(max(nnz.value, 1), np.uint8)
+    check(lib().fv_fill_pattern_host(kind, int(level), n, ptr.ctypes.data_as(ip), col.ctypes.data_as(ip),
+                                     C.byref(nnz), fptr.ctypes.data_as(ip), fcol.ctypes.data_as(ip),
+                                     amap.ctypes.data_as(ip), fill.ctypes.data_as(C.POINTER(C.c_uint8))),
+          "fill pattern")
+    return fptr, fcol[:nnz.value], amap[:len(col)], fill[:nnz.value]
+
+
 class IncompleteCholesky(Preconditioner):
     def __init__(self, handle, n, matrix):
         self.handle, self.n, self._m = handle, n, matrix
+
+    @staticmethod
+    def fill_pattern(row_ptr, cols, level: int):
+        """The IC(level) factor pattern from_matrix builds (row_i_sparsity_edit,
+        incomplete_cholesky.rs:35-85), from a host CSR pattern: (fptr, fcol,
+        amap = position of every entry of A, fill = 1 for fill entries)."""
+        return _fill_pattern(1, level, row_ptr, cols)
 
     @classmethod
     def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteCholesky":
@@ -373,6 +400,13 @@ class IncompleteCholesky(Preconditioner):
 class IncompleteLowerUpper(Preconditioner):
     def __init__(self, handle, n, matrix):
         self.handle, self.n, self._m = handle, n, matrix
+
+    @staticmethod
+    def fill_pattern(row_ptr, cols, level: int):
+        """The ILU(level) factor pattern from_matrix builds (row_i_l_sparsity /
+        row_i_u_sparsity, incomplete_lower_upper.rs:30-137), from a host CSR
+        pattern: (fptr, fcol, amap = position of every entry of A)."""
+        return _fill_pattern(2, level, row_ptr, cols)[:3]
 
     @classmethod
     def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteLowerUpper":

@@ -375,6 +375,16 @@ fv_status fv_precond_destroy(fv_precond *P);
 fv_status fv_tile_plan_host(int64_t n, int32_t dim, const double *cell, const int32_t *row_ptr,
                             const int32_t *cols, int32_t direction, int64_t *sizes, int32_t *box_step,
                             int32_t *sptr, int32_t *trow, int32_t *dsrc, double *stats);
+/* The level-k factor pattern fv_ic_factor (kind 1) / fv_ilu_factor (kind 2)
+ * build, computed from a host CSR pattern (n rows, sorted columns): the
+ * depth-first walks of IncompleteCholesky's row_i_sparsity_edit
+ * (incomplete_cholesky.rs:35-85) and IncompleteLowerUpper's row_i_l_sparsity /
+ * row_i_u_sparsity (incomplete_lower_upper.rs:30-137), rows sorted.  Call
+ * with fcol == NULL to receive *nnz only; then fptr (n + 1), fcol (*nnz) and,
+ * optionally, amap (row_ptr[n]: position of every entry of A in the pattern)
+ * and fill (*nnz, kind 1 only: 1 for entries that are not entries of A). */
+fv_status fv_fill_pattern_host(int32_t kind, int32_t level, int64_t n, const int32_t *row_ptr, const int32_t *cols,
+                               int64_t *nnz, int32_t *fptr, int32_t *fcol, int32_t *amap, uint8_t *fill);
 
 /* conjugate_gradient / bi_conjugate_gradient_stab.  x is the initial guess on
  * input and the solution on output (device vectors).  P may be NULL (identity). */

@@ -112,3 +112,32 @@ def test_ilu1_factor_and_iterations(fv, orc):
                          maxit=2000)
     _, i1 = orc.bicgstab(ptr, cols, vals, p1, rhs, rtol=1e-10, atol=1e-10, maxit=2000)
     assert i1["iterations"] < i0["iterations"]
+
+
+@pytest.mark.parametrize("kind,level", [("ilu", 1), ("ilu", 2), ("ic", 2), ("ic", 3)])
+def test_library_fill_pattern_equals_oracle(fv, orc, kind, level):
+    """The library's own walk (rows split over host threads, joined in row
+    order) gives the oracle's arrays; amap places every entry of A."""
+    case = convdiff_3d(fv, 12, seed=7) if kind == "ilu" else diffusion_2d(fv, 40, seed=7)
+    ptr, cols, vals, _ = oracle_system(orc, case)
+    fptr, fcol, fill = orc.fill_pattern(kind, level, ptr, cols)
+    cls = fv.IncompleteLowerUpper if kind == "ilu" else fv.IncompleteCholesky
+    got = cls.fill_pattern(ptr, cols, level)
+    assert np.array_equal(got[0], fptr) and np.array_equal(got[1], fcol)
+    if kind == "ic":
+        assert np.array_equal(got[3], fill)
+    amap = got[2]
+    rows = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    assert np.array_equal(fcol[amap], cols)
+    assert (amap >= fptr[rows]).all() and (amap < fptr[rows + 1]).all()
+
+
+def test_library_fill_pattern_rejects_bad_patterns(fv):
+    from fvb200._lib import FvError
+    ptr = np.array([0, 2, 4], np.int32)
+    with pytest.raises(FvError):
+        fv.IncompleteLowerUpper.fill_pattern(ptr, np.array([1, 0, 0, 1], np.int32), 1)  # unsorted row
+    with pytest.raises(FvError):
+        fv.IncompleteLowerUpper.fill_pattern(ptr, np.array([0, 2, 0, 1], np.int32), 1)  # column out of range
+    empty = fv.IncompleteLowerUpper.fill_pattern(np.zeros(1, np.int32), np.zeros(0, np.int32), 1)
+    assert len(empty[0]) == 1 and len(empty[1]) == 0
