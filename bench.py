@@ -758,7 +758,7 @@ def serve_arm(args, rank, world, local_rank):
 
     from fvb200.serve import solve_wave
     srv = Server(fv, workers=args.serve_workers, max_wave_cells=args.serve_wave_cells,
-                 max_wave_requests=args.serve_wave_requests,
+                 max_wave_requests=args.serve_wave_requests, wave_order=args.serve_wave_order,
                  solve_fn=functools.partial(solve_wave, precision=args.serve_precision))
     t0 = time.time()
     keys = sorted({(r.kind, r.side) for r in reqs})
@@ -811,7 +811,7 @@ def serve_arm(args, rank, world, local_rank):
                    "mix": "50% 2D diffusion (CG+IC0) / 50% 3D convection-diffusion (BiCGStab+ILU0)",
                    "sizes": "lognormal, 1st/99th pct 10k/2M cells, clipped; 2D sides x16, 3D sides x4",
                    "workers": args.serve_workers, "max_wave_cells": args.serve_wave_cells,
-                   "max_wave_requests": args.serve_wave_requests,
+                   "max_wave_requests": args.serve_wave_requests, "wave_order": args.serve_wave_order,
                    "outer_tolerance": 1e-10},
         "p50_ms": round(stats["p50_ms"], 1) if stats["p50_ms"] is not None else None,
         "p99_ms": round(stats["p99_ms"], 1) if stats["p99_ms"] is not None else None,
@@ -883,6 +883,7 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=2)
     ap.add_argument("--serve-wave-cells", type=int, default=48_000_000)
     ap.add_argument("--serve-wave-requests", type=int, default=512)
+    ap.add_argument("--serve-wave-order", default="size", choices=["size", "fifo"])
     ap.add_argument("--serve-time-limit", type=float, default=600.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -12,6 +12,15 @@ immediately takes the next admitted requests (slots are refilled as they
 free up).  Per-problem reductions never mix problems, so a request's result
 is the same alone and in any wave.
 
+A wave lasts as long as its slowest problem, which grows with the problem's
+size, and every request of a wave completes when the wave does.  With
+wave_order "size" (the default) waves are therefore built from one size
+class: worker 0 takes the largest admitted requests first (the longest solves
+start at once, which keeps the stream's span short), the other workers the
+smallest (short waves, so most requests complete early); a request that has
+waited longer than `aging_s` is taken first by any worker.  wave_order "fifo"
+packs requests in arrival order.
+
 Meshes are built on the host per (kind, size) and cached; the request's seed
 drives its diffusivity and source fields.
 """
@@ -166,7 +175,13 @@ class Server:
     it is a parameter so the scheduling can be exercised without a GPU."""
 
     def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
-                 max_wave_requests: int = 512, solve_fn=None, make_stream=None):
+                 max_wave_requests: int = 512, solve_fn=None, make_stream=None, wave_order: str = "size",
+                 size_ratio: float = 4.0, aging_s: float = 5.0):
+        if wave_order not in ("size", "fifo"):
+            raise ValueError(f"wave_order must be 'size' or 'fifo', not {wave_order!r}")
+        self.wave_order = wave_order
+        self.size_ratio = float(size_ratio)
+        self.aging_s = float(aging_s)
         self.fv = fv
         self.cache = MeshCache(fv)
         self.workers = workers
@@ -192,6 +207,35 @@ class Server:
 
     def _cost(self, r: Request) -> int:
         return BYTES_PER_CELL[r.kind] * r.cells
+
+    def _take_wave(self, worker: int, now: float) -> list[Request]:
+        """Remove the next wave from self.admitted (caller holds the lock)."""
+        q = self.admitted
+        if self.wave_order == "fifo" or now - q[0].arrival > self.aging_s:
+            kind = q[0].kind
+            order = [r for r in q if r.kind == kind]
+            fits = lambda r, first: True  # noqa: E731
+        elif worker == 0:  # the largest requests, down to size_ratio below the largest
+            kind = max(q, key=lambda r: r.cells).kind
+            order = sorted((r for r in q if r.kind == kind), key=lambda r: -r.cells)
+            fits = lambda r, first: r.cells * self.size_ratio >= first.cells  # noqa: E731
+        else:  # the smallest requests, up to size_ratio above the smallest
+            kind = min(q, key=lambda r: r.cells).kind
+            order = sorted((r for r in q if r.kind == kind), key=lambda r: r.cells)
+            fits = lambda r, first: r.cells <= first.cells * self.size_ratio  # noqa: E731
+        wave, cells = [], 0
+        for r in order:
+            if len(wave) == self.max_wave_requests:
+                break
+            if wave and (cells + r.cells > self.max_wave_cells or not fits(r, wave[0])):
+                if self.wave_order == "fifo":
+                    continue
+                break
+            wave.append(r)
+            cells += r.cells
+        taken = {id(r) for r in wave}
+        self.admitted = collections.deque(r for r in q if id(r) not in taken)
+        return wave
 
     def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True) -> dict:
         """Serve `requests` (arrival times relative to now).  Returns latency and
@@ -221,7 +265,7 @@ class Server:
                         pass
                 time.sleep(0.0005)
 
-        def worker():
+        def worker(index):
             stream = self.make_stream()
             while True:
                 with self.lock:
@@ -229,18 +273,7 @@ class Server:
                         self.lock.wait(0.01)
                     if stop.is_set() and not self.admitted:
                         return
-                    kind = self.admitted[0].kind
-                    wave, cells = [], 0
-                    rest = collections.deque()
-                    while self.admitted and len(wave) < self.max_wave_requests:
-                        r = self.admitted.popleft()
-                        if r.kind == kind and (cells + r.cells <= self.max_wave_cells or not wave):
-                            wave.append(r)
-                            cells += r.cells
-                        else:
-                            rest.append(r)
-                    rest.extend(self.admitted)
-                    self.admitted = rest
+                    wave = self._take_wave(index, time.perf_counter() - t0)
                     wid = self.waves
                     self.waves += 1
                 start = time.perf_counter() - t0
@@ -264,7 +297,7 @@ class Server:
                     self.lock.notify_all()
 
         adm = threading.Thread(target=admit_loop, daemon=True)
-        ws = [threading.Thread(target=worker, daemon=True) for _ in range(self.workers)]
+        ws = [threading.Thread(target=worker, args=(k,), daemon=True) for k in range(self.workers)]
         adm.start()
         for w in ws:
             w.start()
