@@ -176,7 +176,7 @@ class Server:
 
     def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
                  max_wave_requests: int = 512, solve_fn=None, make_stream=None, wave_order: str = "size",
-                 size_ratio: float = 4.0, aging_s: float = 5.0):
+                 size_ratio: float = 4.0, aging_s: float = 30.0):
         if wave_order not in ("size", "fifo"):
             raise ValueError(f"wave_order must be 'size' or 'fifo', not {wave_order!r}")
         self.wave_order = wave_order
