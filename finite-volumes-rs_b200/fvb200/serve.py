@@ -19,7 +19,9 @@ class: worker 0 takes the largest admitted requests first (the longest solves
 start at once, which keeps the stream's span short), the other workers the
 smallest (short waves, so most requests complete early); a request that has
 waited longer than `aging_s` is taken first by any worker.  wave_order "fifo"
-packs requests in arrival order.
+packs requests in arrival order.  A wave is formed once its oldest request
+has waited `batch_window_s` (or the admitted requests fill a wave, or no
+more requests are due), so a wave does not start with the first arrival alone.
 
 Meshes are built on the host per (kind, size) and cached; the request's seed
 drives its diffusivity and source fields.
@@ -176,12 +178,14 @@ class Server:
 
     def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
                  max_wave_requests: int = 512, solve_fn=None, make_stream=None, wave_order: str = "size",
-                 size_ratio: float = 4.0, aging_s: float = 30.0):
+                 size_ratio: float = 4.0, aging_s: float = 30.0,
+                 batch_window_s: float = 0.05):
         if wave_order not in ("size", "fifo"):
             raise ValueError(f"wave_order must be 'size' or 'fifo', not {wave_order!r}")
         self.wave_order = wave_order
         self.size_ratio = float(size_ratio)
         self.aging_s = float(aging_s)
+        self.batch_window_s = float(batch_window_s)
         self.fv = fv
         self.cache = MeshCache(fv)
         self.workers = workers
@@ -269,8 +273,17 @@ class Server:
             stream = self.make_stream()
             while True:
                 with self.lock:
-                    while not self.admitted and not stop.is_set():
-                        self.lock.wait(0.01)
+                    while not stop.is_set():
+                        if self.admitted:
+                            # a batching window: the oldest request waits up to
+                            # batch_window_s for others to join its wave
+                            wait = self.admitted[0].arrival + self.batch_window_s - (time.perf_counter() - t0)
+                            full = sum(r.cells for r in self.admitted) >= self.max_wave_cells
+                            if wait <= 0 or full or not pending:
+                                break
+                            self.lock.wait(min(wait, 0.01))
+                        else:
+                            self.lock.wait(0.01)
                     if stop.is_set() and not self.admitted:
                         return
                     wave = self._take_wave(index, time.perf_counter() - t0)

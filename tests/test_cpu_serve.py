@@ -117,3 +117,18 @@ def test_wave_order_is_checked(fv):
     from fvb200.serve import Server
     with pytest.raises(ValueError):
         Server(fv, budget_bytes=1, solve_fn=lambda *a: None, make_stream=_Stream, wave_order="random")
+
+
+def test_batching_window_groups_early_arrivals(fv):
+    """The first arrival waits up to batch_window_s for requests that arrive
+    right after it, so they share its wave."""
+    from fvb200.serve import Request, Server
+    reqs = [Request(0, 0.0, "2d", 10, 0, cells=1000)] + [Request(k, 0.02, "2d", 10, k, cells=1000)
+                                                          for k in range(1, 6)]
+
+    def solve(fv, cache, wave, stream):
+        time.sleep(0.01)
+
+    srv = Server(fv, workers=1, budget_bytes=1 << 40, solve_fn=solve, make_stream=_Stream, batch_window_s=0.1)
+    stats = srv.run(reqs, time_limit=30.0, warm=False)
+    assert stats["completed"] == 6 and stats["waves"] == 1
