@@ -145,10 +145,12 @@ fv_status fv_fill_pattern(int kind, int level, int64_t n, const int32_t *ptr, co
                           std::vector<int32_t> &fptr, std::vector<int32_t> &fcol, std::vector<int32_t> &amap,
                           std::vector<uint8_t> &fill) {
     try {
-        // one range per thread, at least 256 rows each, at most 16 threads
-        // (each holds 4 bytes of visited marks per row of A)
+        // one range per thread, at least 256 rows each, at most 16 threads;
+        // each thread holds 4 bytes of visited marks per row of A, and all
+        // threads' marks together stay within 1 GiB
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const int64_t nt = std::max<int64_t>(1, std::min<int64_t>({(int64_t)hw, 16, n / 256}));
+        const int64_t by_memory = (int64_t(1) << 30) / std::max<int64_t>(1, 4 * n);
+        const int64_t nt = std::max<int64_t>(1, std::min<int64_t>({(int64_t)hw, 16, n / 256, by_memory}));
         std::vector<Part> parts((size_t)nt);
         for (int64_t p = 0; p < nt; ++p) {
             parts[(size_t)p].r0 = n * p / nt;
