@@ -525,6 +525,28 @@ fv_status apply_or_copy(fv_precond *P, const double *r, double *z, int64_t n, in
 
 int batch_size(int64_t n) { return n >= (1 << 20) ? 4 : 8; }
 
+// One pinned int per host thread for the done flag of loop_until_done,
+// allocated on first use and kept for the thread's life (freeing pinned
+// memory may synchronise the device); nullptr if it cannot be allocated.
+int *pinned_flag() {
+    struct Holder {
+        int *p = nullptr;
+        bool tried = false;
+        ~Holder() {
+            if (p) cudaFreeHost(p);
+        }
+    };
+    thread_local Holder h;
+    if (!h.tried) {
+        h.tried = true;
+        if (cudaHostAlloc((void **)&h.p, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+            h.p = nullptr;
+            cudaGetLastError();
+        }
+    }
+    return h.p;
+}
+
 // Runs body(stream) -- one batch of iterations -- until the device state says
 // done.  The batch is captured once into a CUDA graph on a private stream (the
 // legacy default stream cannot be captured) and replayed, so the GPU runs the
@@ -555,7 +577,46 @@ fv_status loop_until_done(const Workspace &w, cudaStream_t st, Body body, Solver
         cudaGetLastError();
     }
     fv_status s = FV_OK;
-    if (graph_ok) {
+    int *done_h = pinned_flag();
+    cudaEvent_t evd = nullptr;
+    if (graph_ok && done_h && cudaEventCreateWithFlags(&evd, cudaEventDisableTiming) == cudaSuccess) {
+        // The next replay is queued before the host waits for the previous
+        // replay's done flag (copied into pinned memory behind it), so the GPU
+        // does not idle while the host reads, nor while its thread is
+        // descheduled.  One replay may run after convergence: its kernels see
+        // the done flag and return at once, so the results do not change.
+        auto replay = [&]() -> fv_status {
+            const cudaError_t e = cudaGraphLaunch(gx, cs);
+            if (e != cudaSuccess) {
+                fv_internal_set_cuda_error(e, "cudaGraphLaunch");
+                return FV_ERR_CUDA;
+            }
+            fv_note_launches(per_replay);
+            return FV_OK;
+        };
+        auto flag_after = [&]() -> fv_status {
+            FV_CUDA_TRY(cudaMemcpyAsync(done_h, &w.S->done, sizeof(int), cudaMemcpyDeviceToHost, cs));
+            FV_CUDA_TRY(cudaEventRecord(evd, cs));
+            return FV_OK;
+        };
+        s = replay();
+        if (s == FV_OK) s = flag_after();
+        while (s == FV_OK) {
+            s = replay();
+            if (s != FV_OK) break;
+            const cudaError_t e = cudaEventSynchronize(evd);
+            if (e != cudaSuccess) {
+                fv_internal_set_cuda_error(e, "cudaEventSynchronize");
+                s = FV_ERR_CUDA;
+                break;
+            }
+            if (*(volatile int *)done_h) break;
+            s = flag_after();
+        }
+        if (s == FV_OK) s = read_state(w, h, cs);
+        cudaEventRecord(ev, cs);
+        cudaStreamWaitEvent(st, ev, 0);
+    } else if (graph_ok) {
         while (true) {
             cudaError_t e = cudaGraphLaunch(gx, cs);
             if (e != cudaSuccess) {
@@ -577,6 +638,7 @@ fv_status loop_until_done(const Workspace &w, cudaStream_t st, Body body, Solver
             if (s != FV_OK || h.done) break;
         }
     }
+    if (evd) cudaEventDestroy(evd);
     if (gx) cudaGraphExecDestroy(gx);
     if (ev) cudaEventDestroy(ev);
     if (cs) cudaStreamDestroy(cs);
