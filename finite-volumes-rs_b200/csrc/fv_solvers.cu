@@ -769,9 +769,10 @@ extern "C" fv_status fv_bicgstab_host(const fv_csr *A, fv_precond *P, const doub
 // ------------------------------------------------------------------ fv_cg_noalloc
 // Allocation-free conjugate gradient.  fv_cg takes its Krylov workspace from
 // cudaMallocAsync on every call; this variant takes it from one statically
-// sized device array that the CUDA module reserves when the library is loaded
-// on a GPU.  It launches the same kernels in the same order as fv_cg, so its
-// results are the same bits.
+// sized device array that is created when this file's CUDA module is loaded on
+// a device (under lazy module loading, the CUDA 12 default: at the first
+// launch from, or symbol lookup in, this module on that device).  It launches
+// the same kernels in the same order as fv_cg, so its results are the same bits.
 namespace {
 constexpr int64_t kNoAllocMaxRows = FV_NOALLOC_MAX_ROWS;
 constexpr int64_t kNoAllocMaxHist = FV_NOALLOC_MAX_ITERATIONS + 3;
@@ -786,23 +787,62 @@ constexpr size_t kNoAllocBytes =
 // device address.
 static __device__ __align__(256) unsigned char g_cg_noalloc_scratch[kNoAllocBytes];
 
+#include <cuda.h>  // CUcontext / CUresult types only; the driver calls are reached through the runtime
+
 #include <mutex>
 static std::mutex g_cg_noalloc_mu;
-static void *g_cg_noalloc_addr[256];
+struct NoAllocSlot {
+    void *addr = nullptr;
+    unsigned long long ctx_id = 0;  // unique id of the context the address belongs to (0: none yet)
+};
+static NoAllocSlot g_cg_noalloc_slot[256];
 
-// Device address of the scratch array on the current device, looked up once
-// per device (with that device current) and cached.
+// Unique id of the calling thread's current context (cuCtxGetId, unique over
+// the process's life), or 0 when the driver does not provide it.
+static unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device.  Set-up runs
+// once per device, with that device current: cudaGetSymbolAddress, checked.
+// The address is kept together with the id of the context it belongs to and
+// looked up again when that context has been replaced (cudaDeviceReset, or a
+// primary context released and re-created), so a stale address is never used.
 static fv_status cg_noalloc_scratch(void **out) {
     int dev = -1;
     FV_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return FV_ERR_INVALID;
+    const unsigned long long ctx = current_context_id();  // 0 while no context is current on this thread
     std::lock_guard<std::mutex> lock(g_cg_noalloc_mu);
-    if (!g_cg_noalloc_addr[dev]) {
+    NoAllocSlot &slot = g_cg_noalloc_slot[dev];
+    if (!slot.addr || ctx == 0 || slot.ctx_id != ctx) {
         void *p = nullptr;
-        FV_CUDA_TRY(cudaGetSymbolAddress(&p, g_cg_noalloc_scratch));
-        g_cg_noalloc_addr[dev] = p;
+        FV_CUDA_TRY(cudaGetSymbolAddress(&p, g_cg_noalloc_scratch));  // makes the primary context current
+        slot.addr = p;
+        slot.ctx_id = current_context_id();
     }
-    *out = g_cg_noalloc_addr[dev];
+    *out = slot.addr;
     return FV_OK;
 }
 

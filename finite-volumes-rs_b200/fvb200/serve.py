@@ -92,22 +92,44 @@ class MeshCache:
         self.d = collections.OrderedDict()
         self.cells = 0
         self.lock = threading.Lock()
+        self.building = {}  # key -> Event of the one thread building that mesh
+
+    def _build(self, kind, side):
+        return (self.fv.Mesh.square(side, 0.2, 17 + side, on_device=self.on_device) if kind == "2d"
+                else self.fv.Mesh.cube(side, 0.15, 17 + side, on_device=self.on_device))
 
     def get(self, kind, side):
+        """The mesh of (kind, side): built by the first thread that asks for it
+        (outside the lock); threads asking for the same key meanwhile wait for
+        that build instead of building it again, so each mesh is built, counted
+        and inserted once."""
         key = (kind, side)
-        with self.lock:
-            if key in self.d:
-                self.d.move_to_end(key)
-                return self.d[key]
-        m = (self.fv.Mesh.square(side, 0.2, 17 + side, on_device=self.on_device) if kind == "2d"
-             else self.fv.Mesh.cube(side, 0.15, 17 + side, on_device=self.on_device))
-        with self.lock:
-            self.d[key] = m
-            self.cells += m.n_cells
-            while self.cells > self.cap and len(self.d) > 1:
-                _, old = self.d.popitem(last=False)
-                self.cells -= old.n_cells
-        return m
+        while True:
+            with self.lock:
+                if key in self.d:
+                    self.d.move_to_end(key)
+                    return self.d[key]
+                ev = self.building.get(key)
+                owner = ev is None
+                if owner:
+                    ev = threading.Event()
+                    self.building[key] = ev
+            if not owner:
+                ev.wait()
+                continue  # built (or its build failed: then this thread tries)
+            try:
+                m = self._build(kind, side)
+                with self.lock:
+                    self.d[key] = m
+                    self.cells += m.n_cells
+                    while self.cells > self.cap and len(self.d) > 1:
+                        _, old = self.d.popitem(last=False)
+                        self.cells -= old.n_cells
+                return m
+            finally:
+                with self.lock:
+                    del self.building[key]
+                ev.set()
 
 
 def request_fields(m, req: Request):

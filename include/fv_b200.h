@@ -458,11 +458,21 @@ fv_status fv_batch_destroy(fv_batch *B);
  *
  * Limits: at most FV_NOALLOC_MAX_ROWS rows and FV_NOALLOC_MAX_ITERATIONS
  * iterations; larger requests return FV_ERR_INVALID (fv_last_error() names
- * the limit).  The array (about 8.6 MB) is reserved on every GPU that loads
- * the library and held until the process exits.
+ * the limit).  The array (about 8.6 MB) belongs to the solvers' CUDA module
+ * and is held until the process exits on every GPU where that module is
+ * loaded.  Under lazy module loading (the CUDA 12 default,
+ * CUDA_MODULE_LOADING=LAZY) the module, and with it the array, is created on
+ * a device at the first solver call there (fv_cg, fv_bicgstab or this one),
+ * so that first call does take device memory: make one call on each device
+ * before the phase in which nothing may be allocated (with
+ * CUDA_MODULE_LOADING=EAGER the array is created when the library's kernels
+ * are loaded).
  * The first call on each device looks up the array's device address with
  * cudaGetSymbolAddress (that device must be current); make that first call
- * before any stream capture.  All calls share the one array: calls that
+ * before any stream capture.  The address is looked up again when the
+ * device's context has been replaced (cudaDeviceReset), so a reset never
+ * leaves a stale address behind; every handle made before the reset (A, P)
+ * is invalid after it, as for the rest of this library.  All calls share the one array: calls that
  * overlap on the GPU (other streams, other host threads) race and must be
  * serialised by the caller.  info->device_ms is left at 0.  A and P are
  * created beforehand by the allocating calls (fv_assemble / fv_csr_create_host,

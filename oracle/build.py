@@ -12,7 +12,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SRC = [HERE / "oracle.c", HERE / "oracle_mpi.c"]
+SRC = [HERE / "oracle.c", HERE / "oracle_mpi.c", HERE / "oracle_mesh.c"]
 
 
 def build(force: bool = False) -> Path:

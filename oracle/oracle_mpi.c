@@ -269,3 +269,186 @@ done:
     free(part);
     return 0;
 }
+
+/* ------------------------------------------------------------ assembly per rank
+ * What each rank does in assemble (fvm/assembly.rs:11-78) for its own cells:
+ * rank t owns the rows [lo_t, hi_t) (contiguous partitions, as above), builds
+ * their sorted cell_to_cell rows (dmatrix.rs:38-50) and adds every face
+ * contribution that lands in them, in ascending face order.  A row therefore
+ * receives the same additions in the same order as in the single-rank oracle
+ * (or_pattern + or_assemble), and every value equals it bit for bit.  Terms:
+ * c_conv*convection(Upwind(F), F) + c_lap*laplacian(Orthogonal, kappa)
+ * + c_src*source(f), boundary closure (bndi, bnde). */
+static int cmp_i32_mpi(const void *a, const void *b) {
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+static int row_pattern(int64_t c, const int32_t *cell_face_ptr, const int32_t *cell_faces, const int32_t *owner,
+                       const int32_t *neighbor, int32_t *tmp) {
+    int len = 0;
+    tmp[len++] = (int32_t)c;
+    for (int32_t k = cell_face_ptr[c]; k < cell_face_ptr[c + 1]; ++k) {
+        const int32_t f = cell_faces[k], nb = neighbor[f];
+        if (nb < 0) continue;
+        const int32_t other = (nb == (int32_t)c) ? owner[f] : nb;
+        int dup = 0;
+        for (int q = 1; q < len; ++q)
+            if (tmp[q] == other) dup = 1;
+        if (!dup) {
+            if (len >= 64) return -1;
+            tmp[len++] = other;
+        }
+    }
+    qsort(tmp, (size_t)len, sizeof(int32_t), cmp_i32_mpi);
+    return len;
+}
+
+/* Pattern on P threads: cols == NULL only counts (returns nnz in *nnz_out). */
+int or_pattern_par(int64_t n_cells, const int32_t *cell_face_ptr, const int32_t *cell_faces, const int32_t *owner,
+                   const int32_t *neighbor, int P, int32_t *row_ptr, int32_t *cols, int64_t *nnz_out) {
+    int bad = 0;
+    if (!cols) {
+#pragma omp parallel for num_threads(P) schedule(static) reduction(| : bad)
+        for (int64_t c = 0; c < n_cells; ++c) {
+            int32_t tmp[64];
+            const int len = row_pattern(c, cell_face_ptr, cell_faces, owner, neighbor, tmp);
+            if (len < 0) bad = 1;
+            row_ptr[c + 1] = len < 0 ? 0 : len;
+        }
+        if (bad) return 2;
+        row_ptr[0] = 0;
+        for (int64_t c = 0; c < n_cells; ++c) row_ptr[c + 1] += row_ptr[c];
+        *nnz_out = row_ptr[n_cells];
+        return 0;
+    }
+#pragma omp parallel for num_threads(P) schedule(static)
+    for (int64_t c = 0; c < n_cells; ++c) {
+        int32_t tmp[64];
+        const int len = row_pattern(c, cell_face_ptr, cell_faces, owner, neighbor, tmp);
+        for (int q = 0; q < len; ++q) cols[row_ptr[c] + q] = tmp[q];
+    }
+    *nnz_out = row_ptr[n_cells];
+    return 0;
+}
+
+static int64_t find_mpi(const int32_t *ptr, const int32_t *col, int64_t i, int32_t j) {
+    int64_t lo = ptr[i], hi = ptr[i + 1];
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (col[mid] < j)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return (lo < ptr[i + 1] && col[lo] == j) ? lo : -1;
+}
+
+int or_assemble_par(int32_t dim, int64_t n_cells, int64_t n_faces, int64_t n_bfaces, const int32_t *owner,
+                    const int32_t *neighbor, const double *area, const double *face_center,
+                    const double *cell_center, const double *volume, double c_lap, double c_conv, double c_src,
+                    const double *kappa, const double *flux, const double *source, const double *bndi,
+                    const double *bnde, const int32_t *row_ptr, const int32_t *cols, int P, double *vals,
+                    double *rhs) {
+    const int64_t fb0 = n_faces - n_bfaces;
+    int bad = 0;
+#pragma omp parallel num_threads(P) reduction(| : bad)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const int64_t lo = n_cells * t / nt, hi = n_cells * (t + 1) / nt;
+        for (int64_t k = row_ptr[lo]; k < row_ptr[hi]; ++k) vals[k] = 0.0;
+        /* cell loop (assembly.rs:26-32) */
+        for (int64_t c = lo; c < hi; ++c) {
+            const double l = 0.0;
+            const double r = c_src != 0.0 ? c_src * (-source[c]) : 0.0;
+            const int64_t kd = find_mpi(row_ptr, cols, c, (int32_t)c);
+            if (kd < 0) {
+                bad = 1;
+                continue;
+            }
+            vals[kd] = l * volume[c];
+            rhs[c] = r * volume[c];
+        }
+        /* face loop (assembly.rs:35-75), contributions to own rows only */
+        for (int64_t f = 0; f < n_faces && !bad; ++f) {
+            const int64_t i = owner[f], j = neighbor[f];
+            const int own_i = i >= lo && i < hi, own_j = j >= lo && j < hi;
+            if (!own_i && !own_j) continue;
+            const double *ci = cell_center + i * dim;
+            const double *cj = j >= 0 ? cell_center + j * dim : face_center + f * dim;
+            double dvec[3], dd = 0.0;
+            for (int d = 0; d < dim; ++d) dvec[d] = cj[d] - ci[d];
+            for (int d = 0; d < dim; ++d) dd += dvec[d] * dvec[d];
+            const double tt = 1.0 / sqrt(dd); /* Orthogonal (orthogonal.rs:26-46) */
+            double lap0 = 0.0, lap1 = 0.0, conv0 = 0.0, conv1 = 0.0;
+            if (c_lap != 0.0) {
+                lap0 = kappa[f] * (-tt);
+                lap1 = kappa[f] * tt;
+            }
+            if (c_conv != 0.0) { /* Upwind (upwind.rs:26-33) */
+                const double F = flux[f];
+                if (F > 0.0) {
+                    conv0 = 1.0 * F;
+                    conv1 = 0.0 * F;
+                } else {
+                    conv0 = 0.0 * F;
+                    conv1 = 1.0 * F;
+                }
+            }
+            double li, lj;
+            if (c_conv != 0.0 && c_lap != 0.0) {
+                li = c_conv * conv0 + c_lap * lap0;
+                lj = c_conv * conv1 + c_lap * lap1;
+            } else if (c_lap != 0.0) {
+                li = c_lap * lap0;
+                lj = c_lap * lap1;
+            } else {
+                li = c_conv * conv0;
+                lj = c_conv * conv1;
+            }
+            const double r = 0.0;
+            li = li * area[f];
+            lj = lj * area[f];
+            const double ra = r * area[f];
+            if (j >= 0) {
+                if (own_i) {
+                    const int64_t kii = find_mpi(row_ptr, cols, i, (int32_t)i);
+                    const int64_t kij = find_mpi(row_ptr, cols, i, (int32_t)j);
+                    if (kii < 0 || kij < 0) {
+                        bad = 1;
+                        continue;
+                    }
+                    vals[kii] += li;
+                    vals[kij] += lj;
+                    rhs[i] += ra;
+                }
+                if (own_j) {
+                    const int64_t kji = find_mpi(row_ptr, cols, j, (int32_t)i);
+                    const int64_t kjj = find_mpi(row_ptr, cols, j, (int32_t)j);
+                    if (kji < 0 || kjj < 0) {
+                        bad = 1;
+                        continue;
+                    }
+                    vals[kji] -= li;
+                    vals[kjj] -= lj;
+                    rhs[j] -= ra;
+                }
+            } else {
+                if (f < fb0) {
+                    bad = 1;
+                    continue;
+                }
+                const double bi = bndi[f - fb0], be = bnde[f - fb0];
+                const int64_t kii = find_mpi(row_ptr, cols, i, (int32_t)i);
+                if (kii < 0) {
+                    bad = 1;
+                    continue;
+                }
+                vals[kii] += li;
+                vals[kii] += lj * bi;
+                rhs[i] += ra - lj * be;
+            }
+        }
+    }
+    return bad ? 2 : 0;
+}

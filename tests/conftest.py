@@ -1,9 +1,23 @@
+import os
 import sys
 from pathlib import Path
 
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
+
+
+def reference_file(rel: str):
+    """A file of the reference checkout named by the FV_REFERENCE_DIR
+    environment variable, or None when the variable is unset or the file is
+    absent (tests that need it skip)."""
+    base = os.environ.get("FV_REFERENCE_DIR")
+    if not base:
+        return None
+    p = Path(base) / rel
+    return p if p.exists() else None
+
+
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "finite-volumes-rs_b200"))
 

@@ -1,6 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the CPU oracle.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (FV_REFERENCE_DIR=<reference checkout> also
+                                                   writes square_su2_input.npz)
 
 The reference crate cannot be built in this environment (no Rust toolchain,
 no MPI), so these vectors come from the oracle (oracle/oracle.c, a
@@ -47,7 +48,36 @@ def compute(fv, orc, name):
     }
 
 
+def square_su2_input():
+    """The parsed contents of the reference's square.su2 (the input of its mesh
+    known-answer test, core/mesh/io.rs:569-590), read from the reference
+    checkout named by FV_REFERENCE_DIR; None when it is not available."""
+    import os
+    from oracle import mesh_ref
+    base = os.environ.get("FV_REFERENCE_DIR")
+    path = Path(base) / "src/core/mesh/examples/square.su2" if base else None
+    if path is None or not path.exists():
+        return None
+    dim, nodes, elements, boundaries = mesh_ref.read_su2(path.read_text())
+    bkeys = list(boundaries.items())
+    return {
+        "dim": np.array(dim), "nodes": np.array(nodes),
+        "elem_kind": np.array([k for k, _ in elements], np.int32),
+        "elem_ptr": np.concatenate([[0], np.cumsum([len(n) for _, n in elements])]).astype(np.int32),
+        "elem_nodes": np.array([v for _, n in elements for v in n], np.int32),
+        "bnd_ptr": np.concatenate([[0], np.cumsum([len(k) for k, _ in bkeys])]).astype(np.int32),
+        "bnd_nodes": np.array([v for k, _ in bkeys for v in k], np.int32),
+        "bnd_marker": np.array([mk for _, mk in bkeys], np.int32),
+    }
+
+
 def main():
+    su2 = square_su2_input()
+    if su2 is not None:
+        np.savez_compressed(HERE / "square_su2_input.npz", **su2)
+        print("square_su2_input", {k: v.shape for k, v in su2.items()})
+    if "--su2-only" in sys.argv:
+        return
     from fvb200.build import build
     build()
     import fvb200 as fv

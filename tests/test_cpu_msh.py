@@ -14,8 +14,9 @@ from pathlib import Path
 
 import numpy as np
 import pytest
+from conftest import reference_file
 
-SQUARE_SU2 = Path("/root/reference/src/core/mesh/examples/square.su2")
+SQUARE_SU2 = reference_file("src/core/mesh/examples/square.su2")
 
 _FIELDS = ("face_node_ptr", "face_nodes", "face_patch", "cell_face_ptr", "cell_faces", "face_owner",
            "face_neighbor", "face_area", "face_normal", "face_center", "cell_center", "cell_volume", "nodes")
@@ -110,7 +111,7 @@ def test_from_faces_equals_element_build(fv):
         _same(m2, m)
 
 
-@pytest.mark.skipif(not SQUARE_SU2.exists(), reason="reference fixture not mounted")
+@pytest.mark.skipif(SQUARE_SU2 is None, reason="FV_REFERENCE_DIR unset: reference checkout not available")
 def test_reference_read_write_square_mesh(fv, tmp_path):
     """io.rs:592-608: square.su2 -> write -> read; 121 nodes, 220 faces, 100 cells,
     total volume 1 and a closed boundary within 10 eps, before and after."""

@@ -132,3 +132,37 @@ def test_batching_window_groups_early_arrivals(fv):
     srv = Server(fv, workers=1, budget_bytes=1 << 40, solve_fn=solve, make_stream=_Stream, batch_window_s=0.1)
     stats = srv.run(reqs, time_limit=30.0, warm=False)
     assert stats["completed"] == 6 and stats["waves"] == 1
+
+
+def test_mesh_cache_builds_each_key_once_under_concurrent_gets():
+    """Threads asking for the same (kind, side) at once get one mesh object,
+    built once, and the cache's cell count holds it once."""
+    import threading
+    import time as _time
+    from types import SimpleNamespace
+
+    from fvb200.serve import MeshCache
+
+    builds = []
+
+    class FakeMesh:
+        @staticmethod
+        def square(side, jitter, seed, on_device=True):
+            builds.append(side)
+            _time.sleep(0.05)  # a slow build: the other threads arrive meanwhile
+            return SimpleNamespace(n_cells=2 * side * side)
+
+    cache = MeshCache(SimpleNamespace(Mesh=FakeMesh), capacity_cells=10_000)
+    got = []
+    ts = [threading.Thread(target=lambda: got.append(cache.get("2d", 16))) for _ in range(6)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert builds == [16]
+    assert len(got) == 6 and all(g is got[0] for g in got)
+    assert cache.cells == 2 * 16 * 16
+    # eviction keeps the count equal to the meshes held
+    cache.get("2d", 40)
+    cache.get("2d", 60)
+    assert cache.cells == sum(m.n_cells for m in cache.d.values()) and cache.cells <= 10_000

@@ -164,7 +164,7 @@ def test_solvers_at_benchmark_tolerance(fv, orc):
     info = fv.conjugate_gradient(x, A, b, fv.IncompleteCholesky.from_matrix(A, 0), None,
                                  fv.LinearSolverOptions(1e-8, 1e-8, 5000))
     assert abs(info.iterations - io["iterations"]) <= 2
-    assert _rel(x.numpy(), xo) <= 1e-10 or info.iterations != io["iterations"]
+    assert _rel(x.numpy(), xo) <= 1e-10
 
 
 def test_identity_preconditioner_and_zero_rhs(fv, orc):
