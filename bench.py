@@ -354,7 +354,10 @@ def gpu_arm(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
     t_spmv = time_kernel(torch, lambda: A.imul(y, x), 20, stream)
     t_prec = time_kernel(torch, lambda: P.precondition(z, b), 10, stream)
-    t_asm = time_kernel(torch, lambda: fv.assemble(eq, bc, mesh, lhs=A), 10, stream)
+    # the assembly kernel alone: the fv_assemble C call with prebuilt descriptors into a preallocated rhs
+    from fvb200.linalg import assembly_launcher
+    b_fixed = fv.DistributedVector.from_size(N)
+    t_asm = time_kernel(torch, assembly_launcher(eq, bc, mesh, A, b_fixed), 10, stream)
     t_fac = time_kernel(torch, lambda: P.refactor(), 3, stream)
     F, Fb = mesh.n_faces, mesh.n_boundary_faces
     bytes_spmv = 12 * nnz + 20 * N

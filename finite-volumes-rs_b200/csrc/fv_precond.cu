@@ -92,6 +92,7 @@ struct fv_precond {
     unsigned epoch = 0;
     int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned);
                                   // 3: level chunks, next chunk prefetched
+    int sweep_blocks = 0;         // blocks of 8 warps per sweep launch (0: sweep_grid's choice)
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
@@ -104,6 +105,13 @@ struct fv_precond {
     const fv_csr *orig = nullptr;
     int32_t *amap = nullptr;
     int level = 0;
+    // reordered factorisation (fv_*_factor_perm): `fill` is B = Q A Q^T, perm[i]
+    // = the row of A that is B's row i; the sweeps gather the right-hand side
+    // through perm and scatter the result back, the backward sweep's own output
+    // (B's numbering, polled by its dependants) lives in zint / zint32
+    int32_t *perm = nullptr;
+    double *zint = nullptr;
+    float *zint32 = nullptr;
     // box-tiled sweeps: per-slot records (factor values in slot order) and
     // slot-ordered right-hand sides, FP64 and FP32; rebuilt when the factors change
     void *t_rec64[2] = {nullptr, nullptr}, *t_rec32[2] = {nullptr, nullptr};
@@ -760,21 +768,35 @@ __device__ __forceinline__ bool fv_slot_ready<float>(const float *p, float &v) {
     return b != FV_SENTINEL_U32;
 }
 
+// The permutation of a reordered factorisation (fv_ilu0_factor_perm and
+// friends): the factor's row i is row nat[i] of the caller's vectors.  The
+// forward sweep reads its right-hand side at nat[i] (gather); the backward
+// sweep also stores its result at out[nat[i]] (scatter).  Row groups of a
+// batch are indexed in the caller's numbering.  nat == nullptr: no
+// permutation.
+template <typename T>
+struct SweepPerm {
+    const int32_t *nat = nullptr;
+    bool gather = false;
+    T *out = nullptr;
+};
+
 template <typename T, bool UNIT, int MAXL>
 __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restrict__ order,
                                                const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                const T *__restrict__ val, const T *__restrict__ dinv,
                                                const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
-                                               int *err, const int *skip, fv_row_skip rs) {
+                                               int *err, const int *skip, fv_row_skip rs, SweepPerm<T> pm) {
     if (skip && *(volatile const int *)skip) return;  // a converged solve: no warp takes a ticket
     const int64_t nchunks = (n + 31) / 32;
     int64_t chunk;
     while (take_chunk(&ctrl[0], nchunks, chunk)) {
         const int64_t idx = chunk * 32 + (threadIdx.x & 31);
         if (idx >= n) continue;
-        const int i = __ldg(&order[idx]);
+        const int i = order ? __ldg(&order[idx]) : (int)idx;
+        const int nat = pm.nat ? __ldg(&pm.nat[i]) : i;  // the row in the caller's numbering
         // a converged problem's rows (and all their dependencies) are skipped together
-        if (rs.group && rs.done[(int64_t)__ldg(&rs.group[i]) * rs.stride]) continue;
+        if (rs.group && rs.done[(int64_t)__ldg(&rs.group[nat]) * rs.stride]) continue;
         const int k0 = __ldg(&ptr[i]);
         const int m = __ldg(&ptr[i + 1]) - k0;
         int c[MAXL];
@@ -785,7 +807,7 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
                 c[q] = __ldg(&col[k0 + q]);
                 v[q] = __ldg(&val[k0 + q]);
             }
-        T s = rhs[i];
+        T s = rhs[pm.gather ? nat : i];
         const T d = UNIT ? T(1) : __ldg(&dinv[i]);
         unsigned pending = 0;
 #pragma unroll
@@ -814,6 +836,7 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
             if (q < m) s = s - v[q] * xv[q];
         const T r = UNIT ? s : d * s;
         fv_publish(&x[i], r);
+        if (pm.out) pm.out[nat] = r;
         // sentinel resets come after the publish: a store to the slot just
         // read would otherwise sit on the row's critical path
         if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
@@ -830,7 +853,7 @@ __global__ void __launch_bounds__(256) k_sweep(int64_t n, const int32_t *__restr
 // current chunk and its dependencies (earlier tickets) are finished.
 template <typename T, int MAXL>
 struct SweepRow {
-    int i, m;
+    int i, m, nat;
     bool live;
     int c[MAXL];
     T v[MAXL];
@@ -841,12 +864,14 @@ template <typename T, bool UNIT, int MAXL>
 __device__ __forceinline__ void sweep_stage(SweepRow<T, MAXL> &r, int64_t chunk, int64_t n,
                                             const int32_t *__restrict__ order, const int32_t *__restrict__ ptr,
                                             const int32_t *__restrict__ col, const T *__restrict__ val,
-                                            const T *__restrict__ dinv, const T *rhs, const fv_row_skip &rs) {
+                                            const T *__restrict__ dinv, const T *rhs, const fv_row_skip &rs,
+                                            const SweepPerm<T> &pm) {
     const int64_t idx = chunk * 32 + (threadIdx.x & 31);
     r.live = idx < n;
     if (!r.live) return;
-    r.i = __ldg(&order[idx]);
-    if (rs.group && rs.done[(int64_t)__ldg(&rs.group[r.i]) * rs.stride]) {
+    r.i = order ? __ldg(&order[idx]) : (int)idx;
+    r.nat = pm.nat ? __ldg(&pm.nat[r.i]) : r.i;
+    if (rs.group && rs.done[(int64_t)__ldg(&rs.group[r.nat]) * rs.stride]) {
         r.live = false;
         return;
     }
@@ -858,7 +883,7 @@ __device__ __forceinline__ void sweep_stage(SweepRow<T, MAXL> &r, int64_t chunk,
             r.c[q] = __ldg(&col[k0 + q]);
             r.v[q] = __ldg(&val[k0 + q]);
         }
-    r.s = rhs[r.i];
+    r.s = rhs[pm.gather ? r.nat : r.i];
     r.d = UNIT ? T(1) : __ldg(&dinv[r.i]);
 }
 
@@ -867,17 +892,17 @@ __global__ void __launch_bounds__(256) k_sweep_pf(int64_t n, const int32_t *__re
                                                   const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                   const T *__restrict__ val, const T *__restrict__ dinv,
                                                   const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
-                                                  int *err, const int *skip, fv_row_skip rs) {
+                                                  int *err, const int *skip, fv_row_skip rs, SweepPerm<T> pm) {
     if (skip && *(volatile const int *)skip) return;
     const int64_t nchunks = (n + 31) / 32;
     int64_t chunk;
     bool have = take_chunk(&ctrl[0], nchunks, chunk);
     SweepRow<T, MAXL> a, b;
-    if (have) sweep_stage<T, UNIT, MAXL>(a, chunk, n, order, ptr, col, val, dinv, rhs, rs);
+    if (have) sweep_stage<T, UNIT, MAXL>(a, chunk, n, order, ptr, col, val, dinv, rhs, rs, pm);
     while (have) {
         int64_t next;
         const bool have_next = take_chunk(&ctrl[0], nchunks, next);
-        if (have_next) sweep_stage<T, UNIT, MAXL>(b, next, n, order, ptr, col, val, dinv, rhs, rs);
+        if (have_next) sweep_stage<T, UNIT, MAXL>(b, next, n, order, ptr, col, val, dinv, rhs, rs, pm);
         if (a.live) {
             T xv[MAXL];
             unsigned pending = 0;
@@ -908,6 +933,7 @@ __global__ void __launch_bounds__(256) k_sweep_pf(int64_t n, const int32_t *__re
                 if (q < a.m) s = s - a.v[q] * xv[q];
             const T r = UNIT ? s : a.d * s;
             fv_publish(&x[a.i], r);
+            if (pm.out) pm.out[a.nat] = r;
             if (rhs_reset) fv_reset_slot(&rhs_reset[a.i]);
             if (next_reset) fv_reset_slot(&next_reset[a.i]);
         }
@@ -923,16 +949,17 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
                                                     const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                                     const T *__restrict__ val, const T *__restrict__ dinv,
                                                     const T *rhs, T *x, T *rhs_reset, T *next_reset, unsigned *ctrl,
-                                                    int *err, const int *skip, fv_row_skip rs) {
+                                                    int *err, const int *skip, fv_row_skip rs, SweepPerm<T> pm) {
     if (skip && *(volatile const int *)skip) return;
     const int64_t nchunks = (n + 31) / 32;
     int64_t chunk;
     while (take_chunk(&ctrl[0], nchunks, chunk)) {
         const int64_t idx = chunk * 32 + (threadIdx.x & 31);
         if (idx >= n) continue;
-        const int i = order[idx];
-        if (rs.group && rs.done[(int64_t)rs.group[i] * rs.stride]) continue;
-        T s = rhs[i];
+        const int i = order ? order[idx] : (int)idx;
+        const int nat = pm.nat ? pm.nat[i] : i;
+        if (rs.group && rs.done[(int64_t)rs.group[nat] * rs.stride]) continue;
+        T s = rhs[pm.gather ? nat : i];
         if (rhs_reset) fv_reset_slot(&rhs_reset[i]);
         if (next_reset) fv_reset_slot(&next_reset[i]);
         const int k1 = ptr[i + 1];
@@ -942,6 +969,7 @@ __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__
         }
         const T r = UNIT ? s : dinv[i] * s;
         fv_publish(&x[i], r);
+        if (pm.out) pm.out[nat] = r;
     }
     leave(&ctrl[0], &ctrl[1]);
 }
@@ -950,28 +978,25 @@ template <typename T, bool UNIT>
 static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int32_t *order, const int32_t *ptr,
                          const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x, T *rhs_reset,
                          T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs = {},
-                         bool prefetch = false) {
+                         bool prefetch = false, SweepPerm<T> pm = {}) {
+#define FV_SWEEP(...)                                                                                           \
+    fv_note_launch(), __VA_ARGS__<<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset, next_reset, \
+                                                     ctrl, err, skip, rs, pm)
     if (prefetch && maxl <= 4)
-        fv_note_launch(), k_sweep_pf<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                   next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep_pf<T, UNIT, 4>);
     else if (prefetch && maxl <= 8)
-        fv_note_launch(), k_sweep_pf<T, UNIT, 8><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                   next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep_pf<T, UNIT, 8>);
     else if (maxl <= 4)
-        fv_note_launch(), k_sweep<T, UNIT, 4><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep<T, UNIT, 4>);
     else if (maxl <= 8)
-        fv_note_launch(), k_sweep<T, UNIT, 8><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep<T, UNIT, 8>);
     else if (maxl <= 16)
-        fv_note_launch(), k_sweep<T, UNIT, 16><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                 next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep<T, UNIT, 16>);
     else if (maxl <= 32)
-        fv_note_launch(), k_sweep<T, UNIT, 32><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                 next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep<T, UNIT, 32>);
     else
-        fv_note_launch(), k_sweep_long<T, UNIT><<<G, 256, 0, st>>>(n, order, ptr, col, val, dinv, rhs, x, rhs_reset,
-                                                                  next_reset, ctrl, err, skip, rs);
+        FV_SWEEP(k_sweep_long<T, UNIT>);
+#undef FV_SWEEP
 }
 
 // The same sweep over box tiles (fv_tiles.cu).  A warp takes a box (tickets
@@ -1592,7 +1617,25 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
         FV_CUDA_TRY(cudaGetLastError());
         return FV_OK;
     }
-    const int G = sweep_grid(n);
+    const int G = P->sweep_blocks > 0 ? P->sweep_blocks : sweep_grid(n);
+    if (P->perm) {  // reordered factorisation: gather r, sweep in B's numbering, scatter z
+        const bool pf = P->schedule == 3;
+        SweepPerm<double> fwd, bwd;
+        fwd.nat = bwd.nat = P->perm;
+        fwd.gather = true;
+        bwd.out = z;
+        if (P->kind == 2)
+            launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr,
+                                       r, P->tmp, nullptr, P->zint, P->ctrl, P->err, skip, rs, pf, fwd);
+        else
+            launch_sweep<double, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv,
+                                        r, P->tmp, nullptr, P->zint, P->ctrl, P->err, skip, rs, pf, fwd);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_sweep<double, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv,
+                                    P->tmp, P->zint, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs, pf, bwd);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1648,6 +1691,10 @@ fv_status fv_precond_make_f32(fv_precond *P, cudaStream_t st) {
         FV_CUDA_TRY(cudaMalloc(&P->dinv32, sizeof(float) * n));
         FV_CUDA_TRY(cudaMalloc(&P->tmp32, sizeof(float) * n));
         FV_CUDA_TRY(cudaMemsetAsync(P->tmp32, 0xFF, sizeof(float) * n, st));
+        if (P->perm) {
+            FV_CUDA_TRY(cudaMalloc(&P->zint32, sizeof(float) * n));
+            FV_CUDA_TRY(cudaMemsetAsync(P->zint32, 0xFF, sizeof(float) * n, st));
+        }
     }
     const int G = 148 * 8;
     if (s->nnz_l) fv_note_launch(), k_to_f32<<<G, 256, 0, st>>>(s->nnz_l, P->l_val, P->l32);
@@ -1671,7 +1718,25 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
         return FV_OK;
     }
     if (!P->l32) return FV_ERR_INVALID;
-    const int G = sweep_grid(n);
+    const int G = P->sweep_blocks > 0 ? P->sweep_blocks : sweep_grid(n);
+    if (P->perm) {  // reordered factorisation: gather r, sweep in B's numbering, scatter z
+        const bool pf = P->schedule == 3;
+        SweepPerm<float> fwd, bwd;
+        fwd.nat = bwd.nat = P->perm;
+        fwd.gather = true;
+        bwd.out = z;
+        if (P->kind == 2)
+            launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
+                                      P->tmp32, nullptr, P->zint32, P->ctrl, P->err, skip, rs, pf, fwd);
+        else
+            launch_sweep<float, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, P->dinv32,
+                                       r, P->tmp32, nullptr, P->zint32, P->ctrl, P->err, skip, rs, pf, fwd);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
+                                   P->tmp32, P->zint32, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs, pf, bwd);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1725,6 +1790,9 @@ extern "C" fv_status fv_precond_destroy(fv_precond *P) {
     cudaFree(P->dinv32);
     cudaFree(P->tmp32);
     cudaFree(P->amap);
+    cudaFree(P->perm);
+    cudaFree(P->zint);
+    cudaFree(P->zint32);
     for (int d = 0; d < 2; ++d) {
         cudaFree(P->t_rec64[d]);
         cudaFree(P->t_rec32[d]);
@@ -1984,14 +2052,252 @@ extern "C" fv_status fv_ilu0_factor(const fv_csr *A, void *stream, fv_precond **
     *out = nullptr;
     return factor_common(A, 2, fv_stream(stream), out);
 }
+// ------------------------------------------------------------------ reordered factorisation
+// IC(0) / ILU(0) of B = Q A Q^T (row i of B is row perm[i] of A, columns
+// renumbered the same way and sorted), applied in A's numbering:
+// z = Q^T M_B^{-1} Q r.  B lives in P->fill with amap[k] = the position in B
+// of A's entry k, so refactorisation is the fill path's scatter.
+namespace {
+__global__ void k_perm_inverse(int64_t n, const int32_t *__restrict__ perm, int32_t *__restrict__ iperm,
+                               int *__restrict__ bad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = perm[i];
+        if (p < 0 || p >= n) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        if (atomicExch(&iperm[p], (int32_t)i) != -1) atomicOr(bad, 1);  // p listed twice
+    }
+}
+__global__ void k_perm_rowlen(int64_t n, const int32_t *__restrict__ perm, const int32_t *__restrict__ aptr,
+                              int32_t *__restrict__ len) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+        len[i] = i < n ? aptr[perm[i] + 1] - aptr[perm[i]] : 0;
+}
+// rows of at most 32 entries (factor_common's limit)
+__global__ void k_perm_rows(int64_t n, const int32_t *__restrict__ perm, const int32_t *__restrict__ iperm,
+                            const int32_t *__restrict__ aptr, const int32_t *__restrict__ acol,
+                            const int32_t *__restrict__ bptr, int32_t *__restrict__ bcol, int32_t *__restrict__ amap,
+                            int *__restrict__ bad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t old = perm[i];
+        const int32_t k0 = aptr[old], m = aptr[old + 1] - k0, b0 = bptr[i];
+        if (m > 32) {
+            atomicOr(bad, 2);
+            continue;
+        }
+        int32_t c[32], src[32];
+        for (int t = 0; t < m; ++t) {  // insertion sort by the new column
+            const int32_t ct = iperm[acol[k0 + t]];
+            int q = t;
+            while (q > 0 && c[q - 1] > ct) {
+                c[q] = c[q - 1];
+                src[q] = src[q - 1];
+                --q;
+            }
+            c[q] = ct;
+            src[q] = k0 + t;
+        }
+        for (int t = 0; t < m; ++t) {
+            bcol[b0 + t] = c[t];
+            amap[src[t]] = b0 + t;
+        }
+    }
+}
+}  // namespace
+
+static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, int kind, cudaStream_t st,
+                                  fv_precond **out) {
+    fv_csr *A = const_cast<fv_csr *>(Ac);
+    if (!A || !perm_host || !out || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
+    const int64_t n = A->nrows, nnz = A->nnz;
+    fv_csr *B = new (std::nothrow) fv_csr();
+    if (!B) return FV_ERR_ALLOC;
+    B->nrows = B->ncols = n;
+    B->nnz = nnz;
+    int32_t *perm = nullptr, *iperm = nullptr, *len = nullptr, *amap = nullptr;
+    int *bad = nullptr;
+    void *scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    int hbad = 0;
+    cudaError_t e = cudaMalloc(&perm, sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&B->row_ptr, sizeof(int32_t) * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&B->cols, sizeof(int32_t) * (nnz ? nnz : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&B->vals, sizeof(double) * (nnz ? nnz : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&amap, sizeof(int32_t) * (nnz ? nnz : 1));
+    if (e == cudaSuccess) e = fv_malloc_async(&iperm, sizeof(int32_t) * n, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&len, sizeof(int32_t) * (n + 1), st);
+    if (e == cudaSuccess) e = fv_malloc_async(&bad, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(perm, perm_host, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(iperm, 0xFF, sizeof(int32_t) * n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), st);
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>((n + 256) / 256, 148 * 8));
+    if (e == cudaSuccess) {
+        fv_note_launch(), k_perm_inverse<<<G, 256, 0, st>>>(n, perm, iperm, bad);
+        fv_note_launch(), k_perm_rowlen<<<G, 256, 0, st>>>(n, perm, A->row_ptr, len);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, len, B->row_ptr, n + 1, st);
+    if (e == cudaSuccess) e = fv_malloc_async(&scan_tmp, scan_bytes ? scan_bytes : 1, st);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, len, B->row_ptr, n + 1, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && !hbad) {  // columns only once perm is known to be a permutation
+        fv_note_launch(), k_perm_rows<<<G, 256, 0, st>>>(n, perm, iperm, A->row_ptr, A->cols, B->row_ptr, B->cols,
+                                                        amap, bad);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (iperm) cudaFreeAsync(iperm, st);
+    if (len) cudaFreeAsync(len, st);
+    if (bad) cudaFreeAsync(bad, st);
+    if (scan_tmp) cudaFreeAsync(scan_tmp, st);
+    if (e != cudaSuccess || hbad) {
+        if (e != cudaSuccess) fv_internal_set_cuda_error(e, "reordered factorisation");
+        if (hbad & 1) fv_internal_set_error_text("perm is not a permutation of 0..n-1");
+        if (hbad & 2) fv_internal_set_error_text("a row has more than 32 entries");
+        cudaFree(perm);
+        cudaFree(amap);
+        fv_csr_destroy(B);
+        if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+        return (hbad & 2) ? FV_ERR_UNSUPPORTED : FV_ERR_INVALID;
+    }
+    fv_precond tmp;  // scatter through a stand-in so the values are in place before factorising
+    tmp.fill = B;
+    tmp.orig = A;
+    tmp.amap = amap;
+    fv_status s = scatter_fill(&tmp, st);
+    tmp.fill = nullptr;
+    tmp.amap = nullptr;
+    fv_precond *P = nullptr;
+    if (s == FV_OK) s = factor_common(B, kind, st, &P);
+    if (s == FV_OK) {
+        e = cudaMalloc(&P->zint, sizeof(double) * n);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P->zint, 0xFF, sizeof(double) * n, st);
+        if (e != cudaSuccess) {
+            fv_internal_set_cuda_error(e, "reordered factorisation");
+            fv_precond_destroy(P);
+            P = nullptr;
+            s = e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+        }
+    }
+    if (s != FV_OK) {
+        cudaFree(perm);
+        cudaFree(amap);
+        fv_csr_destroy(B);
+        return s;
+    }
+    P->fill = B;
+    P->orig = A;
+    P->amap = amap;
+    P->perm = perm;
+    *out = P;
+    return FV_OK;
+}
+
+static fv_status perm_factor(const fv_csr *A, const int32_t *perm_host, int kind, void *stream, fv_precond **out) {
+    if (!out) return FV_ERR_INVALID;
+    *out = nullptr;
+    return fv_host_guard([&] { return perm_factor_impl(A, perm_host, kind, fv_stream(stream), out); });
+}
+
+extern "C" fv_status fv_ic0_factor_perm(const fv_csr *A, const int32_t *perm, void *stream, fv_precond **out) {
+    return perm_factor(A, perm, 1, stream, out);
+}
+extern "C" fv_status fv_ilu0_factor_perm(const fv_csr *A, const int32_t *perm, void *stream, fv_precond **out) {
+    return perm_factor(A, perm, 2, stream, out);
+}
+extern "C" fv_status fv_precond_perm(const fv_precond *P, int32_t *perm_host, void *stream) {
+    if (!P || !perm_host || !P->perm) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    FV_CUDA_TRY(cudaMemcpyAsync(perm_host, P->perm, sizeof(int32_t) * P->n, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    return FV_OK;
+}
+
+// The box-colour ordering (fv_order.cpp) of a matrix assembled on a mesh:
+// cell centres from the mesh, the domain box of every problem from its
+// boundary faces' centres (a face belongs to its owner's problem).
+static fv_status order_boxes_impl(const fv_csr *A, int32_t n_problems, const int64_t *offsets,
+                                  int32_t rows_per_box, int32_t *perm_host, fv_order_info *info, cudaStream_t st) {
+    if (!A || !perm_host || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
+    const fv_mesh *m = A->mesh;
+    if (!m || m->n_cells != A->nrows) {
+        fv_internal_set_error_text("fv_order_boxes: the matrix was not assembled on a mesh (use fv_order_boxes_host)");
+        return FV_ERR_INVALID;
+    }
+    const int64_t n = A->nrows, nnz = A->nnz, nbf = m->n_bfaces, fb0 = m->n_faces - m->n_bfaces;
+    const int np = n_problems > 1 ? n_problems : 1;
+    std::vector<int64_t> off((size_t)np + 1);
+    if (np > 1) {
+        if (!offsets || offsets[0] != 0 || offsets[np] != n) return FV_ERR_INVALID;
+        for (int p = 0; p < np; ++p)
+            if (offsets[p + 1] <= offsets[p]) return FV_ERR_INVALID;
+        std::copy(offsets, offsets + np + 1, off.begin());
+    } else {
+        off[0] = 0;
+        off[1] = n;
+    }
+    std::vector<int32_t> ptr((size_t)n + 1), col((size_t)(nnz ? nnz : 1));
+    std::vector<double4> cell((size_t)n), bfc((size_t)(nbf ? nbf : 1));
+    std::vector<int2> bfo((size_t)(nbf ? nbf : 1));
+    FV_CUDA_TRY(cudaMemcpyAsync(ptr.data(), A->row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    if (nnz) FV_CUDA_TRY(cudaMemcpyAsync(col.data(), A->cols, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaMemcpyAsync(cell.data(), m->cell, sizeof(double4) * n, cudaMemcpyDeviceToHost, st));
+    if (nbf) {
+        FV_CUDA_TRY(cudaMemcpyAsync(bfc.data(), m->bface_center, sizeof(double4) * nbf, cudaMemcpyDeviceToHost, st));
+        FV_CUDA_TRY(cudaMemcpyAsync(bfo.data(), m->face_cells + fb0, sizeof(int2) * nbf, cudaMemcpyDeviceToHost, st));
+    }
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    const int dim = m->dim;
+    std::vector<double> lo((size_t)np * dim), hi((size_t)np * dim);
+    std::vector<char> seen((size_t)np, 0);
+    for (int64_t f = 0; f < nbf; ++f) {  // the boundary's face centres span each problem's domain
+        const int64_t c = bfo[f].x;
+        const int p = (int)(std::upper_bound(off.begin(), off.end(), c) - off.begin()) - 1;
+        if (p < 0 || p >= np) continue;
+        const double *x = &bfc[f].x;
+        for (int d = 0; d < dim; ++d) {
+            double &l = lo[(size_t)p * dim + d], &h = hi[(size_t)p * dim + d];
+            if (!seen[p] || x[d] < l) l = x[d];
+            if (!seen[p] || x[d] > h) h = x[d];
+        }
+        seen[p] = 1;
+    }
+    bool all_seen = true;
+    for (int p = 0; p < np; ++p) all_seen = all_seen && seen[p];
+    const double *lo_p = all_seen ? lo.data() : nullptr, *hi_p = all_seen ? hi.data() : nullptr;
+    if (np == 1)
+        return fv_order_boxes_host(n, dim, &cell[0].x, 4, lo_p, hi_p, ptr.data(), col.data(), rows_per_box,
+                                   perm_host, info);
+    return fv_order_boxes_batch_host(np, off.data(), dim, &cell[0].x, 4, lo_p, hi_p, ptr.data(), col.data(),
+                                     rows_per_box, perm_host, info);
+}
+
+extern "C" fv_status fv_order_boxes(const fv_csr *A, int32_t n_problems, const int64_t *offsets,
+                                    int32_t rows_per_box, int32_t *perm_host, fv_order_info *info, void *stream) {
+    return fv_host_guard(
+        [&] { return order_boxes_impl(A, n_problems, offsets, rows_per_box, perm_host, info, fv_stream(stream)); });
+}
+
+// Blocks (of 8 warps) per sweep launch; 0 restores the default (2 per SM,
+// tuned for latency-bound natural-order sweeps).  Any grid is correct: rows
+// are handed out by ticket in a dependency-respecting order.
+extern "C" fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks) {
+    if (!P || blocks < 0 || blocks > 148 * 32) return FV_ERR_INVALID;
+    P->sweep_blocks = blocks;
+    return FV_OK;
+}
+
 // Value-only refactorisation into an existing preconditioner (same matrix object).
 extern "C" fv_status fv_precond_refactor(fv_precond *P, void *stream) {
     if (!P) return FV_ERR_INVALID;
     fv_precond *q = P;
     cudaStream_t st = fv_stream(stream);
     if (P->kind == 3) return diag_compute(P, st);
-    if (P->fill) {  // level k: new values of the original matrix into the fill pattern
-        if (P->kind == 1) FV_TRY(check_symmetric(const_cast<fv_csr *>(P->orig), st));
+    if (P->fill) {  // level k / reordered: new values of the original matrix into the factorised one
+        if (P->kind == 1 && !P->perm) FV_TRY(check_symmetric(const_cast<fv_csr *>(P->orig), st));
         FV_TRY(scatter_fill(P, st));
     }
     return factor_common(P->A, P->kind, st, &q);

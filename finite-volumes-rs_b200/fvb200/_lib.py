@@ -107,6 +107,12 @@ class FvComm(C.Structure):
 
 
 vp = C.c_void_p
+class OrderInfo(C.Structure):
+    """fv_order_info: the box-colour ordering's grid, colours and levels."""
+    _fields_ = [("n_boxes", C.c_int64), ("boxes_per_axis", C.c_int32 * 3), ("n_colours", C.c_int32),
+                ("n_levels", C.c_int32)]
+
+
 _SIGS = {
     # host mesh
     "fv_host_mesh_from_elements": [C.c_int32, i64, dp, i64, ip, ip, ip, i64, ip, ip, ip, P(P(HostMesh_))],
@@ -159,6 +165,14 @@ _SIGS = {
     "fv_cg_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
     "fv_bicgstab_host": [vp, vp, dp, dp, SolverOptions, P(SolverInfo), vp],
     "fv_cg_noalloc": [vp, vp, vp, vp, SolverOptions, P(SolverInfo), vp],
+    "fv_ic0_factor_perm": [vp, ip, vp, P(vp)],
+    "fv_ilu0_factor_perm": [vp, ip, vp, P(vp)],
+    "fv_precond_perm": [vp, ip, vp],
+    "fv_precond_set_grid": [vp, C.c_int32],
+    "fv_order_boxes_host": [i64, C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip, P(OrderInfo)],
+    "fv_order_boxes_batch_host": [C.c_int32, P(i64), C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip,
+                                  P(OrderInfo)],
+    "fv_order_boxes": [vp, C.c_int32, P(i64), C.c_int32, ip, P(OrderInfo), vp],
     "fv_batch_create": [vp, C.c_int32, P(i64), C.c_int32, vp, P(vp)],
     "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_bicgstab": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],

@@ -19,7 +19,7 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libfvb200.so"
 
 CUDA_SOURCES = ["fv_assembly.cu", "fv_precond.cu", "fv_solvers.cu", "fv_batch.cu", "fv_dist.cu", "fv_tiles.cu", "fv_fill.cu", "fv_meshbuild.cu", "fv_vector.cu"]
-HOST_SOURCES = ["meshgen.cpp"]
+HOST_SOURCES = ["meshgen.cpp", "fv_order.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objdir = PKG.parent / "_build"
     objdir.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = objdir / (src.stem + ".o")
         cmd = [nvcc, *NVCC_FLAGS, *(extra or []), "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(src), "-o", str(obj)]
@@ -64,8 +64,14 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
                    "-I", str(INCLUDE), "-I", "/usr/local/cuda/include", "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, check=False), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(tmp),
            "-Xcompiler", "-fopenmp", "-lgomp"]

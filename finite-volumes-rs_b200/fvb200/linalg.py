@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import BcDesc, FvError, SolverInfo, SolverOptions, TermsDesc, check, exiting, lib
+from ._lib import BcDesc, FvError, OrderInfo, SolverInfo, SolverOptions, TermsDesc, check, exiting, lib
 from .streams import stream_handle
 
 
@@ -208,7 +208,38 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
     pair of arrays (bndi, bnde) over the boundary faces.  Passing `lhs` from an earlier call
     on the same mesh refills its values in place (value-only re-assembly).
     """
-    torch = _torch()
+    dm, t, bc, keep = _assembly_descriptors(equation, boundary_condition, mesh, stream)
+    rhs = DistributedVector.from_size(mesh.n_cells)
+    h = lhs.handle if lhs is not None else C.c_void_p()
+    check(lib().fv_assemble(dm.handle, C.byref(t), C.byref(bc), C.byref(h), rhs.ptr(), stream_handle(stream)),
+          "assemble")
+    # torch's caching allocator is stream ordered: the temporaries in `keep`
+    # are not reused before the assembly kernel has consumed them
+    del keep
+    if lhs is None:
+        lhs = DistributedMatrix(h, keepalive=dm)
+    return lhs, rhs
+
+
+def assembly_launcher(equation, boundary_condition, mesh, lhs: DistributedMatrix, rhs: DistributedVector,
+                      stream=None):
+    """A zero-argument callable that re-assembles `equation` into `lhs` and
+    `rhs` (value-only, resident pattern) with one fv_assemble call: the term
+    descriptors are built once, so each call is the C call alone (for timing
+    the assembly kernel)."""
+    dm, t, bc, keep = _assembly_descriptors(equation, boundary_condition, mesh, stream)
+    h = lhs.handle
+    sh = stream_handle(stream)
+
+    def run():
+        check(lib().fv_assemble(dm.handle, C.byref(t), C.byref(bc), C.byref(h), rhs.ptr(), sh), "assemble")
+
+    run.keep = keep  # the descriptors' device arrays live as long as the callable
+    return run
+
+
+def _assembly_descriptors(equation, boundary_condition, mesh, stream):
+    """(device mesh, TermsDesc, BcDesc, tensors the descriptors point into)."""
     dm = mesh.device(stream)
     c_lap, c_conv, c_src = equation.coefficients()
     keep = []
@@ -266,16 +297,7 @@ def assemble(equation, boundary_condition, mesh, lhs: DistributedMatrix | None =
     be = _dev_f64(bnde)
     keep += [bi, be]
     bc = BcDesc(bi.data_ptr(), be.data_ptr())
-    rhs = DistributedVector.from_size(mesh.n_cells)
-    h = lhs.handle if lhs is not None else C.c_void_p()
-    check(lib().fv_assemble(dm.handle, C.byref(t), C.byref(bc), C.byref(h), rhs.ptr(), stream_handle(stream)),
-          "assemble")
-    # torch's caching allocator is stream ordered: the temporaries in `keep`
-    # are not reused before the assembly kernel has consumed them
-    del keep
-    if lhs is None:
-        lhs = DistributedMatrix(h, keepalive=dm)
-    return lhs, rhs
+    return dm, t, bc, keep
 
 
 def compute_gradients(gradients: DistributedVector, values, boundary_condition, mesh, stream=None) -> None:
@@ -297,6 +319,8 @@ def compute_gradients(gradients: DistributedVector, values, boundary_condition, 
 
 class Preconditioner:
     handle = C.c_void_p()
+    perm = None          # reordered factorisations: perm[i] = the row of A that is row i of the factors
+    order_info = None
 
     def precondition(self, solution: DistributedVector, rhs: DistributedVector, comm=None, stream=None) -> None:
         """solution = M^-1 rhs (Preconditioner::precondition, preconditioners/mod.rs:13-17)."""
@@ -341,6 +365,10 @@ class Preconditioner:
                                         st.ctypes.data_as(C.POINTER(C.c_double))), "schedule")
         return act.value, st
 
+    def set_grid(self, blocks: int):
+        """Blocks of 8 warps per sweep launch (0 = default); same results for any grid."""
+        check(lib().fv_precond_set_grid(self.handle, int(blocks)), "set_grid")
+
     def refactor(self, stream=None):
         """Value-only refactorisation after the matrix values changed."""
         check(lib().fv_precond_refactor(self.handle, stream_handle(stream)), "refactor")
@@ -379,6 +407,78 @@ def _fill_pattern(kind: int, level: int, row_ptr, cols):
     return fptr, fcol[:nnz.value], amap[:len(col)], fill[:nnz.value]
 
 
+def order_boxes(matrix: "DistributedMatrix", rows_per_box: int = 0, offsets=None, stream=None):
+    """Box-colour ordering of a matrix assembled on a mesh (fv_order_boxes):
+    (perm, info) with perm[i] = the row of the matrix that becomes row i of
+    the reordered one, info = dict(n_boxes, boxes_per_axis, n_colours,
+    n_levels).  rows_per_box 0: 32 in 2D, 384 in 3D.  offsets: the row
+    offsets of the independent problems of a batch (each ordered on its own)."""
+    n = matrix.nrows()
+    perm = np.empty(n, np.int32)
+    info = OrderInfo()
+    np_, offp = 1, None
+    if offsets is not None:
+        off = np.ascontiguousarray(offsets, np.int64)
+        np_, offp = len(off) - 1, off.ctypes.data_as(C.POINTER(C.c_int64))
+    check(lib().fv_order_boxes(matrix.handle, np_, offp, int(rows_per_box),
+                               perm.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(info), stream_handle(stream)),
+          "order_boxes")
+    return perm, _order_info(info)
+
+
+def order_boxes_host(cell_center, row_ptr, cols, rows_per_box: int = 0, lo=None, hi=None):
+    """The same ordering from host arrays (fv_order_boxes_host): cell_center
+    n x dim, a CSR pattern, optional domain box lo / hi."""
+    cc = np.ascontiguousarray(cell_center, np.float64)
+    n, dim = cc.shape
+    ptr = np.ascontiguousarray(row_ptr, np.int32)
+    col = np.ascontiguousarray(cols, np.int32)
+    perm = np.empty(n, np.int32)
+    info = OrderInfo()
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    lo_a = np.ascontiguousarray(lo, np.float64) if lo is not None else None
+    hi_a = np.ascontiguousarray(hi, np.float64) if hi is not None else None
+    check(lib().fv_order_boxes_host(n, dim, cc.ctypes.data_as(dp), dim,
+                                    lo_a.ctypes.data_as(dp) if lo_a is not None else None,
+                                    hi_a.ctypes.data_as(dp) if hi_a is not None else None,
+                                    ptr.ctypes.data_as(ip), col.ctypes.data_as(ip), int(rows_per_box),
+                                    perm.ctypes.data_as(ip), C.byref(info)), "order_boxes_host")
+    return perm, _order_info(info)
+
+
+def _order_info(info):
+    return {"n_boxes": int(info.n_boxes), "boxes_per_axis": [int(v) for v in info.boxes_per_axis],
+            "n_colours": int(info.n_colours), "n_levels": int(info.n_levels)}
+
+
+def _factor(kind: str, matrix, level, ordering, stream, offsets=None):
+    """Natural order (the reference's factorisation) when ordering is None;
+    else the reordered factorisation of Q A Q^T with ordering = "boxes" (the
+    box-colour ordering; per problem with `offsets`) or a permutation array
+    (perm[i] = the row of A that becomes row i).  Returns (handle, perm or
+    None, order info or None)."""
+    h = C.c_void_p()
+    if ordering is None:
+        fn = lib().fv_ic_factor if kind == "ic" else lib().fv_ilu_factor
+        check(fn(matrix.handle, int(level), stream_handle(stream), C.byref(h)),
+              "IncompleteCholesky" if kind == "ic" else "IncompleteLowerUpper")
+        return h, None, None
+    if level != 0:
+        raise FvError(8, "reordered factorisation: level 0 only")
+    info = None
+    if isinstance(ordering, str):
+        if ordering != "boxes":
+            raise ValueError(f"unknown ordering {ordering!r}")
+        perm, info = order_boxes(matrix, offsets=offsets, stream=stream)
+    else:
+        perm = np.ascontiguousarray(ordering, np.int32)
+    fn = lib().fv_ic0_factor_perm if kind == "ic" else lib().fv_ilu0_factor_perm
+    check(fn(matrix.handle, perm.ctypes.data_as(C.POINTER(C.c_int32)), stream_handle(stream), C.byref(h)),
+          "reordered factorisation")
+    return h, perm, info
+
+
 class IncompleteCholesky(Preconditioner):
     def __init__(self, handle, n, matrix):
         self.handle, self.n, self._m = handle, n, matrix
@@ -391,10 +491,16 @@ class IncompleteCholesky(Preconditioner):
         return _fill_pattern(1, level, row_ptr, cols)
 
     @classmethod
-    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteCholesky":
-        h = C.c_void_p()
-        check(lib().fv_ic_factor(matrix.handle, int(level), stream_handle(stream), C.byref(h)), "IncompleteCholesky")
-        return cls(h, matrix.nrows(), matrix)
+    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None, ordering=None,
+                    offsets=None) -> "IncompleteCholesky":
+        """IncompleteCholesky::from_matrix(A, level) (incomplete_cholesky.rs:205).
+        ordering: None = the reference's natural row order; "boxes" or a
+        permutation = the reordered factorisation (fv_ic0_factor_perm);
+        offsets: a batch's problem row offsets for "boxes"."""
+        h, perm, info = _factor("ic", matrix, level, ordering, stream, offsets)
+        P = cls(h, matrix.nrows(), matrix)
+        P.perm, P.order_info = perm, info
+        return P
 
 
 class IncompleteLowerUpper(Preconditioner):
@@ -409,11 +515,16 @@ class IncompleteLowerUpper(Preconditioner):
         return _fill_pattern(2, level, row_ptr, cols)[:3]
 
     @classmethod
-    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None) -> "IncompleteLowerUpper":
-        h = C.c_void_p()
-        check(lib().fv_ilu_factor(matrix.handle, int(level), stream_handle(stream), C.byref(h)),
-              "IncompleteLowerUpper")
-        return cls(h, matrix.nrows(), matrix)
+    def from_matrix(cls, matrix: DistributedMatrix, level: int = 0, stream=None, ordering=None,
+                    offsets=None) -> "IncompleteLowerUpper":
+        """IncompleteLowerUpper::from_matrix(A, level) (incomplete_lower_upper.rs:266).
+        ordering: None = the reference's natural row order; "boxes" or a
+        permutation = the reordered factorisation (fv_ilu0_factor_perm);
+        offsets: a batch's problem row offsets for "boxes"."""
+        h, perm, info = _factor("ilu", matrix, level, ordering, stream, offsets)
+        P = cls(h, matrix.nrows(), matrix)
+        P.perm, P.order_info = perm, info
+        return P
 
 
 class DiagonalPreconditioner(Preconditioner):

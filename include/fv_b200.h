@@ -361,6 +361,9 @@ fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bw
  * steps, share of dependencies read from shared memory forward / backward
  * (zeros without a tiling).  Both schedules give the same bits. */
 fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats);
+/* Blocks of 8 warps per launch of the level-chunk sweeps (1..4736; 0 = the
+ * default of 2 per SM).  A tuning knob: any grid gives the same results. */
+fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks);
 fv_status fv_precond_destroy(fv_precond *P);
 /* The box-tile plan fv_ic0_factor / fv_ilu0_factor make for a matrix
  * assembled on a mesh, computed from host arrays (cell: n x 4 doubles, the
@@ -444,6 +447,67 @@ fv_status fv_batch_cg(fv_batch *B, fv_precond *P, const double *b, double *x, co
 fv_status fv_batch_bicgstab(fv_batch *B, fv_precond *P, const double *b, double *x, const fv_batch_options *opt,
                             fv_batch_info *info, void *stream);
 fv_status fv_batch_destroy(fv_batch *B);
+
+/* ------------------------------------------------------------------------ */
+/* Reordered factorisations (the perf mode of the triangular sweeps).
+ *
+ * No counterpart in the reference, which factorises in the natural row order
+ * (incomplete_lower_upper.rs:200-261, incomplete_cholesky.rs:87-145, applied
+ * by the sweeps of incomplete_lower_upper.rs:287-329 and
+ * incomplete_cholesky.rs:217-255).  In that order a 3D mesh's sweeps have a
+ * level count proportional to the mesh's extent, and every level is a
+ * dependency handoff between SMs.  These calls factorise B = Q A Q^T instead,
+ * for a permutation Q of the caller's choice (perm[i] = the row of A that
+ * becomes row i of B; host memory), and apply it in A's numbering:
+ * z = Q^T M_B^{-1} Q r.  The factors are the reference's algorithm run on B
+ * (bit for bit: fv_precond_export returns B's factors), so the preconditioner
+ * is a different one from A's natural-order factorisation and the Krylov
+ * iteration counts differ.  fv_precond_refactor moves A's new values into B
+ * (same pattern).  Errors: FV_ERR_INVALID when perm is not a permutation of
+ * 0..n-1, else as fv_ic0_factor / fv_ilu0_factor. */
+fv_status fv_ic0_factor_perm(const fv_csr *A, const int32_t *perm, void *stream, fv_precond **out);
+fv_status fv_ilu0_factor_perm(const fv_csr *A, const int32_t *perm, void *stream, fv_precond **out);
+/* The permutation of a reordered preconditioner (n entries; FV_ERR_INVALID otherwise). */
+fv_status fv_precond_perm(const fv_precond *P, int32_t *perm, void *stream);
+
+/* Box-colour ordering for fv_*_factor_perm.  The cells are grouped into
+ * boxes of their centres (about rows_per_box rows each, a grid over the
+ * domain box lo..hi shaped like the domain), the boxes coloured greedily so
+ * that no two coupled boxes share a colour, and the rows numbered colour by
+ * colour, box by box, in natural order inside a box; the rows are then sorted
+ * (stably) by their level in that ordering's forward dependency graph, which
+ * keeps the graph and makes every level a contiguous range of rows.  The
+ * sweeps then have about (colours) x (levels inside a box) levels, each
+ * spanning all boxes of a colour.  On meshes whose boxes align with the
+ * element grid two colours suffice.  O(n + nnz) on the host. */
+typedef struct fv_order_info {
+    int64_t n_boxes;            /* occupied boxes */
+    int32_t boxes_per_axis[3];  /* grid (1 on unused axes; the first problem's for a batch) */
+    int32_t n_colours;
+    int32_t n_levels;           /* levels of the forward sweep in the new order */
+} fv_order_info;
+/* cell_center: n points of `dim` coordinates, point i at cell_center + i * center_stride;
+ * lo / hi: the domain box (NULL: the centres' bounding box); row_ptr / cols: the
+ * CSR pattern of A (host).  perm (out): n entries.  rows_per_box <= 0 takes the
+ * default: 32 rows in 2D, 384 in 3D (4 x 4 squares of 2 triangles, 4^3 hexes of
+ * 6 tetrahedra). */
+fv_status fv_order_boxes_host(int64_t n, int32_t dim, const double *cell_center, int64_t center_stride,
+                              const double *lo, const double *hi, const int32_t *row_ptr, const int32_t *cols,
+                              int32_t rows_per_box, int32_t *perm, fv_order_info *info);
+/* A block-diagonal union of independent problems (problem p = rows
+ * offsets[p]..offsets[p+1]-1, coupled to nothing else): each problem ordered
+ * as above within its own domain box (lo / hi: dim values per problem, or
+ * NULL), then all rows sorted stably by (level, problem): the union has the
+ * largest problem's level count. */
+fv_status fv_order_boxes_batch_host(int32_t n_problems, const int64_t *offsets, int32_t dim,
+                                    const double *cell_center, int64_t center_stride, const double *lo,
+                                    const double *hi, const int32_t *row_ptr, const int32_t *cols,
+                                    int32_t rows_per_box, int32_t *perm, fv_order_info *info);
+/* The same for a matrix assembled on a device mesh: centres from the mesh, the
+ * domain box(es) from its boundary faces (FV_ERR_INVALID for a matrix without
+ * mesh).  n_problems <= 1: one problem; else offsets as above. */
+fv_status fv_order_boxes(const fv_csr *A, int32_t n_problems, const int64_t *offsets, int32_t rows_per_box,
+                         int32_t *perm, fv_order_info *info, void *stream);
 
 /* Allocation-free conjugate gradient.  No counterpart in the reference crate.
  *

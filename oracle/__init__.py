@@ -64,6 +64,7 @@ def lib():
             "or_diag_create": ([i64, ip, ip, dp, P(C.c_int)], vp),
             "or_precond_free": ([vp], None),
             "or_precond_nnz": ([vp], i64),
+            "or_perm_create": ([i64, ip, vp], vp),
             "or_precond_ndropped": ([vp], i64),
             "or_precond_export": ([vp, ip, ip, dp, dp], None),
             "or_levels": ([i64, ip, ip, C.c_int32, ip], C.c_int32),
@@ -281,6 +282,23 @@ class Precond:
         self.status = st.value
         self.kind = kind
 
+    @classmethod
+    def reordered(cls, kind, ptr, cols, vals, perm):
+        """The product's reordered preconditioner restated: `kind` factorised on
+        B = Q A Q^T (perm[i] = the row of A that is row i of B), applied in A's
+        numbering as z = Q^T M_B^{-1} Q r.  Factors (export) are B's."""
+        bp, bc, bv = permute(ptr, cols, vals, perm)
+        inner = cls(kind, bp, bc, bv)
+        if not inner.h:
+            return inner
+        p = np.ascontiguousarray(perm, np.int32)
+        self = cls.__new__(cls)
+        self.n, self.kind, self.status = inner.n, kind, inner.status
+        self._keep = inner._keep + (p,)
+        self.h = lib().or_perm_create(inner.n, _pi(p), inner.h)
+        inner.h = None  # owned by the wrapper now
+        return self
+
     def ok(self):
         return bool(self.h)
 
@@ -303,6 +321,24 @@ class Precond:
         if getattr(self, "h", None):
             lib().or_precond_free(self.h)
             self.h = None
+
+
+def permute(ptr, cols, vals, perm):
+    """B = Q A Q^T as CSR with sorted rows: row i of B is row perm[i] of A, every
+    column j renumbered to the position of j in perm."""
+    ptr, cols, vals = _i(ptr), _i(cols), _d(vals)
+    perm = np.ascontiguousarray(perm, np.int64)
+    n = len(ptr) - 1
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    lens = np.diff(ptr)[perm]
+    bptr = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=bptr[1:])
+    src = np.repeat(ptr[perm].astype(np.int64) - bptr[:-1], lens) + np.arange(bptr[-1])
+    rows = np.repeat(np.arange(n), lens)
+    bc = inv[cols[src]]
+    order = np.lexsort((bc, rows))
+    return bptr.astype(np.int32), bc[order].astype(np.int32), vals[src][order]
 
 
 def levels(ptr, cols, upper=False):

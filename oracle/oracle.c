@@ -561,9 +561,14 @@ double or_dot(int64_t n, const double *a, const double *b) {
 }
 
 /* ---------------------------------------------------------- preconditioners */
-typedef struct {
-    int kind;    /* 1 = IC, 2 = ILU, 3 = diagonal */
+typedef struct or_precond_s {
+    int kind;    /* 1 = IC, 2 = ILU, 3 = diagonal, 4 = reordered (wraps `inner`) */
     int64_t n;
+    /* reordered: inner is the preconditioner of B = Q A Q^T, perm[i] = the row
+     * of A that is row i of B; wr / wz are work vectors in B's numbering */
+    int32_t *perm;
+    struct or_precond_s *inner;
+    double *wr, *wz;
     /* IC: l (lower incl. diag), sp_t (upper pattern), l_vt, inv_diag */
     csr_t l;
     int32_t *spt_ptr, *spt_col;
@@ -582,6 +587,14 @@ static void csr_free(csr_t *a) {
 
 void or_precond_free(or_precond *p) {
     if (!p) return;
+    if (p->kind == 4) {
+        or_precond_free(p->inner);
+        free(p->perm);
+        free(p->wr);
+        free(p->wz);
+        free(p);
+        return;
+    }
     csr_free(&p->l);
     csr_free(&p->lu);
     free(p->spt_ptr);
@@ -814,6 +827,12 @@ or_precond *or_diag_create(int64_t n, const int32_t *ptr, const int32_t *col, co
  * ILU (incomplete_lower_upper.rs:287-329), diagonal (preconditioners/mod.rs:63-67). */
 void or_precond_apply(const or_precond *p, const double *rhs, double *sol) {
     const int64_t n = p->n;
+    if (p->kind == 4) { /* z = Q^T M_B^{-1} Q r */
+        for (int64_t i = 0; i < n; ++i) p->wr[i] = rhs[p->perm[i]];
+        or_precond_apply(p->inner, p->wr, p->wz);
+        for (int64_t i = 0; i < n; ++i) sol[p->perm[i]] = p->wz[i];
+        return;
+    }
     if (p->kind == 3) {
         for (int64_t i = 0; i < n; ++i) sol[i] = p->inv_diag[i] * rhs[i];
         return;
@@ -856,10 +875,37 @@ void or_precond_apply(const or_precond *p, const double *rhs, double *sol) {
     }
 }
 
-/* Factor export.  IC: l (lower incl. diagonal) and inv_diag.  ILU: lu. */
-int64_t or_precond_nnz(const or_precond *p) { return p->kind == 1 ? p->l.ptr[p->n] : p->lu.ptr[p->n]; }
-int64_t or_precond_ndropped(const or_precond *p) { return p->n_dropped; }
+/* The reordered preconditioner of the product's perf mode (no counterpart in
+ * the reference): `inner` (built on B = Q A Q^T, owned from here on) applied
+ * in A's numbering.  perm[i] = the row of A that is row i of B. */
+or_precond *or_perm_create(int64_t n, const int32_t *perm, or_precond *inner) {
+    if (!inner || inner->n != n) return NULL;
+    or_precond *p = (or_precond *)calloc(1, sizeof(or_precond));
+    if (!p) return NULL;
+    p->kind = 4;
+    p->n = n;
+    p->inner = inner;
+    p->perm = (int32_t *)malloc(sizeof(int32_t) * (n ? n : 1));
+    p->wr = (double *)malloc(sizeof(double) * (n ? n : 1));
+    p->wz = (double *)malloc(sizeof(double) * (n ? n : 1));
+    if (!p->perm || !p->wr || !p->wz) {
+        p->inner = NULL;
+        or_precond_free(p);
+        return NULL;
+    }
+    memcpy(p->perm, perm, sizeof(int32_t) * n);
+    return p;
+}
+
+/* Factor export.  IC: l (lower incl. diagonal) and inv_diag.  ILU: lu.
+ * Reordered: the factors of B. */
+int64_t or_precond_nnz(const or_precond *p) {
+    if (p->kind == 4) p = p->inner;
+    return p->kind == 1 ? p->l.ptr[p->n] : p->lu.ptr[p->n];
+}
+int64_t or_precond_ndropped(const or_precond *p) { return p->kind == 4 ? p->inner->n_dropped : p->n_dropped; }
 void or_precond_export(const or_precond *p, int32_t *ptr, int32_t *col, double *val, double *inv_diag) {
+    if (p->kind == 4) p = p->inner;
     const csr_t *a = p->kind == 1 ? &p->l : &p->lu;
     memcpy(ptr, a->ptr, sizeof(int32_t) * (p->n + 1));
     memcpy(col, a->col, sizeof(int32_t) * a->ptr[p->n]);
