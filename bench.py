@@ -45,6 +45,7 @@ WORKLOADS = {
     # inside FP64 reliable updates, to |b - A x| / |b| <= 1e-10
     "cube128_convdiff_mixed": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
                                    solver="bicgstab", precision="mixed"),
+    "cube96_convdiff": dict(kind="3d", n=96, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     "cube64_convdiff": dict(kind="3d", n=64, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     "cube32_convdiff": dict(kind="3d", n=32, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     # batched: 1,024 2D diffusion problems of uneven sizes
@@ -167,6 +168,8 @@ class Clocks:
 
 def sweep_schedule(P):
     """Which sweep schedule the preconditioner uses, with its box-tile plan."""
+    if P.perm is not None:
+        return {"kind": "reordered factorisation: contiguous levels, block tickets (k_sweep_seq)"}
     act, st = P.schedule()
     if act == 3:
         return {"kind": "level chunks, next chunk prefetched"}
@@ -192,7 +195,9 @@ def time_kernel(torch, fn, reps, stream):
     return e0.elapsed_time(e1) / reps / 1e3
 
 
-def gpu_arm(args, rank, world, local_rank):
+def setup_single(args, wl, rank, world, local_rank):
+    """Build the library, the seeded problem of a single-problem workload on
+    the device and its equation; returns the shared context."""
     import torch
     torch.cuda.set_device(local_rank)
     from fvb200.build import build
@@ -203,30 +208,47 @@ def gpu_arm(args, rank, world, local_rank):
         dist.barrier()
     build()
     import fvb200 as fv
-    from fvb200._lib import lib
-    wl = WORKLOADS[args.workload]
     t0 = time.time()
     prob = make_problem(fv, wl, seed=1000 + rank, on_device=True)
-    mesh = prob["mesh"]
     t_mesh = time.time() - t0
     t_mesh_dev = device_mesh_build_s(fv, wl, 1000 + rank)
     dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.current_stream()
     T = {k: torch.as_tensor(prob[k], device=dev) for k in ("kappa", "source", "bndi", "bnde")}
     T["flux"] = torch.as_tensor(prob["flux"], device=dev) if prob["flux"] is not None else None
-    eq = equation(fv, prob, T)
-    bc = (T["bndi"], T["bnde"])
+    return dict(fv=fv, torch=torch, wl=wl, prob=prob, mesh=prob["mesh"], T=T, eq=equation(fv, prob, T),
+                bc=(T["bndi"], T["bnde"]), t_mesh=t_mesh, t_mesh_dev=t_mesh_dev, dev=dev, world=world,
+                local_rank=local_rank, A=None)
+
+
+def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, kernels=True):
+    """Time `steps` steps (after `warmup`) of one single-problem workload:
+    value assembly into the resident pattern, refactorisation and a solve from
+    x0 = 0 (BiCGStab + ILU(0) in 3D, CG + IC(0) in 2D) to rtol = atol = 1e-8
+    (FP64), or the FP32 Krylov + FP32 factors inside FP64 reliable updates to
+    |b - Ax|/|b| <= 1e-10 (precision "mixed").  ordering None = the
+    reference's natural order; "boxes" = the reordered factorisation."""
+    fv, torch, wl = ctx["fv"], ctx["torch"], ctx["wl"]
+    from fvb200._lib import lib
+    world, local_rank = ctx["world"], ctx["local_rank"]
+    mesh, eq, bc, T, prob = ctx["mesh"], ctx["eq"], ctx["bc"], ctx["T"], ctx["prob"]
+    stream = torch.cuda.current_stream()
     Pcls = fv.IncompleteLowerUpper if wl["solver"] == "bicgstab" else fv.IncompleteCholesky
     solve = fv.bi_conjugate_gradient_stab if wl["solver"] == "bicgstab" else fv.conjugate_gradient
     opts = fv.LinearSolverOptions(RTOL, RTOL, 10000)
     N = mesh.n_cells
 
     # first pass builds the resident pattern, symbolic analysis and factor storage
-    A, b = fv.assemble(eq, bc, mesh)
-    P = Pcls.from_matrix(A, 0)
+    if ctx["A"] is None:
+        ctx["A"], _ = fv.assemble(eq, bc, mesh)
+    A = ctx["A"]
+    _, b = fv.assemble(eq, bc, mesh, lhs=A)
+    t0 = time.perf_counter()
+    P = Pcls.from_matrix(A, 0, ordering=ordering)
+    torch.cuda.synchronize()
+    t_factor_setup = time.perf_counter() - t0
     x = fv.DistributedVector.from_size(N)
 
-    mixed = wl.get("precision") == "mixed"
+    mixed = precision == "mixed"
     if mixed:
         from types import SimpleNamespace
 
@@ -252,22 +274,20 @@ def gpu_arm(args, rank, world, local_rank):
                                    fallback=int(o["fp64_fallback"][0]), final=float(o["final_residual"][0]))
         return solve(x, A, b, P, None, opts)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         info = step_b()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    clk = Clocks(local_rank)
+    clk = Clocks(local_rank, f"_{ordering or 'natural'}_{precision}")
     clk.start()
     torch.cuda.synchronize()
     L0 = lib().fv_launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    lat = []
-    iters = []
+    lat, iters, phases = [], [], []
     e0.record(stream)
-    phases = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(stream)
@@ -288,120 +308,140 @@ def gpu_arm(args, rank, world, local_rank):
     lat_ms = [a.elapsed_time(c) for a, c in lat]
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        t = torch.tensor([elapsed], device=ctx["dev"], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-    # correctness of the last step: true residual of the solution
+    # correctness of the last step: true residual, and error against a tight FP64 solve
     r = fv.DistributedVector.from_size(N)
     A.imul(r, x)
     relres = float(torch.linalg.norm(r.data - b.data) / torch.linalg.norm(b.data))
+    if ctx.get("x_tight") is None:
+        Pn = Pcls.from_matrix(A, 0)
+        xt = fv.DistributedVector.from_size(N)
+        solve(xt, A, b, Pn, None, fv.LinearSolverOptions(1e-13, 1e-13, 20000))
+        ctx["x_tight"] = xt
+        del Pn
+    xt = ctx["x_tight"]
+    err_tight = float(torch.linalg.norm(x.data - xt.data) / torch.linalg.norm(xt.data))
     mixed_info = None
     if mixed:
-        xt = fv.DistributedVector.from_size(N)
-        solve(xt, A, b, P, None, fv.LinearSolverOptions(1e-13, 1e-13, 20000))
-        err = float(torch.linalg.norm(x.data - xt.data) / torch.linalg.norm(xt.data))
         mixed_info = {"refinement_steps": info.refinements, "fp64_fallback": info.fallback,
-                      "final_fp64_residual": info.final, "rel_err_vs_fp64_tight": err}
-        del xt
+                      "final_fp64_residual": info.final}
+    res = dict(elapsed=elapsed, steps=steps, N=N, nnz=A.shape()[2], iters=iters, lat_ms=lat_ms, relres=relres,
+               err_tight=err_tight, launches=launches, clocks=clocks, phase_ms=phase_ms, mixed_info=mixed_info,
+               order_info=P.order_info, levels=P.levels()[2:], schedule=sweep_schedule(P),
+               factor_setup_s=round(t_factor_setup, 3), x=x.numpy())
 
-    # ---- end to end through the public API with host buffers
-    pin = {k: torch.empty(len(prob[k]), dtype=torch.float64).pin_memory()
-           for k in ("kappa", "source", "bndi", "bnde") + (("flux",) if prob["flux"] is not None else ())}
-    for k, t in pin.items():
-        t.copy_(torch.from_numpy(prob[k]))
-    x_host = torch.empty(N, dtype=torch.float64).pin_memory()
-    h2d = sum(t.numel() * 8 for t in pin.values())
-
-    def e2e_step():
+    if e2e:
+        # ---- end to end through the public API with host buffers
+        pin = {k: torch.empty(len(prob[k]), dtype=torch.float64).pin_memory()
+               for k in ("kappa", "source", "bndi", "bnde") + (("flux",) if prob["flux"] is not None else ())}
         for k, t in pin.items():
-            T[k].copy_(t, non_blocking=True)
-        step_b()
-        x_host.copy_(x.data, non_blocking=True)
+            t.copy_(torch.from_numpy(prob[k]))
+        x_host = torch.empty(N, dtype=torch.float64).pin_memory()
+        h2d = sum(t.numel() * 8 for t in pin.values())
 
-    e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    clk2 = Clocks(local_rank, "_e2e")
-    clk2.start()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2e_lat = []
-    e2.record(stream)
-    for _ in range(args.steps):
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
+        def e2e_step():
+            for k, t in pin.items():
+                T[k].copy_(t, non_blocking=True)
+            step_b()
+            x_host.copy_(x.data, non_blocking=True)
+
         e2e_step()
-        s1.record(stream)
-        e2e_lat.append((s0, s1))
-    e3.record(stream)
-    torch.cuda.synchronize()
-    e2e_clocks = clk2.stop()
-    e2e_elapsed = e2.elapsed_time(e3) / 1e3
-    e2e_lat_ms = [round(a.elapsed_time(c), 1) for a, c in e2e_lat]
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        clk2 = Clocks(local_rank, "_e2e")
+        clk2.start()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2e_lat = []
+        e2.record(stream)
+        for _ in range(steps):
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            e2e_step()
+            s1.record(stream)
+            e2e_lat.append((s0, s1))
+        e3.record(stream)
+        torch.cuda.synchronize()
+        e2e_clocks = clk2.stop()
+        e2e_elapsed = e2.elapsed_time(e3) / 1e3
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_elapsed], device=ctx["dev"], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_elapsed = float(t.item())
+        res.update(e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8,
+                   e2e_lat_ms=[round(a.elapsed_time(c), 1) for a, c in e2e_lat], e2e_clocks=e2e_clocks)
 
-    # ---- per-kernel timing of the hot kernels (roofline)
-    _, _, nnz = A.shape()
-    y = fv.DistributedVector.from_size(N)
-    z = fv.DistributedVector.from_size(N)
-    hbm, peak_kind = peaks()
-    t_spmv = time_kernel(torch, lambda: A.imul(y, x), 20, stream)
-    t_prec = time_kernel(torch, lambda: P.precondition(z, b), 10, stream)
-    # the assembly kernel alone: the fv_assemble C call with prebuilt descriptors into a preallocated rhs
-    from fvb200.linalg import assembly_launcher
-    b_fixed = fv.DistributedVector.from_size(N)
-    t_asm = time_kernel(torch, assembly_launcher(eq, bc, mesh, A, b_fixed), 10, stream)
-    t_fac = time_kernel(torch, lambda: P.refactor(), 3, stream)
-    F, Fb = mesh.n_faces, mesh.n_boundary_faces
-    bytes_spmv = 12 * nnz + 20 * N
-    bytes_prec = 12 * nnz + 40 * N
-    bytes_asm = 32 * F + 24 * Fb + 40 * N + 8 * (F - Fb) + 8 * nnz + 8 * N
-    it_mean = float(np.mean(iters))
-    per_it_spmv = 2 if wl["solver"] == "bicgstab" else 1
-    # share of a step spent in each kernel class (device time), to pick the dominant one
-    step_s = elapsed / args.steps
-    share = {
-        "precond_apply": t_prec * per_it_spmv * it_mean / step_s,
-        "spmv": t_spmv * per_it_spmv * it_mean / step_s,
-        "assembly": t_asm / step_s,
-        "factor": t_fac / step_s,
-    }
-    kern = {
-        "precond_apply": (bytes_prec, t_prec), "spmv": (bytes_spmv, t_spmv), "assembly": (bytes_asm, t_asm),
-    }
-    dom = max(("precond_apply", "spmv", "assembly"), key=lambda k: share[k])
-    bts, tk = kern[dom]
-    ach = bts / tk / 1e9
-    # DRAM bytes per launch measured by ncu on the 1.57M-cell case of the same
-    # kernels (profiles/sweep_cube64.md, profiles/assembly_cube64.md), scaled by
-    # the cell count (the per-cell structure is the same)
-    conv3d = wl["kind"] == "3d" and wl["solver"] == "bicgstab"
-    per_cell = {"precond_apply": 181.66e6 / 1572864 if conv3d else None,
-                "assembly": 253.2e6 / 1572864 if conv3d else None}
-    traffic = per_cell.get(dom)
-    roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(ach / hbm, 4), "peak_kind": peak_kind,
-            "traffic": int(traffic * N) if traffic else None,
-            "traffic_source": "ncu on 1,572,864 cells, scaled by cells" if traffic else None,
-            "algorithmic_bytes": int(bts), "launch_ms": round(tk * 1e3, 4)}
-    others = {k: {"achieved_gbs": round(kern[k][0] / kern[k][1] / 1e9, 1), "frac": round(kern[k][0] / kern[k][1] / 1e9 / hbm, 4),
-                  "launch_ms": round(kern[k][1] * 1e3, 4), "algorithmic_bytes": int(kern[k][0])} for k in kern}
-    res = dict(
-        elapsed=elapsed, steps=args.steps, N=N, nnz=nnz, iters=iters, lat_ms=lat_ms, relres=relres, t_mesh=t_mesh,
-        t_mesh_dev=t_mesh_dev,
-        e2e_elapsed=e2e_elapsed, h2d=h2d, d2h=N * 8, launches=launches, clocks=clocks, roofline=roof,
-        e2e_lat_ms=e2e_lat_ms, e2e_clocks=e2e_clocks, phase_ms=phase_ms,
-        kernels=others, share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3),
-        levels=P.levels()[2:], mesh=mesh, prob=prob, A=A, mixed_info=mixed_info, schedule=sweep_schedule(P),
-    )
+    if kernels:
+        # ---- per-kernel timing of the hot kernels (roofline)
+        nnz = res["nnz"]
+        y = fv.DistributedVector.from_size(N)
+        z = fv.DistributedVector.from_size(N)
+        hbm, peak_kind = peaks()
+        t_spmv = time_kernel(torch, lambda: A.imul(y, x), 20, stream)
+        t_prec = time_kernel(torch, lambda: P.precondition(z, b), 10, stream)
+        # the assembly kernel alone: the fv_assemble C call with prebuilt descriptors into a preallocated rhs
+        from fvb200.linalg import assembly_launcher
+        b_fixed = fv.DistributedVector.from_size(N)
+        t_asm = time_kernel(torch, assembly_launcher(eq, bc, mesh, A, b_fixed), 10, stream)
+        t_fac = time_kernel(torch, lambda: P.refactor(), 3, stream)
+        F, Fb = mesh.n_faces, mesh.n_boundary_faces
+        bytes_spmv = 12 * nnz + 20 * N
+        # ILU(0) apply: 12 nnz + 40 N; IC(0): 2 (12 (nnz + N) / 2 + 28 N); the reordered
+        # sweeps also read the permutation twice (8 N)
+        bytes_prec = (12 * nnz + 40 * N) if wl["solver"] == "bicgstab" else (12 * (nnz + N) + 56 * N)
+        if ordering is not None:
+            bytes_prec += 8 * N
+        bytes_asm = 32 * F + 24 * Fb + 40 * N + 8 * (F - Fb) + 8 * nnz + 8 * N
+        it_mean = float(np.mean(iters))
+        per_it = 2 if wl["solver"] == "bicgstab" else 1
+        step_s = elapsed / steps
+        share = {
+            "precond_apply": t_prec * per_it * it_mean / step_s,
+            "spmv": t_spmv * per_it * it_mean / step_s,
+            "assembly": t_asm / step_s,
+            "factor": t_fac / step_s,
+        }
+        kern = {"precond_apply": (bytes_prec, t_prec), "spmv": (bytes_spmv, t_spmv), "assembly": (bytes_asm, t_asm)}
+        dom = max(("precond_apply", "spmv", "assembly"), key=lambda k: share[k])
+        bts, tk = kern[dom]
+        ach = bts / tk / 1e9
+        res.update(
+            roofline={"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                      "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": int(bts),
+                      "launch_ms": round(tk * 1e3, 4)},
+            kernels={k: {"achieved_gbs": round(kern[k][0] / kern[k][1] / 1e9, 1),
+                         "frac": round(kern[k][0] / kern[k][1] / 1e9 / hbm, 4),
+                         "launch_ms": round(kern[k][1] * 1e3, 4), "algorithmic_bytes": int(kern[k][0])}
+                     for k in kern},
+            share={k: round(v, 4) for k, v in share.items()}, t_factor_ms=round(t_fac * 1e3, 3))
+    del P
     return res
+
+
+def single_summary(res, world, label):
+    """A sub-object of the JSON line for one measured single-problem mode."""
+    K = res["steps"]
+    value = K * world / res["elapsed"]
+    lat = sorted(res["lat_ms"])
+    out = {"label": label, "value": round(value, 4), "unit": "solves/s", "steps": K,
+           "ms_per_step": round(res["elapsed"] / K * 1e3, 3), "iterations": res["iters"],
+           "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+           "dof_iters_per_s": round(res["N"] * float(np.mean(res["iters"])) * value, 1),
+           "true_rel_residual": res["relres"], "rel_err_vs_tight_fp64": res["err_tight"],
+           "levels_fwd_bwd": list(res["levels"]), "ordering_info": res["order_info"],
+           "step_phase_ms_last": res["phase_ms"][-1], "clocks": res["clocks"], "gpu_launches": int(res["launches"])}
+    if res.get("kernels"):
+        out["kernels"] = res["kernels"]
+        out["roofline"] = res["roofline"]
+    if res.get("mixed_info"):
+        out["mixed"] = res["mixed_info"]
+    return out
 
 
 def cpu_full_solve(prob, wl):
@@ -419,12 +459,12 @@ def cpu_full_solve(prob, wl):
     t1 = time.perf_counter()
     pc = oracle.Precond(kind, ptr, cols, vals)
     t2 = time.perf_counter()
-    _, info = solver(ptr, cols, vals, pc, rhs, rtol=RTOL, atol=RTOL, maxit=10000)
+    x, info = solver(ptr, cols, vals, pc, rhs, rtol=RTOL, atol=RTOL, maxit=10000)
     t3 = time.perf_counter()
     sample = (f"oracle (1 thread): one complete solve -- assembly + {kind.upper()}(0) + {wl['solver']} to rtol "
               f"{RTOL} ({info['iterations']} iterations) -- timed, no extrapolation")
     return dict(t_solve=t3 - t0, t_asm=t1 - t0, t_fac=t2 - t1, t_krylov=t3 - t2, iters=int(info["iterations"]),
-                sample=sample)
+                sample=sample, x=x)
 
 
 def oracle_problem(wl, seed):
@@ -666,10 +706,13 @@ def batch_arm(args, rank, world, local_rank):
     bc = (torch.zeros(nb, dtype=torch.float64, device=dev), torch.zeros(nb, dtype=torch.float64, device=dev))
     eq = -fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
     A, b = fv.assemble(eq, bc, mb)
-    P = fv.IncompleteCholesky.from_matrix(A, 0)
+    ordering = None if args.ordering == "natural" else args.ordering
+    t0 = time.time()
+    P = fv.IncompleteCholesky.from_matrix(A, 0, ordering=ordering, offsets=mb.cell_offsets if ordering else None)
+    t_factor_setup = time.time() - t0
     x = fv.DistributedVector.from_size(mb.n_cells)
     tile, tile_times = autotune_tile(A, mb.cell_offsets, P, b, x)
-    sched, sched_times = autotune_schedule(P, b, x)
+    sched, sched_times = autotune_schedule(P, b, x) if ordering is None else (None, {})
     solver = BatchCG(A, mb.cell_offsets, tile)
     # both precisions reach the same FP64 target |b - A x| / |b| <= 1e-10 per problem
     opts_by = {"mixed": dict(precision="mixed", outer_tolerance=BATCH_OUTER_TOL, inner_relative_tolerance=1e-2,
@@ -772,7 +815,7 @@ def batch_arm(args, rank, world, local_rank):
                 other_it_max=int(np.max(out_other["iterations"])),
                 nnz=A.shape()[2], tile=tile, tile_times=tile_times, errs=errs, plain_solves=plain_solves,
                 sample=len(sample), sides=sides, levels=P.levels()[2:], schedule=sweep_schedule(P),
-                sched_times=sched_times)
+                sched_times=sched_times, order_info=P.order_info, factor_setup_s=round(t_factor_setup, 2))
 
 
 BATCH_OUTER_TOL = 1e-10
@@ -804,7 +847,8 @@ def serve_arm(args, rank, world, local_rank):
     from fvb200.serve import solve_wave
     srv = Server(fv, workers=args.serve_workers, max_wave_cells=args.serve_wave_cells,
                  max_wave_requests=args.serve_wave_requests, wave_order=args.serve_wave_order,
-                 solve_fn=functools.partial(solve_wave, precision=args.serve_precision))
+                 solve_fn=functools.partial(solve_wave, precision=args.serve_precision,
+                                            ordering=None if args.ordering == "natural" else args.ordering))
     t0 = time.time()
     keys = sorted({(r.kind, r.side) for r in reqs})
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
@@ -851,7 +895,7 @@ def serve_arm(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-inner/f64-refinement" if args.serve_precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": args.workload, "arrival_rate_per_s": args.serve_rate,
-                   "precision": args.serve_precision,
+                   "precision": args.serve_precision, "ordering": args.ordering,
                    "arrival_window_s": args.serve_duration, "requests": len(reqs),
                    "mix": "50% 2D diffusion (CG+IC0) / 50% 3D convection-diffusion (BiCGStab+ILU0)",
                    "sizes": "lognormal, 1st/99th pct 10k/2M cells, clipped; 2D sides x16, 3D sides x4",
@@ -902,7 +946,8 @@ def main_batch(args, rank, world, local_rank):
         "outer_steps_max": int(np.max(out["outer_steps"])), "iterations_max": int(np.max(its)),
         "fp64_fallback_problems": int(np.sum(out["fp64_fallback"])),
         "launched_iterations": int(out["launched_iterations"]), "levels_fwd_bwd": list(res["levels"]),
-        "sweep_schedule": res["schedule"],
+        "sweep_schedule": res["schedule"], "ordering": args.ordering, "ordering_info": res["order_info"],
+        "factor_setup_s": res["factor_setup_s"],
         "autotune_tile_s": {str(k): round(v, 4) for k, v in res["tile_times"].items()},
         "autotune_sweep_schedule_ms": {str(k): round(v, 3) for k, v in res["sched_times"].items()},
         "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "mesh_build_s": round(res["t_mesh"], 2),
@@ -919,6 +964,10 @@ def main():
     ap.add_argument("--workload", default="cube128_convdiff", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ordering", default="boxes", choices=["boxes", "natural"],
+                    help="factorisation order of the single-problem workloads: the reordered perf mode (boxes) "
+                         "or the reference's natural order")
+    ap.add_argument("--no-configs", action="store_true", help="only the headline workload (no sub-configs)")
     ap.add_argument("--batch-count", type=int, default=1024)
     ap.add_argument("--plain-sample", type=int, default=8)
     ap.add_argument("--batch-precision", default="auto", choices=["auto", "mixed", "fp64"])
@@ -952,55 +1001,108 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    res = gpu_arm(args, rank, world, local_rank)
     wl = WORKLOADS[args.workload]
+    ordering = None if args.ordering == "natural" else args.ordering
+    precision = wl.get("precision", "fp64")
+    ctx = setup_single(args, wl, rank, world, local_rank)
+    res = measure_single(ctx, ordering, args.steps, args.warmup, precision=precision, e2e=True, kernels=True)
     K = args.steps
     solves = K * world
     value = solves / res["elapsed"]
     it_mean = float(np.mean(res["iters"]))
     N = res["N"]
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cs = cpu_full_solve(res["prob"], wl)
-            cpu = {"value": round(1.0 / cs["t_solve"], 6), "unit": "solves/s", "cores": 1, "kind": "port",
-                   "sample": cs["sample"], "iterations": cs["iters"],
-                   "phase_s": {"assemble": round(cs["t_asm"], 2), "factor": round(cs["t_fac"], 2),
-                               "krylov": round(cs["t_krylov"], 2)}}
-        except Exception as e:  # pragma: no cover - reported, not fatal
-            cpu = {"value": None, "unit": "solves/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
     lat = sorted(res["lat_ms"])
+    cfg = config_of(args, wl, N, res["nnz"])
+    cfg["ordering"] = args.ordering
     line = {
         "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(res["elapsed"] / K * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_of(args, wl, N, res["nnz"]),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "dof_iters_per_s": round(N * it_mean * solves / res["elapsed"], 1),
         "iterations": res["iters"], "step_phase_ms": res["phase_ms"],
         "p50_ms": round(float(np.percentile(lat, 50)), 3),
         "p99_ms": round(float(np.percentile(lat, 99)), 3), "true_rel_residual": res["relres"],
+        "rel_err_vs_tight_fp64": res["err_tight"],
         "roofline": res["roofline"], "kernels": res["kernels"], "time_share": res["share"],
-        "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]), "sweep_schedule": res["schedule"],
-        "cpu_baseline": cpu,
+        "factor_ms": res["t_factor_ms"], "levels_fwd_bwd": list(res["levels"]), "ordering_info": res["order_info"],
+        "factor_setup_s": res["factor_setup_s"], "sweep_schedule": res["schedule"],
         "e2e": {"value": round(solves / res["e2e_elapsed"], 6), "unit": "solves/s",
                 "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"],
                 "step_ms": res["e2e_lat_ms"], "clocks": res["e2e_clocks"]},
         "gpu_launches": int(res["launches"]),
         "clocks": res["clocks"],
-        "mesh_build_s": round(res["t_mesh"], 2),
-        "mesh_build": {"where": "device (fv_mesh_build_*)", "with_read_back_and_fields_s": round(res["t_mesh"], 2),
-                       "elements_then_device_build_s": round(res["t_mesh_dev"], 3)},
+        "mesh_build_s": round(ctx["t_mesh"], 2),
+        "mesh_build": {"where": "device (fv_mesh_build_*)", "with_read_back_and_fields_s": round(ctx["t_mesh"], 2),
+                       "elements_then_device_build_s": round(ctx["t_mesh_dev"], 3)},
     }
     if res.get("mixed_info"):
         line["dtype"] = "f32-inner/f64-refinement"
-        line["config"]["precision"] = "FP32 BiCGStab + FP32 ILU(0), FP64 reliable updates to |b-Ax|/|b| <= 1e-10"
+        line["config"]["precision"] = "FP32 Krylov + FP32 factors, FP64 reliable updates to |b-Ax|/|b| <= 1e-10"
         line["mixed"] = res["mixed_info"]
+    x_gpu = {args.ordering: res["x"]}
+    if world == 1 and not args.no_configs:
+        # the same problem in the other ordering, and the FP32/FP64 form (config "mixed")
+        other = "natural" if ordering is not None else "boxes"
+        ro = measure_single(ctx, None if other == "natural" else other, max(3, K // 4), 2, e2e=False, kernels=True)
+        x_gpu[other] = ro["x"]
+        line["orderings"] = {args.ordering: single_summary(res, world, f"{wl['solver']}, {args.ordering} order, FP64"),
+                             other: single_summary(ro, world, f"{wl['solver']}, {other} order, FP64")}
+        del ro
+        if precision == "fp64":
+            rm = measure_single(ctx, ordering, max(3, K // 4), 2, precision="mixed", e2e=False, kernels=False)
+            line["configs"] = {f"{args.workload}_mixed": single_summary(
+                rm, world, "FP32 Krylov + FP32 factors inside FP64 reliable updates to |b-Ax|/|b| <= 1e-10, "
+                f"{args.ordering} order")}
+            del rm
+        if args.workload == "cube128_convdiff":
+            line.setdefault("configs", {}).update(square_configs(args))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cs = cpu_full_solve(ctx["prob"], wl)
+            cpu = {"value": round(1.0 / cs["t_solve"], 6), "unit": "solves/s", "cores": 1, "kind": "port",
+                   "sample": cs["sample"], "iterations": cs["iters"],
+                   "phase_s": {"assemble": round(cs["t_asm"], 2), "factor": round(cs["t_fac"], 2),
+                               "krylov": round(cs["t_krylov"], 2)}}
+            # the oracle's natural-order solution against the GPU's (the same algorithm)
+            if "natural" in x_gpu:
+                xo = cs["x"]
+                cpu["rel_err_gpu_natural_vs_oracle"] = float(np.linalg.norm(x_gpu["natural"] - xo) / np.linalg.norm(xo))
+        except Exception as e:  # pragma: no cover - reported, not fatal
+            cpu = {"value": None, "unit": "solves/s", "cores": 1, "kind": "port", "sample": f"failed: {e}"}
+    line["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def square_configs(args):
+    """Config "square256_diffusion" (the CPU-runnable 2D case) on the GPU in
+    both orderings, with the GPU solutions checked against the oracle's."""
+    wl = WORKLOADS["square256_diffusion"]
+    ctx = setup_single(args, wl, 0, 1, 0)
+    out = {}
+    import oracle
+    c = ctx["prob"]["coef"]
+    p = ctx["prob"]
+    ptr, cols, vals, rhs = oracle.assemble(p["mesh"], c[0], c[1], c[2], kappa=p["kappa"], flux=p["flux"],
+                                           source=p["source"], bndi=p["bndi"], bnde=p["bnde"])
+    for name, ordering in (("natural", None), ("boxes", "boxes")):
+        r = measure_single(ctx, ordering, args.steps, args.warmup, e2e=False, kernels=True)
+        sm = single_summary(r, 1, f"cg+ic0, {name} order, FP64")
+        if ordering is None:
+            pc = oracle.Precond("ic", ptr, cols, vals)
+        else:
+            perm = ctx["fv"].IncompleteCholesky.from_matrix(ctx["A"], 0, ordering="boxes").perm
+            pc = oracle.Precond.reordered("ic", ptr, cols, vals, perm)
+        xo, io = oracle.cg(ptr, cols, vals, pc, rhs, rtol=RTOL, atol=RTOL, maxit=20000)
+        sm["oracle_iterations"] = int(io["iterations"])
+        sm["rel_err_vs_oracle_same_ordering"] = float(np.linalg.norm(r["x"] - xo) / np.linalg.norm(xo))
+        out[f"square256_diffusion_{name}"] = sm
+    return out
 
 
 if __name__ == "__main__":

@@ -92,7 +92,8 @@ struct fv_precond {
     unsigned epoch = 0;
     int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned);
                                   // 3: level chunks, next chunk prefetched
-    int sweep_blocks = 0;         // blocks of 8 warps per sweep launch (0: sweep_grid's choice)
+    int sweep_blocks = 0;         // blocks of 8 warps per sweep launch (0: the kernels' default)
+    int sweep_rpt = 0;            // rows per thread of the reordered sweeps (0: default)
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
     int *err = nullptr;
     int64_t n_dropped = 0;
@@ -943,6 +944,96 @@ __global__ void __launch_bounds__(256) k_sweep_pf(int64_t n, const int32_t *__re
     leave(&ctrl[0], &ctrl[1]);
 }
 
+// Sweep of a reordered factorisation (fv_*_factor_perm with a level-sorted
+// ordering such as fv_order_boxes): every level is a contiguous range of rows
+// and rows of one level are never coupled, so rows are taken in index order
+// (forward) or reverse index order (backward: the forward levels descending
+// are a valid schedule of the upper triangle, whose dependencies always lie at
+// higher indices).  A block takes 256 * RPT consecutive rows per ticket (one
+// atomic per block chunk instead of one per warp), every thread loads the
+// static data of all its RPT rows before it polls any dependency, and there is
+// no level-order indirection, so a wide level streams at memory speed.
+// Deadlock-free for any grid: tickets are taken in order by running blocks,
+// every dependency lies at a lower position (earlier chunk, or earlier row of
+// the same chunk, which its thread handles first), so the lowest unfinished
+// row always belongs to a running block and has its inputs.
+template <typename T, bool UNIT, int MAXL, int RPT, bool REV>
+__global__ void __launch_bounds__(256) k_sweep_seq(int64_t n, const int32_t *__restrict__ ptr,
+                                                   const int32_t *__restrict__ col, const T *__restrict__ val,
+                                                   const T *__restrict__ dinv, const T *rhs, T *x, T *rhs_reset,
+                                                   T *next_reset, unsigned *ctrl, int *err, const int *skip,
+                                                   fv_row_skip rs, SweepPerm<T> pm) {
+    if (skip && *(volatile const int *)skip) return;
+    constexpr int CH = 256 * RPT;
+    const int64_t nchunks = (n + CH - 1) / CH;
+    __shared__ unsigned s_ticket;
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = atomicAdd(&ctrl[0], 1u);
+        __syncthreads();
+        const int64_t chunk = s_ticket;
+        __syncthreads();  // every thread has read the ticket before thread 0 takes the next
+        if (chunk >= nchunks) break;
+        int i[RPT], nat[RPT], m[RPT], c[RPT][MAXL];
+        T v[RPT][MAXL], sr[RPT], d[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+            const int64_t idx = chunk * CH + q * 256 + threadIdx.x;
+            m[q] = -1;  // not live
+            if (idx >= n) continue;
+            i[q] = REV ? (int)(n - 1 - idx) : (int)idx;
+            nat[q] = pm.nat ? __ldg(&pm.nat[i[q]]) : i[q];
+            if (rs.group && rs.done[(int64_t)__ldg(&rs.group[nat[q]]) * rs.stride]) continue;
+            const int k0 = __ldg(&ptr[i[q]]);
+            m[q] = __ldg(&ptr[i[q] + 1]) - k0;
+#pragma unroll
+            for (int t = 0; t < MAXL; ++t)
+                if (t < m[q]) {
+                    c[q][t] = __ldg(&col[k0 + t]);
+                    v[q][t] = __ldg(&val[k0 + t]);
+                }
+            sr[q] = rhs[pm.gather ? nat[q] : i[q]];
+            d[q] = UNIT ? T(1) : __ldg(&dinv[i[q]]);
+        }
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+            if (m[q] < 0) continue;
+            T xv[MAXL];
+            unsigned pending = 0;
+#pragma unroll
+            for (int t = 0; t < MAXL; ++t)
+                if (t < m[q] && !fv_slot_ready(&x[c[q][t]], xv[t])) pending |= 1u << t;
+            if (pending) {
+                const unsigned long long t0 = fv_globaltimer();
+                for (unsigned it = 1; pending; ++it) {
+#pragma unroll
+                    for (int t = 0; t < MAXL; ++t)
+                        if ((pending >> t) & 1u)
+                            if (fv_slot_ready(&x[c[q][t]], xv[t])) pending &= ~(1u << t);
+                    if (pending && (it & 255u) == 0) {
+                        if (*(volatile int *)err || fv_globaltimer() - t0 > FV_WAIT_LIMIT_NS) {
+                            if (!*(volatile int *)err) atomicOr(err, FV_DEV_TIMEOUT);
+#pragma unroll
+                            for (int t = 0; t < MAXL; ++t)
+                                if ((pending >> t) & 1u) xv[t] = T(NAN);
+                            pending = 0;
+                        }
+                    }
+                }
+            }
+            T s = sr[q];
+#pragma unroll
+            for (int t = 0; t < MAXL; ++t)
+                if (t < m[q]) s = s - v[q][t] * xv[t];
+            const T r = UNIT ? s : d[q] * s;
+            fv_publish(&x[i[q]], r);
+            if (pm.out) pm.out[nat[q]] = r;
+            if (rhs_reset) fv_reset_slot(&rhs_reset[i[q]]);
+            if (next_reset) fv_reset_slot(&next_reset[i[q]]);
+        }
+    }
+    leave(&ctrl[0], &ctrl[1]);
+}
+
 // Rows longer than 32 entries on the swept side: one dependency at a time.
 template <typename T, bool UNIT>
 __global__ void __launch_bounds__(256) k_sweep_long(int64_t n, const int32_t *__restrict__ order,
@@ -997,6 +1088,40 @@ static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int3
     else
         FV_SWEEP(k_sweep_long<T, UNIT>);
 #undef FV_SWEEP
+}
+
+// The reordered factorisation's sweeps (k_sweep_seq); rows_per_thread 1, 2, 4
+// or 8.  Falls back to the level-chunk kernels for rows longer than 8 entries
+// on the swept side.
+template <typename T, bool UNIT, bool REV>
+static void launch_sweep_seq(int maxl, int rpt, int G, cudaStream_t st, int64_t n, const int32_t *order,
+                             const int32_t *ptr, const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x,
+                             T *rhs_reset, T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs,
+                             SweepPerm<T> pm) {
+    if (maxl > 8) {
+        launch_sweep<T, UNIT>(maxl, G, st, n, order, ptr, col, val, dinv, rhs, x, rhs_reset, next_reset, ctrl, err,
+                              skip, rs, false, pm);
+        return;
+    }
+#define FV_SEQ(ML, R)                                                                                               \
+    fv_note_launch(), k_sweep_seq<T, UNIT, ML, R, REV><<<G, 256, 0, st>>>(n, ptr, col, val, dinv, rhs, x, rhs_reset, \
+                                                                          next_reset, ctrl, err, skip, rs, pm)
+#define FV_SEQ_R(ML)          \
+    if (rpt <= 1)             \
+        FV_SEQ(ML, 1);        \
+    else if (rpt <= 2)        \
+        FV_SEQ(ML, 2);        \
+    else if (rpt <= 4)        \
+        FV_SEQ(ML, 4);        \
+    else                      \
+        FV_SEQ(ML, 8)
+    if (maxl <= 4) {
+        FV_SEQ_R(4);
+    } else {
+        FV_SEQ_R(8);
+    }
+#undef FV_SEQ_R
+#undef FV_SEQ
 }
 
 // The same sweep over box tiles (fv_tiles.cu).  A warp takes a box (tickets
@@ -1604,6 +1729,18 @@ extern "C" fv_status fv_diag_factor(const fv_csr *A, void *stream, fv_precond **
     return FV_OK;
 }
 
+// Rows per thread and blocks of the reordered sweeps unless set by
+// fv_precond_set_grid: one row per thread and up to 8 blocks of 256 threads
+// per SM (measured on the 12.6M-row ILU(0) apply: 0.47 ms at 1 row / 1184
+// blocks, 0.51-0.52 at 2 rows, 0.75 at 4 rows, 1.28 at 8 rows: a block waits
+// for its slowest row at every ticket, so short chunks keep more rows moving).
+static int seq_rpt(const fv_precond *P) { return P->sweep_rpt > 0 ? P->sweep_rpt : 1; }
+static int seq_grid(const fv_precond *P, int64_t n, int rpt) {
+    if (P->sweep_blocks > 0) return P->sweep_blocks;
+    const int64_t chunks = (n + 256LL * rpt - 1) / (256LL * rpt);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 148 * 8));
+}
+
 // z = M^-1 r.  r must not alias z.  The forward sweep writes P->tmp and
 // pre-fills z with the sentinel; the backward sweep consumes tmp (resetting it
 // to the sentinel for the next apply) and writes z.
@@ -1624,15 +1761,20 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
         fwd.nat = bwd.nat = P->perm;
         fwd.gather = true;
         bwd.out = z;
+        (void)pf;
+        const int R = seq_rpt(P), Gs = seq_grid(P, n, R);
         if (P->kind == 2)
-            launch_sweep<double, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, nullptr,
-                                       r, P->tmp, nullptr, P->zint, P->ctrl, P->err, skip, rs, pf, fwd);
+            launch_sweep_seq<double, true, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                  P->l_val, nullptr, r, P->tmp, nullptr, P->zint, P->ctrl, P->err,
+                                                  skip, rs, fwd);
         else
-            launch_sweep<double, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l_val, P->dinv,
-                                        r, P->tmp, nullptr, P->zint, P->ctrl, P->err, skip, rs, pf, fwd);
+            launch_sweep_seq<double, false, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                   P->l_val, P->dinv, r, P->tmp, nullptr, P->zint, P->ctrl, P->err,
+                                                   skip, rs, fwd);
         FV_CUDA_TRY(cudaGetLastError());
-        launch_sweep<double, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val, P->dinv,
-                                    P->tmp, P->zint, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs, pf, bwd);
+        launch_sweep_seq<double, false, true>(s->max_upper, R, Gs, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val,
+                                              P->dinv, P->tmp, P->zint, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs,
+                                              bwd);
         FV_CUDA_TRY(cudaGetLastError());
         return FV_OK;
     }
@@ -1725,15 +1867,20 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
         fwd.nat = bwd.nat = P->perm;
         fwd.gather = true;
         bwd.out = z;
+        (void)pf;
+        const int R = seq_rpt(P), Gs = seq_grid(P, n, R);
         if (P->kind == 2)
-            launch_sweep<float, true>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, nullptr, r,
-                                      P->tmp32, nullptr, P->zint32, P->ctrl, P->err, skip, rs, pf, fwd);
+            launch_sweep_seq<float, true, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                 P->l32, nullptr, r, P->tmp32, nullptr, P->zint32, P->ctrl, P->err,
+                                                 skip, rs, fwd);
         else
-            launch_sweep<float, false>(s->max_lower, G, st, n, s->fwd_order, s->l_ptr, s->l_col, P->l32, P->dinv32,
-                                       r, P->tmp32, nullptr, P->zint32, P->ctrl, P->err, skip, rs, pf, fwd);
+            launch_sweep_seq<float, false, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                  P->l32, P->dinv32, r, P->tmp32, nullptr, P->zint32, P->ctrl,
+                                                  P->err, skip, rs, fwd);
         FV_CUDA_TRY(cudaGetLastError());
-        launch_sweep<float, false>(s->max_upper, G, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32, P->dinv32,
-                                   P->tmp32, P->zint32, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs, pf, bwd);
+        launch_sweep_seq<float, false, true>(s->max_upper, R, Gs, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32,
+                                             P->dinv32, P->tmp32, P->zint32, P->tmp32, nullptr, P->ctrl + 2, P->err,
+                                             skip, rs, bwd);
         FV_CUDA_TRY(cudaGetLastError());
         return FV_OK;
     }
@@ -2281,12 +2428,13 @@ extern "C" fv_status fv_order_boxes(const fv_csr *A, int32_t n_problems, const i
         [&] { return order_boxes_impl(A, n_problems, offsets, rows_per_box, perm_host, info, fv_stream(stream)); });
 }
 
-// Blocks (of 8 warps) per sweep launch; 0 restores the default (2 per SM,
-// tuned for latency-bound natural-order sweeps).  Any grid is correct: rows
+// Blocks (of 8 warps) per sweep launch and rows per thread of the reordered
+// sweeps; 0 restores the defaults.  Any setting gives the same results: rows
 // are handed out by ticket in a dependency-respecting order.
-extern "C" fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks) {
-    if (!P || blocks < 0 || blocks > 148 * 32) return FV_ERR_INVALID;
+extern "C" fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks, int32_t rows_per_thread) {
+    if (!P || blocks < 0 || blocks > 148 * 32 || rows_per_thread < 0 || rows_per_thread > 8) return FV_ERR_INVALID;
     P->sweep_blocks = blocks;
+    P->sweep_rpt = rows_per_thread;
     return FV_OK;
 }
 

@@ -168,7 +168,7 @@ _SIGS = {
     "fv_ic0_factor_perm": [vp, ip, vp, P(vp)],
     "fv_ilu0_factor_perm": [vp, ip, vp, P(vp)],
     "fv_precond_perm": [vp, ip, vp],
-    "fv_precond_set_grid": [vp, C.c_int32],
+    "fv_precond_set_grid": [vp, C.c_int32, C.c_int32],
     "fv_order_boxes_host": [i64, C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip, P(OrderInfo)],
     "fv_order_boxes_batch_host": [C.c_int32, P(i64), C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip,
                                   P(OrderInfo)],

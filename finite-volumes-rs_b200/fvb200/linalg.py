@@ -365,9 +365,10 @@ class Preconditioner:
                                         st.ctypes.data_as(C.POINTER(C.c_double))), "schedule")
         return act.value, st
 
-    def set_grid(self, blocks: int):
-        """Blocks of 8 warps per sweep launch (0 = default); same results for any grid."""
-        check(lib().fv_precond_set_grid(self.handle, int(blocks)), "set_grid")
+    def set_grid(self, blocks: int, rows_per_thread: int = 0):
+        """Sweep launch shape (fv_precond_set_grid): blocks per launch and rows
+        per thread of the reordered sweeps, 0 = defaults; same results for any shape."""
+        check(lib().fv_precond_set_grid(self.handle, int(blocks), int(rows_per_thread)), "set_grid")
 
     def refactor(self, stream=None):
         """Value-only refactorisation after the matrix values changed."""

@@ -145,10 +145,12 @@ BYTES_PER_CELL = {"2d": 700, "3d": 1100}   # resident estimate: mesh, CSR, facto
 
 
 def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol=1e-10, keep_solution=False,
-               precision="mixed"):
+               precision="mixed", ordering="boxes"):
     """Pack requests of one kind into one batch and solve it on `stream` to
     |b - A x| / |b| <= outer_tol per request: FP32 Krylov inside FP64
-    refinement (precision "mixed") or FP64 throughout ("fp64")."""
+    refinement (precision "mixed") or FP64 throughout ("fp64").  ordering
+    "boxes": every request's IC(0)/ILU(0) in its own box-colour order (the
+    union then has the largest request's level count); None: natural order."""
     import torch
     kind = reqs[0].kind
     with torch.cuda.stream(stream):
@@ -168,7 +170,8 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
             fl = mb.face_field(fls)
             eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
         A, b = fv.assemble(eq, bc, mb, stream=stream)
-        P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(A, 0, stream=stream)
+        P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(
+            A, 0, stream=stream, ordering=ordering, offsets=mb.cell_offsets if ordering else None)
         x = fv.DistributedVector.from_size(mb.n_cells)
         solver = BatchCG(A, mb.cell_offsets, tile_rows, stream=stream)
         if precision == "mixed":

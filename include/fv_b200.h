@@ -361,9 +361,11 @@ fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bw
  * steps, share of dependencies read from shared memory forward / backward
  * (zeros without a tiling).  Both schedules give the same bits. */
 fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats);
-/* Blocks of 8 warps per launch of the level-chunk sweeps (1..4736; 0 = the
- * default of 2 per SM).  A tuning knob: any grid gives the same results. */
-fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks);
+/* Sweep launch shape: blocks of 256 threads per sweep launch (1..4736; 0 =
+ * the default: 2 per SM for natural-order sweeps, up to 8 per SM for the
+ * reordered ones) and rows per thread of the reordered sweeps (1, 2, 4 or 8;
+ * 0 = 1).  A tuning knob: every shape gives the same results. */
+fv_status fv_precond_set_grid(fv_precond *P, int32_t blocks, int32_t rows_per_thread);
 fv_status fv_precond_destroy(fv_precond *P);
 /* The box-tile plan fv_ic0_factor / fv_ilu0_factor make for a matrix
  * assembled on a mesh, computed from host arrays (cell: n x 4 doubles, the

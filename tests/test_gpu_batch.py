@@ -230,3 +230,52 @@ def test_batch_with_diagonal_preconditioner(fv, orc):
     o1 = BatchCG(A1, mb1.cell_offsets, 256).solve(P1, b1, x1, precision="mixed", outer_tolerance=1e-10)
     r0, r1 = mb.cell_offsets[1], mb.cell_offsets[2]
     assert np.array_equal(x1.numpy(), x2.numpy()[r0:r1]) and int(o1["iterations"][0]) == int(o2["iterations"][1])
+
+
+def test_batch_reordered_per_problem_and_same_alone_and_in_mix(fv, orc):
+    """Box ordering per problem (offsets): each problem's factors are the
+    oracle's on that problem's own reordered matrix, the union has the largest
+    problem's level count, batched FP64 CG matches the oracle per problem, and
+    a problem's result is the same bits alone and in a mix (FP64 and mixed)."""
+    from fvb200.batch import BatchCG
+    probs = _problems(fv, [12, 20, 8, 16], seed0=700)
+    target = 2
+    results = {}
+    for name, subset in (("alone", [target]), ("mix", list(range(len(probs))))):
+        sel = [probs[i] for i in subset]
+        mb, A, b = _union_system(fv, sel)
+        P = fv.IncompleteCholesky.from_matrix(A, 0, ordering="boxes", offsets=mb.cell_offsets)
+        if name == "mix":
+            levels = []
+            xs = None
+            x = fv.DistributedVector.from_size(mb.n_cells)
+            out = BatchCG(A, mb.cell_offsets, 256).solve(P, b, x, precision="fp64", relative_tolerance=1e-10,
+                                                         absolute_tolerance=1e-10, max_iterations=3000)
+            xs = x.numpy()
+            for k, (m, kf, sc) in enumerate(sel):
+                nb = m.n_boundary_faces
+                ptr, cols, vals, rhs = orc.assemble(m, -1.0, 0.0, -1.0, kappa=kf, source=sc, bndi=np.zeros(nb),
+                                                    bnde=np.zeros(nb))
+                perm, info = fv.order_boxes_host(m.cell_center, ptr, cols, 0, np.zeros(2), np.ones(2))
+                levels.append(info["n_levels"])
+                o = orc.Precond.reordered("ic", ptr, cols, vals, perm)
+                xo, io = orc.cg(ptr, cols, vals, o, rhs, rtol=1e-10, atol=1e-10, maxit=3000)
+                r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+                assert abs(int(out["iterations"][k]) - io["iterations"]) <= 2
+                assert np.linalg.norm(xs[r0:r1] - xo) <= 1e-10 * np.linalg.norm(xo)
+                # this problem's rows of the union's permutation, in order, are its own ordering
+                own = P.perm[(P.perm >= r0) & (P.perm < r1)] - r0
+                assert np.array_equal(own, perm)
+            assert P.levels()[2] == max(levels) == P.order_info["n_levels"]
+        for precision in ("fp64", "mixed"):
+            x = fv.DistributedVector.from_size(mb.n_cells)
+            out = BatchCG(A, mb.cell_offsets, 512).solve(P, b, x, precision=precision, relative_tolerance=1e-8,
+                                                        absolute_tolerance=1e-8, outer_tolerance=1e-10)
+            k = subset.index(target)
+            r0, r1 = mb.cell_offsets[k], mb.cell_offsets[k + 1]
+            results[(name, precision)] = (x.numpy()[r0:r1].copy(), int(out["iterations"][k]))
+    for precision in ("fp64", "mixed"):
+        xa, ia = results[("alone", precision)]
+        xm, im = results[("mix", precision)]
+        assert ia == im
+        assert np.array_equal(xa, xm)

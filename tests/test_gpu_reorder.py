@@ -52,8 +52,8 @@ def test_reordered_factors_levels_and_apply_bit_exact(fv, orc, which):
     assert np.array_equal(fl, of) and np.array_equal(bl, ob) and (nf, nb) == (onf, onb)
     assert nf == info["n_levels"]
     rng = np.random.default_rng(7)
-    for grid in (0, 148, 1184, 0):  # repeated applies (sentinel resets) at several grids
-        P.set_grid(grid)
+    for grid, rpt in ((0, 0), (148, 1), (1184, 2), (37, 8), (0, 0)):  # repeated applies at several shapes
+        P.set_grid(grid, rpt)
         r = rng.standard_normal(len(rhs))
         z = fv.DistributedVector.from_size(len(rhs))
         P.precondition(z, fv.DistributedVector(r))
