@@ -614,7 +614,8 @@ def transient_arm(args, rank, world, local_rank):
         if A is None:
             A, b = fv.assemble(eq, bc, mesh)
             ev[1].record(stream)
-            P = fv.IncompleteLowerUpper.from_matrix(A, 0)
+            P = fv.IncompleteLowerUpper.from_matrix(A, 0, ordering=None if args.ordering == "natural"
+                                                    else args.ordering)
         else:
             _, b = fv.assemble(eq, bc, mesh, lhs=A)
             ev[1].record(stream)
@@ -657,7 +658,7 @@ def transient_arm(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "cells": N, "dt": wl["dt"], "solver": "bicgstab+ilu0",
-                   "rtol": RTOL, "parallelism": f"replicas x{world}"},
+                   "ordering": args.ordering, "rtol": RTOL, "parallelism": f"replicas x{world}"},
         "iterations": its, "step_phase_ms": ph, "phase_names": ["assemble", "refactor", "solve"],
         "gpu_launches": int(launches), "clocks": clocks,
     }
@@ -911,8 +912,7 @@ def serve_arm(args, rank, world, local_rank):
         "speedup_vs_plain_fp64": round(stats["solves_per_s"] / plain_rate, 2) if plain_rate > 0 else None,
         "gpu_launches": int(launches), "clocks": clocks, "mesh_build_s": round(t_mesh, 1),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def main_batch(args, rank, world, local_rank):
@@ -952,8 +952,7 @@ def main_batch(args, rank, world, local_rank):
         "autotune_sweep_schedule_ms": {str(k): round(v, 3) for k, v in res["sched_times"].items()},
         "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "mesh_build_s": round(res["t_mesh"], 2),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -995,7 +994,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if WORKLOADS[args.workload]["kind"] in ("batch", "serve", "transient"):
         kind = WORKLOADS[args.workload]["kind"]
-        {"batch": main_batch, "serve": serve_arm, "transient": transient_arm}[kind](args, rank, world, local_rank)
+        line = {"batch": main_batch, "serve": serve_arm, "transient": transient_arm}[kind](args, rank, world,
+                                                                                         local_rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
@@ -1056,6 +1058,15 @@ def main():
             del rm
         if args.workload == "cube128_convdiff":
             line.setdefault("configs", {}).update(square_configs(args))
+            from types import SimpleNamespace
+            sub = SimpleNamespace(**vars(args))
+            sub.workload = "batch1024_diffusion"
+            sub.steps, sub.warmup, sub.plain_sample = 1, 2, 4
+            line["configs"]["batch1024_diffusion"] = main_batch(sub, rank, world, local_rank)
+            sub = SimpleNamespace(**vars(args))
+            sub.workload = "serve_mixed"
+            sub.plain_sample = 4
+            line["configs"]["serve_mixed"] = serve_arm(sub, rank, world, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -958,7 +958,7 @@ __global__ void __launch_bounds__(256) k_sweep_pf(int64_t n, const int32_t *__re
 // the same chunk, which its thread handles first), so the lowest unfinished
 // row always belongs to a running block and has its inputs.
 template <typename T, bool UNIT, int MAXL, int RPT, bool REV>
-__global__ void __launch_bounds__(256) k_sweep_seq(int64_t n, const int32_t *__restrict__ ptr,
+__global__ void __launch_bounds__(256, RPT == 1 ? 5 : 1) k_sweep_seq(int64_t n, const int32_t *__restrict__ ptr,
                                                    const int32_t *__restrict__ col, const T *__restrict__ val,
                                                    const T *__restrict__ dinv, const T *rhs, T *x, T *rhs_reset,
                                                    T *next_reset, unsigned *ctrl, int *err, const int *skip,
@@ -966,34 +966,58 @@ __global__ void __launch_bounds__(256) k_sweep_seq(int64_t n, const int32_t *__r
     if (skip && *(volatile const int *)skip) return;
     constexpr int CH = 256 * RPT;
     const int64_t nchunks = (n + CH - 1) / CH;
-    __shared__ unsigned s_ticket;
-    for (;;) {
-        if (threadIdx.x == 0) s_ticket = atomicAdd(&ctrl[0], 1u);
-        __syncthreads();
-        const int64_t chunk = s_ticket;
-        __syncthreads();  // every thread has read the ticket before thread 0 takes the next
-        if (chunk >= nchunks) break;
-        int i[RPT], nat[RPT], m[RPT], c[RPT][MAXL];
+    // tickets alternate between two slots: thread 0 writes slot k%2 at chunk k,
+    // and every thread reads it before the barrier of chunk k+1
+    __shared__ unsigned s_ticket[2];
+    if (threadIdx.x == 0) s_ticket[0] = atomicAdd(&ctrl[0], 1u);
+    __syncthreads();
+    int64_t chunk = s_ticket[0];
+    // row bounds and caller-numbered rows of a chunk, loaded one chunk ahead
+    int i[RPT], nat[RPT], k0[RPT], k1[RPT];
+    auto addresses = [&](int64_t ch) {
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+            const int64_t idx = ch * CH + q * 256 + threadIdx.x;
+            k0[q] = 0;
+            k1[q] = -1;  // not live
+            if (ch >= nchunks || idx >= n) continue;
+            i[q] = REV ? (int)(n - 1 - idx) : (int)idx;
+            nat[q] = pm.nat ? __ldg(&pm.nat[i[q]]) : i[q];
+            k0[q] = __ldg(&ptr[i[q]]);
+            k1[q] = __ldg(&ptr[i[q] + 1]);
+        }
+    };
+    addresses(chunk);
+    for (unsigned k = 1; chunk < nchunks; ++k) {
+        // the next ticket is taken now, so its atomic overlaps this chunk's
+        // work; a block's tickets increase, so the lowest unfinished row is
+        // always in some block's current chunk
+        if (threadIdx.x == 0) s_ticket[k & 1] = atomicAdd(&ctrl[0], 1u);
+        int ci[RPT], cnat[RPT], m[RPT], c[RPT][MAXL];
         T v[RPT][MAXL], sr[RPT], d[RPT];
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
-            const int64_t idx = chunk * CH + q * 256 + threadIdx.x;
-            m[q] = -1;  // not live
-            if (idx >= n) continue;
-            i[q] = REV ? (int)(n - 1 - idx) : (int)idx;
-            nat[q] = pm.nat ? __ldg(&pm.nat[i[q]]) : i[q];
-            if (rs.group && rs.done[(int64_t)__ldg(&rs.group[nat[q]]) * rs.stride]) continue;
-            const int k0 = __ldg(&ptr[i[q]]);
-            m[q] = __ldg(&ptr[i[q] + 1]) - k0;
+            ci[q] = i[q];
+            cnat[q] = nat[q];
+            m[q] = k1[q] - k0[q];
+            if (m[q] < 0) continue;
+            // a converged problem's rows (and all their dependencies) are skipped together
+            if (rs.group && rs.done[(int64_t)__ldg(&rs.group[cnat[q]]) * rs.stride]) {
+                m[q] = -1;
+                continue;
+            }
 #pragma unroll
             for (int t = 0; t < MAXL; ++t)
                 if (t < m[q]) {
-                    c[q][t] = __ldg(&col[k0 + t]);
-                    v[q][t] = __ldg(&val[k0 + t]);
+                    c[q][t] = __ldg(&col[k0[q] + t]);
+                    v[q][t] = __ldg(&val[k0[q] + t]);
                 }
-            sr[q] = rhs[pm.gather ? nat[q] : i[q]];
-            d[q] = UNIT ? T(1) : __ldg(&dinv[i[q]]);
+            sr[q] = rhs[pm.gather ? cnat[q] : ci[q]];
+            d[q] = UNIT ? T(1) : __ldg(&dinv[ci[q]]);
         }
+        __syncthreads();
+        const int64_t next = s_ticket[k & 1];
+        addresses(next);  // the next chunk's bounds load while this chunk waits and computes
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
             if (m[q] < 0) continue;
@@ -1025,11 +1049,12 @@ __global__ void __launch_bounds__(256) k_sweep_seq(int64_t n, const int32_t *__r
             for (int t = 0; t < MAXL; ++t)
                 if (t < m[q]) s = s - v[q][t] * xv[t];
             const T r = UNIT ? s : d[q] * s;
-            fv_publish(&x[i[q]], r);
-            if (pm.out) pm.out[nat[q]] = r;
-            if (rhs_reset) fv_reset_slot(&rhs_reset[i[q]]);
-            if (next_reset) fv_reset_slot(&next_reset[i[q]]);
+            fv_publish(&x[ci[q]], r);
+            if (pm.out) pm.out[cnat[q]] = r;
+            if (rhs_reset) fv_reset_slot(&rhs_reset[ci[q]]);
+            if (next_reset) fv_reset_slot(&next_reset[ci[q]]);
         }
+        chunk = next;
     }
     leave(&ctrl[0], &ctrl[1]);
 }
