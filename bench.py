@@ -858,7 +858,8 @@ def serve_arm(args, rank, world, local_rank):
     clk = Clocks(local_rank)
     clk.start()
     L0 = lib().fv_launch_count()
-    stats = srv.run(reqs, time_limit=args.serve_time_limit)
+    cap = args.serve_time_limit if args.serve_time_limit > 0 else args.serve_duration + 15.0
+    stats = srv.run(reqs, time_limit=cap, drain=False)
     launches = lib().fv_launch_count() - L0
     clocks = clk.stop()
     # plain FP64 per-request path on a sample of the same requests, stratified by
@@ -905,7 +906,9 @@ def serve_arm(args, rank, world, local_rank):
                    "outer_tolerance": 1e-10},
         "p50_ms": round(stats["p50_ms"], 1) if stats["p50_ms"] is not None else None,
         "p99_ms": round(stats["p99_ms"], 1) if stats["p99_ms"] is not None else None,
-        "completed": stats["completed"], "waves": stats["waves"], "cells_per_s": round(stats["cells_per_s"], 1),
+        "completed": stats["completed"], "offered": stats["offered"], "backlog_at_cap": stats["backlog"],
+        "arrived_by_cap": stats["arrived_by_cap"], "wall_cap_s": cap, "failed": stats["failed"],
+        "waves": stats["waves"], "cells_per_s": round(stats["cells_per_s"], 1),
         "max_final_residual": stats["max_residual"],
         "plain_fp64_solves_per_s": round(plain_rate, 3),
         "plain_sample": f"{len(sample)} requests at evenly spaced size quantiles per kind, one at a time, rtol 1e-8",
@@ -972,12 +975,14 @@ def main():
     ap.add_argument("--batch-precision", default="auto", choices=["auto", "mixed", "fp64"])
     ap.add_argument("--serve-precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--serve-rate", type=float, default=2000.0)
-    ap.add_argument("--serve-duration", type=float, default=0.25)
+    ap.add_argument("--serve-duration", type=float, default=60.0)
     ap.add_argument("--serve-workers", type=int, default=2)
     ap.add_argument("--serve-wave-cells", type=int, default=48_000_000)
     ap.add_argument("--serve-wave-requests", type=int, default=512)
     ap.add_argument("--serve-wave-order", default="size", choices=["size", "fifo"])
-    ap.add_argument("--serve-time-limit", type=float, default=600.0)
+    ap.add_argument("--serve-time-limit", type=float, default=0.0,
+                    help="wall cap of the served run (0: arrival window + 15 s); at the cap admission stops, "
+                         "running waves finish, the rest is reported as backlog")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

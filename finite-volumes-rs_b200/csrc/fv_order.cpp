@@ -79,16 +79,52 @@ fv_status order_one(int64_t n, int32_t dim, const double *center, int64_t center
     }
     const int64_t nbox = (int64_t)K[0] * K[1] * K[2];
     if (nbox > (int64_t)1 << 31) return FV_ERR_INVALID;
+    // Box boundaries: each interior boundary moves from its uniform position to
+    // the sparsest slice of cell centres within a quarter box of it.  On a mesh
+    // built on a grid (the square and cube generators, any side) those slices
+    // are the grid lines, so no element is cut and the box graph stays the
+    // grid graph (two colours) even when the side does not divide evenly;
+    // elsewhere fewer cells straddle the boundaries.
+    constexpr int kBins = 128;  // histogram bins per box
+    constexpr int kWin = 2;     // a candidate's score: the centres within +-kWin bins (wide gaps win)
+    std::vector<double> cut[3];
+    for (int d = 0; d < dim; ++d) {
+        if (K[d] <= 1) continue;
+        const int64_t nbins = (int64_t)K[d] * kBins;
+        std::vector<int64_t> hist((size_t)nbins, 0);
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t q = (int64_t)std::floor((center[i * center_stride + d] - lo[d]) / ext[d] * nbins);
+            ++hist[(size_t)std::min<int64_t>(std::max<int64_t>(q, 0), nbins - 1)];
+        }
+        cut[d].resize((size_t)K[d] - 1);
+        for (int k = 1; k < K[d]; ++k) {
+            const int64_t mid = (int64_t)k * kBins;
+            auto score = [&](int64_t q) {
+                int64_t c = 0;
+                for (int64_t u = q - kWin; u <= q + kWin; ++u)
+                    if (u >= 0 && u < nbins) c += hist[(size_t)u];
+                return c;
+            };
+            int64_t best = mid, best_score = score(mid);
+            for (int64_t q = mid - kBins / 4; q <= mid + kBins / 4; ++q) {
+                if (q <= 0 || q >= nbins) continue;
+                // fewest centres nearby; ties go to the bin nearest the uniform position
+                const int64_t sc = score(q);
+                if (sc < best_score || (sc == best_score && std::llabs(q - mid) < std::llabs(best - mid))) {
+                    best = q;
+                    best_score = sc;
+                }
+            }
+            cut[d][k - 1] = lo[d] + ((double)best + 0.5) / nbins * ext[d];
+        }
+    }
     std::vector<int32_t> box((size_t)n);
     for (int64_t i = 0; i < n; ++i) {
         int64_t b = 0;
         for (int d = 0; d < dim; ++d) {
             int64_t q = 0;
-            if (ext[d] > 0) {
-                const double t = (center[i * center_stride + d] - lo[d]) / ext[d] * K[d];
-                q = (int64_t)std::floor(t);
-                q = std::min<int64_t>(std::max<int64_t>(q, 0), K[d] - 1);
-            }
+            if (K[d] > 1)
+                q = std::upper_bound(cut[d].begin(), cut[d].end(), center[i * center_stride + d]) - cut[d].begin();
             b = b * K[d] + q;
         }
         box[i] = (int32_t)b;
@@ -216,25 +252,35 @@ extern "C" fv_status fv_order_boxes_batch_host(int32_t n_problems, const int64_t
     if (n_problems < 1 || !offsets || !row_ptr || offsets[0] != 0 || row_ptr[0] != 0) return FV_ERR_INVALID;
     try {
         const int64_t n = offsets[n_problems];
+        for (int32_t p = 0; p < n_problems; ++p)
+            if (offsets[p + 1] <= offsets[p]) return FV_ERR_INVALID;
         std::vector<int32_t> lperm((size_t)n), lev((size_t)n);
+        std::vector<fv_order_info> one((size_t)n_problems);
+        std::vector<int> st((size_t)n_problems, FV_OK);
+        // the problems are independent: ordered side by side on the host's cores
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int32_t p = 0; p < n_problems; ++p) {
+            const int64_t a = offsets[p], b = offsets[p + 1];
+            try {
+                st[p] = order_one(b - a, dim, cell_center + a * center_stride, center_stride,
+                                  lo ? lo + (int64_t)p * dim : nullptr, hi ? hi + (int64_t)p * dim : nullptr,
+                                  row_ptr + a, cols, (int32_t)a, rows_per_box, lperm.data() + a, lev.data() + a,
+                                  &one[p]);
+            } catch (const std::bad_alloc &) {
+                st[p] = FV_ERR_ALLOC;
+            }
+            if (st[p] == FV_OK)
+                for (int64_t i = a; i < b; ++i) lperm[i] += (int32_t)a;
+        }
         fv_order_info tot{};
         int32_t nlev = 0;
         for (int32_t p = 0; p < n_problems; ++p) {
-            const int64_t a = offsets[p], b = offsets[p + 1];
-            if (b <= a) return FV_ERR_INVALID;
-            fv_order_info one{};
-            const fv_status s = order_one(b - a, dim, cell_center + a * center_stride, center_stride,
-                                          lo ? lo + (int64_t)p * dim : nullptr, hi ? hi + (int64_t)p * dim : nullptr,
-                                          row_ptr + a, cols, (int32_t)a, rows_per_box, lperm.data() + a,
-                                          lev.data() + a, &one);
-            if (s != FV_OK) return s;
-            for (int64_t i = a; i < b; ++i) lperm[i] += (int32_t)a;
-            tot.n_boxes += one.n_boxes;
-            tot.n_colours = std::max(tot.n_colours, one.n_colours);
-            nlev = std::max(nlev, one.n_levels);
-            if (p == 0)
-                for (int d = 0; d < 3; ++d) tot.boxes_per_axis[d] = one.boxes_per_axis[d];
+            if (st[p] != FV_OK) return (fv_status)st[p];
+            tot.n_boxes += one[p].n_boxes;
+            tot.n_colours = std::max(tot.n_colours, one[p].n_colours);
+            nlev = std::max(nlev, one[p].n_levels);
         }
+        for (int d = 0; d < 3; ++d) tot.boxes_per_axis[d] = one[0].boxes_per_axis[d];
         std::vector<int64_t> lptr((size_t)nlev + 1, 0);
         for (int64_t i = 0; i < n; ++i) ++lptr[lev[i] + 1];
         for (int32_t l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];

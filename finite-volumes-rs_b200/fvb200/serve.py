@@ -266,9 +266,12 @@ class Server:
         self.admitted = collections.deque(r for r in q if id(r) not in taken)
         return wave
 
-    def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True) -> dict:
+    def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True, drain: bool = True) -> dict:
         """Serve `requests` (arrival times relative to now).  Returns latency and
-        throughput statistics over the completed requests."""
+        throughput statistics over the completed requests.  At time_limit
+        admission stops; with drain the workers still solve every admitted
+        request, without it they finish their current wave and stop, and the
+        requests left (admitted or still to arrive) are the backlog."""
         if warm:  # one small wave of each kind brings the driver and the caches up
             for kind, side in (("2d", 8), ("3d", 3)):
                 self.solve_fn(self.fv, self.cache, [Request(-1, 0.0, kind, side, 1, cells=1)], self.make_stream())
@@ -309,7 +312,7 @@ class Server:
                             self.lock.wait(min(wait, 0.01))
                         else:
                             self.lock.wait(0.01)
-                    if stop.is_set() and not self.admitted:
+                    if stop.is_set() and (not drain or not self.admitted):
                         return
                     wave = self._take_wave(index, time.perf_counter() - t0)
                     wid = self.waves
@@ -356,6 +359,8 @@ class Server:
         span = (max(r.finish for r in fin) - min(r.arrival for r in fin)) if fin else 0.0
         return {
             "completed": len(fin), "offered": len(requests), "failed": self.failed, "waves": self.waves,
+            "backlog": len(requests) - len(fin) - self.failed,
+            "arrived_by_cap": sum(1 for r in requests if r.arrival <= time_limit),
             "wall_s": wall, "peak_reserved_bytes": self.peak_reserved, "budget_bytes": self.budget,
             "solves_per_s": len(fin) / span if span > 0 else 0.0,
             "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,

@@ -319,7 +319,10 @@ class Precond:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().or_precond_free(self.h)
+            try:
+                lib().or_precond_free(self.h)
+            except Exception:  # interpreter teardown: module globals may be gone already
+                pass
             self.h = None
 
 

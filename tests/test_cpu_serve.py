@@ -166,3 +166,20 @@ def test_mesh_cache_builds_each_key_once_under_concurrent_gets():
     cache.get("2d", 40)
     cache.get("2d", 60)
     assert cache.cells == sum(m.n_cells for m in cache.d.values()) and cache.cells <= 10_000
+
+
+def test_capped_run_stops_at_the_cap_and_reports_the_backlog():
+    """drain=False: at the wall cap admission stops, running waves finish,
+    nothing new starts, and every request is either completed or backlog."""
+    from fvb200.serve import Server, request_stream
+    reqs = request_stream(rate=400.0, duration=2.0, seed=3)
+    solve, _ = _fake_solve(delay_per_cell=1e-7)  # slower than the arrivals: a backlog builds
+    srv = Server(None, workers=2, budget_bytes=10 ** 12, solve_fn=solve, make_stream=_Stream)
+    t0 = time.perf_counter()
+    st = srv.run(reqs, time_limit=1.0, warm=False, drain=False)
+    wall = time.perf_counter() - t0
+    assert st["backlog"] > 0
+    assert st["completed"] + st["backlog"] + st["failed"] == st["offered"] == len(reqs)
+    assert st["arrived_by_cap"] < len(reqs)
+    # the last waves started before the cap; no wave is longer than a few seconds here
+    assert wall < 1.0 + 10.0

@@ -14,12 +14,22 @@ the perf mode (the oracle factorising the same permuted matrix):
 - pattern, assembled coefficients and right-hand side: bit for bit
 - factors, dropped-entry count and level schedules: bit for bit
 - one preconditioner apply: bit for bit
-- the solve at rtol = atol = 1e-8: iterations within +-2 of the oracle's and
-  the true residual below the tolerance.  (At this tolerance two runs whose
-  dot products are summed in different orders may stop one iteration apart,
-  which moves the solution by about one step: ~1e-9 here.)
-- the iterate after a fixed number of iterations (tolerance 0, iteration
-  counts below convergence): within 1e-10 (relative L2) of the oracle's
+- CG at rtol = atol = 1e-8: solution within 1e-10 (relative L2) of the
+  oracle's, iterations within +-2, true residual below the tolerance
+- BiCGStab: the iterate after 10 iterations (tolerance 0) within 1e-10 of
+  the oracle's; at rtol = atol = 1e-8 the true residual below the tolerance
+
+Why BiCGStab is held to less at this size: the reference restarts whenever
+|rho| <= 1e-15 |b| (bi_conjugate_gradient_stab.rs:155-169), and here |b| is
+about 5e-5, so restarts fire all through the solve (39-44 of them) at
+moments set by the last bits of the dot products.  The GPU's and the
+oracle's residual histories (the same factors, bit for bit; dot products
+summed in different orders) agree to 1e-14 at first, drift past 1e-6 by
+iteration ~20 and are unrelated by iteration ~100; perturbing the right-hand
+side by 1e-15 moves the oracle's own count on the 64^3 cube from 87 to 123.
+The stopping iteration of this solver is not a reproducible quantity, so it
+is only bounded (at most 1.5x the oracle's + 2), and the strict comparison
+is made where the two runs are still in step.
 
 The oracle's solves run on host threads side by side (ctypes releases the
 GIL); the config-1 ones take two to three minutes each.
@@ -35,8 +45,8 @@ SOL_TOL = 1e-10  # relative L2 bound on solutions (the FP64 parity bar)
 RTOL = 1e-8
 SEED = 1000
 V = (1.0, 0.5, 0.25)
-# iterations of the fixed-count comparison: below convergence in both orderings
-FIXED_ITERATIONS = {"square256": 500, "cube128": 150}
+# iterations of the fixed-count comparison (see the module docstring for BiCGStab's 10)
+FIXED_ITERATIONS = {"cube128": 10}
 MESH_ARRAYS = ("cell_face_ptr", "cell_faces", "face_owner", "face_neighbor", "face_area", "face_normal",
                "face_center", "cell_center", "cell_volume")
 
@@ -118,14 +128,16 @@ def test_factors_levels_apply_and_solves(fv, orc, problem):
     cg = problem["kind"] == "square256"
     solve = fv.conjugate_gradient if cg else fv.bi_conjugate_gradient_stab
     osolve = orc.cg if cg else orc.bicgstab
-    fixed = FIXED_ITERATIONS[problem["kind"]]
+    runs = {"rtol": (RTOL, 10000)}
+    if not cg:
+        runs["fixed"] = (0.0, FIXED_ITERATIONS[problem["kind"]])
     pairs = {o: _factor_checks(fv, orc, problem, o) for o in (None, "boxes")}
     with ThreadPoolExecutor(max_workers=4) as ex:
         futs = {(o, k): ex.submit(osolve, ptr, cols, vals, po, rhs, rtol=tol, atol=tol, maxit=it)
-                for o, (_, po) in pairs.items() for k, (tol, it) in (("rtol", (RTOL, 10000)), ("fixed", (0.0, fixed)))}
+                for o, (_, po) in pairs.items() for k, (tol, it) in runs.items()}
         gpu = {}
         for o, (P, _) in pairs.items():
-            for k, (tol, it) in (("rtol", (RTOL, 10000)), ("fixed", (0.0, fixed))):
+            for k, (tol, it) in runs.items():
                 x = fv.DistributedVector.from_size(len(rhs))
                 info = solve(x, A, b, P, None, fv.LinearSolverOptions(tol, tol, it))
                 r = fv.DistributedVector.from_size(len(rhs))
@@ -137,8 +149,12 @@ def test_factors_levels_apply_and_solves(fv, orc, problem):
             xg, info, relres = gpu[(o, k)]
             assert info.status == 0
             if k == "rtol":
-                assert abs(info.iterations - io["iterations"]) <= 2, (o, info.iterations, io["iterations"])
-                assert relres <= RTOL * 1.01, (o, relres)
+                if cg:
+                    assert abs(info.iterations - io["iterations"]) <= 2, (o, info.iterations, io["iterations"])
+                    assert np.linalg.norm(xg - xo) <= SOL_TOL * np.linalg.norm(xo), (o, k)
+                else:
+                    assert info.iterations <= 1.5 * io["iterations"] + 2, (o, info.iterations, io["iterations"])
+                assert relres <= RTOL, (o, relres)
             else:
                 assert info.iterations == io["iterations"]
                 assert np.linalg.norm(xg - xo) <= SOL_TOL * np.linalg.norm(xo), (o, k)
