@@ -1115,40 +1115,6 @@ static void launch_sweep(int maxl, int G, cudaStream_t st, int64_t n, const int3
 #undef FV_SWEEP
 }
 
-// The reordered factorisation's sweeps (k_sweep_seq); rows_per_thread 1, 2, 4
-// or 8.  Falls back to the level-chunk kernels for rows longer than 8 entries
-// on the swept side.
-template <typename T, bool UNIT, bool REV>
-static void launch_sweep_seq(int maxl, int rpt, int G, cudaStream_t st, int64_t n, const int32_t *order,
-                             const int32_t *ptr, const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x,
-                             T *rhs_reset, T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs,
-                             SweepPerm<T> pm) {
-    if (maxl > 8) {
-        launch_sweep<T, UNIT>(maxl, G, st, n, order, ptr, col, val, dinv, rhs, x, rhs_reset, next_reset, ctrl, err,
-                              skip, rs, false, pm);
-        return;
-    }
-#define FV_SEQ(ML, R)                                                                                               \
-    fv_note_launch(), k_sweep_seq<T, UNIT, ML, R, REV><<<G, 256, 0, st>>>(n, ptr, col, val, dinv, rhs, x, rhs_reset, \
-                                                                          next_reset, ctrl, err, skip, rs, pm)
-#define FV_SEQ_R(ML)          \
-    if (rpt <= 1)             \
-        FV_SEQ(ML, 1);        \
-    else if (rpt <= 2)        \
-        FV_SEQ(ML, 2);        \
-    else if (rpt <= 4)        \
-        FV_SEQ(ML, 4);        \
-    else                      \
-        FV_SEQ(ML, 8)
-    if (maxl <= 4) {
-        FV_SEQ_R(4);
-    } else {
-        FV_SEQ_R(8);
-    }
-#undef FV_SEQ_R
-#undef FV_SEQ
-}
-
 // The same sweep over box tiles (fv_tiles.cu).  A warp takes a box (tickets
 // in the boxes' dispatch order, every box after the boxes it depends on) and
 // runs its steps in level order, one row per lane.  All static data of a step
@@ -1224,6 +1190,40 @@ __device__ __forceinline__ void cp_async_small(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// The reordered factorisation's sweeps (k_sweep_seq, 1, 2, 4 or 8 rows per
+// thread); rows longer than 8 entries on the swept side fall back to the
+// level-chunk kernels.
+template <typename T, bool UNIT, bool REV>
+static void launch_sweep_seq(int maxl, int rpt, int G, cudaStream_t st, int64_t n, const int32_t *order,
+                             const int32_t *ptr, const int32_t *col, const T *val, const T *dinv, const T *rhs, T *x,
+                             T *rhs_reset, T *next_reset, unsigned *ctrl, int *err, const int *skip, fv_row_skip rs,
+                             SweepPerm<T> pm) {
+    if (maxl > 8) {
+        launch_sweep<T, UNIT>(maxl, G, st, n, order, ptr, col, val, dinv, rhs, x, rhs_reset, next_reset, ctrl, err,
+                              skip, rs, false, pm);
+        return;
+    }
+#define FV_SEQ(ML, R)                                                                                               \
+    fv_note_launch(), k_sweep_seq<T, UNIT, ML, R, REV><<<G, 256, 0, st>>>(n, ptr, col, val, dinv, rhs, x, rhs_reset, \
+                                                                          next_reset, ctrl, err, skip, rs, pm)
+#define FV_SEQ_R(ML)          \
+    if (rpt <= 1)             \
+        FV_SEQ(ML, 1);        \
+    else if (rpt <= 2)        \
+        FV_SEQ(ML, 2);        \
+    else if (rpt <= 4)        \
+        FV_SEQ(ML, 4);        \
+    else                      \
+        FV_SEQ(ML, 8)
+    if (maxl <= 4) {
+        FV_SEQ_R(4);
+    } else {
+        FV_SEQ_R(8);
+    }
+#undef FV_SEQ_R
+#undef FV_SEQ
+}
 
 template <typename T, bool UNIT>
 __global__ void __launch_bounds__(kTileWarps * 32) k_sweep_tiled(int64_t nb, const int32_t *__restrict__ box_step,

@@ -286,7 +286,8 @@ class Precond:
     def reordered(cls, kind, ptr, cols, vals, perm):
         """The product's reordered preconditioner restated: `kind` factorised on
         B = Q A Q^T (perm[i] = the row of A that is row i of B), applied in A's
-        numbering as z = Q^T M_B^{-1} Q r.  Factors (export) are B's."""
+        numbering as z = Q^T M_B^{-1} Q r.  Factors (export) are B's.  The object
+        owns one pair of work vectors: apply it from one thread at a time."""
         bp, bc, bv = permute(ptr, cols, vals, perm)
         inner = cls(kind, bp, bc, bv)
         if not inner.h:

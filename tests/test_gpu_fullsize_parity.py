@@ -132,9 +132,19 @@ def test_factors_levels_apply_and_solves(fv, orc, problem):
     if not cg:
         runs["fixed"] = (0.0, FIXED_ITERATIONS[problem["kind"]])
     pairs = {o: _factor_checks(fv, orc, problem, o) for o in (None, "boxes")}
+    pk = "ic" if cg else "ilu"
+
+    def oracle_precond(o, P, first):
+        # a solve of its own for every concurrent oracle run: the reordered
+        # wrapper's work vectors belong to one object and one thread
+        if first:
+            return pairs[o][1]
+        return orc.Precond(pk, ptr, cols, vals) if o is None else orc.Precond.reordered(pk, ptr, cols, vals, P.perm)
+
     with ThreadPoolExecutor(max_workers=4) as ex:
-        futs = {(o, k): ex.submit(osolve, ptr, cols, vals, po, rhs, rtol=tol, atol=tol, maxit=it)
-                for o, (_, po) in pairs.items() for k, (tol, it) in runs.items()}
+        futs = {(o, k): ex.submit(osolve, ptr, cols, vals, oracle_precond(o, P, j == 0), rhs, rtol=tol, atol=tol,
+                                  maxit=it)
+                for o, (P, _) in pairs.items() for j, (k, (tol, it)) in enumerate(runs.items())}
         gpu = {}
         for o, (P, _) in pairs.items():
             for k, (tol, it) in runs.items():
