@@ -46,6 +46,8 @@ WORKLOADS = {
     "cube128_convdiff_mixed": dict(kind="3d", n=128, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
                                    solver="bicgstab", precision="mixed"),
     "cube96_convdiff": dict(kind="3d", n=96, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
+    "cube96_convdiff_mixed": dict(kind="3d", n=96, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25),
+                                  solver="bicgstab", precision="mixed"),
     "cube64_convdiff": dict(kind="3d", n=64, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     "cube32_convdiff": dict(kind="3d", n=32, jitter=0.15, sigma=0.5, velocity=(1.0, 0.5, 0.25), solver="bicgstab"),
     # batched: 1,024 2D diffusion problems of uneven sizes
