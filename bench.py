@@ -848,10 +848,15 @@ def serve_arm(args, rank, world, local_rank):
     import functools
 
     from fvb200.serve import solve_wave
-    srv = Server(fv, workers=args.serve_workers, max_wave_cells=args.serve_wave_cells,
+    from fvb200.serve import WaveRun
+    ordering = None if args.ordering == "natural" else args.ordering
+    # a refill holds the old and the rebuilt wave on the device for a moment: half-size waves
+    wave_cells = args.serve_wave_cells or (24_000_000 if args.serve_refill else 48_000_000)
+    srv = Server(fv, workers=args.serve_workers, max_wave_cells=wave_cells,
                  max_wave_requests=args.serve_wave_requests, wave_order=args.serve_wave_order,
-                 solve_fn=functools.partial(solve_wave, precision=args.serve_precision,
-                                            ordering=None if args.ordering == "natural" else args.ordering))
+                 solve_fn=functools.partial(solve_wave, precision=args.serve_precision, ordering=ordering),
+                 refill=bool(args.serve_refill),
+                 run_fn=functools.partial(WaveRun, precision=args.serve_precision, ordering=ordering))
     t0 = time.time()
     keys = sorted({(r.kind, r.side) for r in reqs})
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
@@ -903,14 +908,17 @@ def serve_arm(args, rank, world, local_rank):
                    "arrival_window_s": args.serve_duration, "requests": len(reqs),
                    "mix": "50% 2D diffusion (CG+IC0) / 50% 3D convection-diffusion (BiCGStab+ILU0)",
                    "sizes": "lognormal, 1st/99th pct 10k/2M cells, clipped; 2D sides x16, 3D sides x4",
-                   "workers": args.serve_workers, "max_wave_cells": args.serve_wave_cells,
-                   "max_wave_requests": args.serve_wave_requests, "wave_order": args.serve_wave_order,
+                   "workers": args.serve_workers, "max_wave_cells": wave_cells,
+                   "max_wave_requests": args.serve_wave_requests,
+                   "batching": ("slot refill: finished requests leave at once, waiting ones join the running "
+                                "wave, whose running requests carry their state over" if args.serve_refill
+                                else f"whole waves ({args.serve_wave_order} order)"),
                    "outer_tolerance": 1e-10},
         "p50_ms": round(stats["p50_ms"], 1) if stats["p50_ms"] is not None else None,
         "p99_ms": round(stats["p99_ms"], 1) if stats["p99_ms"] is not None else None,
         "completed": stats["completed"], "offered": stats["offered"], "backlog_at_cap": stats["backlog"],
         "arrived_by_cap": stats["arrived_by_cap"], "wall_cap_s": cap, "failed": stats["failed"],
-        "waves": stats["waves"], "cells_per_s": round(stats["cells_per_s"], 1),
+        "waves": stats["waves"], "refills": stats["refills"], "cells_per_s": round(stats["cells_per_s"], 1),
         "max_final_residual": stats["max_residual"],
         "plain_fp64_solves_per_s": round(plain_rate, 3),
         "plain_sample": f"{len(sample)} requests at evenly spaced size quantiles per kind, one at a time, rtol 1e-8",
@@ -979,9 +987,12 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-duration", type=float, default=60.0)
     ap.add_argument("--serve-workers", type=int, default=2)
-    ap.add_argument("--serve-wave-cells", type=int, default=48_000_000)
+    ap.add_argument("--serve-wave-cells", type=int, default=0,
+                    help="cells per wave (0: 24M with slot refill, 48M with whole waves)")
     ap.add_argument("--serve-wave-requests", type=int, default=512)
     ap.add_argument("--serve-wave-order", default="size", choices=["size", "fifo"])
+    ap.add_argument("--serve-refill", type=int, default=1, choices=[0, 1],
+                    help="1: slot refill (running waves take newly admitted requests); 0: whole waves")
     ap.add_argument("--serve-time-limit", type=float, default=0.0,
                     help="wall cap of the served run (0: arrival window + 15 s); at the cap admission stops, "
                          "running waves finish, the rest is reported as backlog")

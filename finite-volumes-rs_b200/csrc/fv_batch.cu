@@ -58,15 +58,14 @@ struct BProb {
     int forced, pad3;       // the pending replacement was forced by the period
     // outer refinement (FP64)
     double bnorm64, res64;
-    int64_t inner_total;
-    int outer_it, outer_done;
+    // stepwise runs: 1 once the retired problem's pending correction is applied
+    int fin, pad4;
 };
 
 struct BGlobal {
     int active;       // problems whose inner solve is running
     int all_done;     // 1 when active == 0 (skips the sweeps)
-    int outer_active; // problems whose refinement is running
-    int pad;
+    int pad[2];
 };
 
 constexpr int TB = 256;  // threads per tile block
@@ -495,6 +494,7 @@ __global__ void __launch_bounds__(TB) kbm_init(Tiles tl, const double *__restric
                                                float *__restrict__ r32, double *partial, BProb *S, BGlobal *G) {
     for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int p = tl.prob[t];
+        if (S[p].done) continue;  // a problem carried over from another batch keeps its state
         double v[1] = {0.0};
         for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) {
             const double bi = b[i];
@@ -611,6 +611,54 @@ __global__ void kbm_flush(Tiles tl, double *__restrict__ x, T *__restrict__ d) {
         }
 }
 
+// ---- stepwise runs
+// The result of every problem that retired since the last call: d = h where
+// BiCGStab's |s| test ended the solve (h non-null), x64 += d (mixed, x64
+// non-null).  Per problem these are the operations kbb_finish and kbm_flush
+// apply at the end of a whole-batch solve.
+template <typename T>
+__global__ void kb_finalize(Tiles tl, T *__restrict__ d, const T *__restrict__ h, double *__restrict__ x64,
+                            const BProb *S) {
+    for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+        const int p = tl.prob[t];
+        if (!S[p].done || S[p].fin) continue;
+        const bool take_h = h && S[p].finish_h == 1;
+        for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) {
+            if (take_h) d[i] = h[i];
+            if (x64) {
+                x64[i] += (double)d[i];
+                d[i] = T(0);
+            }
+        }
+    }
+}
+
+__global__ void kb_mark_fin(int np, BProb *S) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
+        if (S[p].done) S[p].fin = 1;
+}
+
+// Copy the rows of the problems carried over from another batch:
+// seg[3 s .. 3 s + 2] = (source row, destination row, rows) of segment s.
+template <typename T>
+__global__ void kb_adopt(const int64_t *__restrict__ seg, int nseg, const T *__restrict__ src, T *__restrict__ dst) {
+    for (int s = blockIdx.y; s < nseg; s += gridDim.y) {
+        const int64_t a = seg[3 * s], b = seg[3 * s + 1], len = seg[3 * s + 2];
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+            dst[b + i] = src[a + i];
+    }
+}
+
+// The carried-over problems, held as done while the new problems were
+// initialised, run again.
+__global__ void kb_resume(const int32_t *__restrict__ list, int cnt, BProb *S, BGlobal *G) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) S[list[k]].done = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && cnt > 0) {
+        atomicAdd(&G->active, cnt);
+        G->all_done = 0;
+    }
+}
+
 __global__ void k_to_f32b(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
@@ -635,6 +683,16 @@ struct fv_batch {
     size_t vec_bytes = 0;
     void *vec64 = nullptr;  // FP64 fallback workspace (allocated on first need)
     size_t vec64_bytes = 0;
+    // the run begun by fv_batch_begin (or a whole-batch solve)
+    bool run = false, bicg = false, mixed = false;
+    fv_precond *P = nullptr;
+    const double *b = nullptr;
+    double *x = nullptr;
+    fv_batch_options opt{};
+    int64_t launched = 0;        // iterations enqueued for the whole batch
+    std::vector<BProb> hs;       // the problems' state as of the end of the last begin / advance
+    int64_t *seg = nullptr;      // carried-over segments (kb_adopt)
+    int32_t *resume = nullptr;   // carried-over problems (kb_resume)
 };
 
 extern "C" fv_status fv_batch_destroy(fv_batch *B) {
@@ -650,6 +708,8 @@ extern "C" fv_status fv_batch_destroy(fv_batch *B) {
     cudaFree(B->a32);
     cudaFree(B->vec);
     cudaFree(B->vec64);
+    cudaFree(B->seg);
+    cudaFree(B->resume);
     delete B;
     return FV_OK;
 }
@@ -749,17 +809,36 @@ struct MixedArgs {
     const double *b64;
 };
 
+constexpr int kGroupCG = 8;    // CG iterations enqueued between two host checks
+constexpr int kGroupBiCG = 4;  // BiCGStab iterations enqueued between two host checks
+
+// The start of an inner solve for the problems not done: CG (r given; d = 0,
+// z = M^-1 r, p = z) or BiCGStab (r given; d = 0, rh = p = r).
 template <typename T>
-fv_status inner_cg(fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, int G, const Tiles &tl,
-                   cudaStream_t st, int64_t &launched_iters, const MixedArgs &mx) {
+fv_status inner_start(bool bicg, fv_batch *B, fv_precond *P, InnerVecs<T> v, int G, const Tiles &tl,
+                      cudaStream_t st) {
+    const int *skip = &B->G->all_done;
+    if (!bicg) {
+        fv_note_launch(), kb_init<T><<<G, TB, 0, st>>>(tl, v.r, v.d, B->partial, B->S, B->G);
+        FV_TRY(precond<T>(B, P, v.r, v.z, st, skip));
+        fv_note_launch(), kb_init_p<T><<<G, TB, 0, st>>>(tl, v.r, v.z, v.p, B->partial, B->S, B->G);
+    } else {
+        fv_note_launch(), kbb_init<T><<<G, TB, 0, st>>>(tl, v.r, v.d, v.rh, v.p, B->partial, B->S, B->G);
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+// One group of iterations for the problems not done.  Between two groups
+// every problem is at an iteration boundary: CG's state is (d, r, p, rz),
+// BiCGStab's (d, r, rh, p, rho, alpha, omega), plus x64 in mixed mode.
+template <typename T>
+fv_status inner_group(bool bicg, fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, int G, const Tiles &tl,
+                      cudaStream_t st, int64_t &launched_iters, const MixedArgs &mx) {
     const fv_csr *A = B->A;
     const int *skip = &B->G->all_done;
-    fv_note_launch(), kb_init<T><<<G, TB, 0, st>>>(tl, v.r, v.d, B->partial, B->S, B->G);
-    FV_TRY(precond<T>(B, P, v.r, v.z, st, skip));
-    fv_note_launch(), kb_init_p<T><<<G, TB, 0, st>>>(tl, v.r, v.z, v.p, B->partial, B->S, B->G);
-    FV_CUDA_TRY(cudaGetLastError());
-    for (bool done = false; !done;) {
-        for (int q = 0; q < 8; ++q) {
+    if (!bicg) {
+        for (int q = 0; q < kGroupCG; ++q) {
             fv_note_launch(), kb_spmv<T><<<G, TB, 0, st>>>(tl, A->row_ptr, A->cols, vals, v.p, v.ap, B->partial, B->S,
                                                           B->G);
             fv_note_launch(), kb_update<T><<<G, TB, 0, st>>>(tl, v.d, v.r, v.p, v.ap, B->partial, B->S, B->G, mx.cfg);
@@ -774,22 +853,8 @@ fv_status inner_cg(fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, in
             fv_note_launch(), kb_p<T><<<G, TB, 0, st>>>(tl, v.z, v.p, B->S);
             ++launched_iters;
         }
-        FV_TRY(wait_all_done(B, st, done));
-    }
-    if (mx.cfg.on) fv_note_launch(), kbm_flush<T><<<G, TB, 0, st>>>(tl, mx.x64, v.d);
-    FV_CUDA_TRY(cudaGetLastError());
-    return FV_OK;
-}
-
-template <typename T>
-fv_status inner_bicg(fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, int G, const Tiles &tl,
-                     cudaStream_t st, int64_t &launched_iters, const MixedArgs &mx) {
-    const fv_csr *A = B->A;
-    const int *skip = &B->G->all_done;
-    fv_note_launch(), kbb_init<T><<<G, TB, 0, st>>>(tl, v.r, v.d, v.rh, v.p, B->partial, B->S, B->G);
-    FV_CUDA_TRY(cudaGetLastError());
-    for (bool done = false; !done;) {
-        for (int q = 0; q < 4; ++q) {
+    } else {
+        for (int q = 0; q < kGroupBiCG; ++q) {
             FV_TRY(precond<T>(B, P, v.p, v.y, st, skip));
             fv_note_launch(), kbb_spmv1<T><<<G, TB, 0, st>>>(tl, A->row_ptr, A->cols, vals, v.y, v.v, v.rh,
                                                             B->partial, B->S, B->G);
@@ -809,9 +874,22 @@ fv_status inner_bicg(fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, 
             fv_note_launch(), kbb_p<T><<<G, TB, 0, st>>>(tl, v.r, v.v, v.p, v.rh, B->S);
             ++launched_iters;
         }
+    }
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+// A whole inner solve of the problems not done (the FP64 pass over the
+// problems a mixed run could not finish).
+template <typename T>
+fv_status inner_solve(bool bicg, fv_batch *B, fv_precond *P, const T *vals, InnerVecs<T> v, int G, const Tiles &tl,
+                      cudaStream_t st, int64_t &launched_iters, const MixedArgs &mx) {
+    FV_TRY(inner_start<T>(bicg, B, P, v, G, tl, st));
+    for (bool done = false; !done;) {
+        FV_TRY(inner_group<T>(bicg, B, P, vals, v, G, tl, st, launched_iters, mx));
         FV_TRY(wait_all_done(B, st, done));
     }
-    fv_note_launch(), kbb_finish<T><<<G, TB, 0, st>>>(tl, v.d, v.h, B->S);
+    if (bicg) fv_note_launch(), kbb_finish<T><<<G, TB, 0, st>>>(tl, v.d, v.h, B->S);
     if (mx.cfg.on) fv_note_launch(), kbm_flush<T><<<G, TB, 0, st>>>(tl, mx.x64, v.d);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
@@ -849,22 +927,40 @@ InnerVecs<T> carve(void *mem, int64_t n, T *d) {
     return v;
 }
 
-fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, double *x, const fv_batch_options *opt,
-                      fv_batch_info *info, cudaStream_t st) {
+int grid_of(const fv_batch *B) { return (int)std::min<int64_t>(B->ntiles, 148 * 8); }
+
+Tiles tiles_of(const fv_batch *B) { return Tiles{B->ntiles, B->tile_prob, B->tile_row0, B->tile_row1, B->ptile}; }
+
+fv_status ensure_bytes(void *&p, size_t &have, size_t need) {
+    if (have >= need) return FV_OK;
+    cudaFree(p);
+    p = nullptr;
+    have = 0;
+    FV_CUDA_TRY(cudaMalloc(&p, need));
+    have = need;
+    return FV_OK;
+}
+
+fv_status download_state(fv_batch *B, cudaStream_t st) {
+    B->hs.resize(B->np);
+    FV_CUDA_TRY(cudaMemcpyAsync(B->hs.data(), B->S, sizeof(BProb) * B->np, cudaMemcpyDeviceToHost, st));
+    FV_CUDA_TRY(cudaStreamSynchronize(st));
+    return FV_OK;
+}
+
+// Start a run: every problem from x0 = 0, except those that from_problem maps
+// to a running problem of `from`, whose state (the Krylov vectors' rows, x's
+// rows and the per-problem scalars) is carried over unchanged.  Those are held
+// as done while the new problems are initialised, then run again.
+fv_status run_begin(fv_batch *B, fv_precond *P, bool bicg, const double *b, double *x, const fv_batch_options *opt,
+                    const fv_batch *from, const int32_t *from_problem, cudaStream_t st) {
     if (!B || !P || !b || !x || !opt || opt->max_iterations < 0) return FV_ERR_INVALID;
+    if (opt->precision != FV_BATCH_FP64 && opt->precision != FV_BATCH_MIXED) return FV_ERR_INVALID;
     const int64_t n = B->n;
     const int np = B->np;
-    const int G = (int)std::min<int64_t>(B->ntiles, 148 * 8);
-    Tiles tl{B->ntiles, B->tile_prob, B->tile_row0, B->tile_row1, B->ptile};
     const bool mixed = opt->precision == FV_BATCH_MIXED;
-    const size_t need = mixed ? sizeof(float) * 11 * (size_t)n : sizeof(double) * 10 * (size_t)n;
-    if (B->vec_bytes < need) {
-        cudaFree(B->vec);
-        B->vec = nullptr;
-        B->vec_bytes = 0;
-        FV_CUDA_TRY(cudaMalloc(&B->vec, need));
-        B->vec_bytes = need;
-    }
+    std::vector<int32_t> list;
+    std::vector<int64_t> seg;
     std::vector<BProb> hs(np);
     for (int p = 0; p < np; ++p) {
         BProb q{};
@@ -875,81 +971,198 @@ fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, do
         q.max_it = opt->max_iterations;
         hs[p] = q;
     }
+    if (from_problem) {
+        // the carried-over problems must run the same iteration in the new batch:
+        // same method, precision, mixed-precision settings and tile partition
+        if (!from || from == B || !from->run || from->bicg != bicg || from->mixed != mixed || from->tile != B->tile ||
+            (int)from->hs.size() != from->np)
+            return FV_ERR_INVALID;
+        if (mixed && (from->opt.outer_tolerance != opt->outer_tolerance ||
+                      from->opt.inner_relative_tolerance != opt->inner_relative_tolerance))
+            return FV_ERR_INVALID;
+        std::vector<char> used((size_t)from->np, 0);
+        for (int p = 0; p < np; ++p) {
+            const int32_t sp = from_problem[p];
+            if (sp < 0) continue;
+            if (sp >= from->np || used[sp] || from->hs[sp].done) return FV_ERR_INVALID;
+            const int64_t len = B->off[p + 1] - B->off[p];
+            if (from->off[sp + 1] - from->off[sp] != len) return FV_ERR_INVALID;
+            used[sp] = 1;
+            list.push_back(p);
+            seg.insert(seg.end(), {from->off[sp], B->off[p], len});
+            hs[p] = from->hs[sp];
+            hs[p].done = 1;  // held while the new problems start
+            hs[p].ticket = 0;
+        }
+    }
+    const int nfresh = np - (int)list.size();
+    B->run = false;
+    FV_TRY(ensure_bytes(B->vec, B->vec_bytes, mixed ? sizeof(float) * 11 * (size_t)n : sizeof(double) * 10 * (size_t)n));
     FV_CUDA_TRY(cudaMemcpyAsync(B->S, hs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
-    BGlobal g0{np, 0, np, 0};
+    BGlobal g0{nfresh, nfresh == 0 ? 1 : 0, {0, 0}};
     FV_CUDA_TRY(cudaMemcpyAsync(B->G, &g0, sizeof(BGlobal), cudaMemcpyHostToDevice, st));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
-    int64_t iters_launched = 0;
-    fv_status s = FV_OK;
-    std::vector<int> fallback;
+    if (!list.empty()) {
+        cudaFree(B->seg);
+        cudaFree(B->resume);
+        B->seg = nullptr;
+        B->resume = nullptr;
+        FV_CUDA_TRY(cudaMalloc(&B->seg, sizeof(int64_t) * seg.size()));
+        FV_CUDA_TRY(cudaMalloc(&B->resume, sizeof(int32_t) * list.size()));
+        FV_CUDA_TRY(cudaMemcpyAsync(B->seg, seg.data(), sizeof(int64_t) * seg.size(), cudaMemcpyHostToDevice, st));
+        FV_CUDA_TRY(
+            cudaMemcpyAsync(B->resume, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, st));
+    }
+    const int nseg = (int)list.size();
+    const dim3 ag(32, (unsigned)std::min(nseg, 65535));
+    const int G = grid_of(B);
+    const Tiles tl = tiles_of(B);
     if (!mixed) {
         InnerVecs<double> v = carve<double>(B->vec, n, x);
         FV_CUDA_TRY(cudaMemcpyAsync(v.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        MixedArgs none{MixedCfg{0, 0.0, 0.0}, nullptr, nullptr};
-        s = bicg ? inner_bicg<double>(B, P, B->A->vals, v, G, tl, st, iters_launched, none)
-                 : inner_cg<double>(B, P, B->A->vals, v, G, tl, st, iters_launched, none);
+        if (nseg) {
+            const InnerVecs<double> u = carve<double>(from->vec, from->n, from->x);
+            fv_note_launch(), kb_adopt<double><<<ag, 256, 0, st>>>(B->seg, nseg, u.r, v.r);
+            fv_note_launch(), kb_adopt<double><<<ag, 256, 0, st>>>(B->seg, nseg, u.p, v.p);
+            fv_note_launch(), kb_adopt<double><<<ag, 256, 0, st>>>(B->seg, nseg, u.d, v.d);
+            if (bicg) fv_note_launch(), kb_adopt<double><<<ag, 256, 0, st>>>(B->seg, nseg, u.rh, v.rh);
+        }
+        FV_TRY(inner_start<double>(bicg, B, P, v, G, tl, st));
     } else {
         if (!B->a32) FV_CUDA_TRY(cudaMalloc(&B->a32, sizeof(float) * (B->A->nnz ? B->A->nnz : 1)));
         fv_note_launch(), k_to_f32b<<<148 * 8, 256, 0, st>>>(B->A->nnz, B->A->vals, B->a32);
         FV_TRY(fv_precond_make_f32(P, st));
         InnerVecs<float> v = carve<float>(B->vec, n, nullptr);
+        if (nseg) {
+            const InnerVecs<float> u = carve<float>(from->vec, from->n, nullptr);
+            fv_note_launch(), kb_adopt<float><<<ag, 256, 0, st>>>(B->seg, nseg, u.r, v.r);
+            fv_note_launch(), kb_adopt<float><<<ag, 256, 0, st>>>(B->seg, nseg, u.p, v.p);
+            fv_note_launch(), kb_adopt<float><<<ag, 256, 0, st>>>(B->seg, nseg, u.d, v.d);
+            if (bicg) fv_note_launch(), kb_adopt<float><<<ag, 256, 0, st>>>(B->seg, nseg, u.rh, v.rh);
+            fv_note_launch(), kb_adopt<double><<<ag, 256, 0, st>>>(B->seg, nseg, from->x, x);
+        }
         fv_note_launch(), kbm_init<<<G, TB, 0, st>>>(tl, b, x, v.r, B->partial, B->S, B->G);
-        MixedArgs mx{MixedCfg{1, opt->outer_tolerance, opt->inner_relative_tolerance}, x, b};
-        s = bicg ? inner_bicg<float>(B, P, B->a32, v, G, tl, st, iters_launched, mx)
-                 : inner_cg<float>(B, P, B->a32, v, G, tl, st, iters_launched, mx);
-        // FP64 fallback for the problems the FP32 run could not finish
-        if (s == FV_OK) {
-            FV_CUDA_TRY(cudaMemcpyAsync(hs.data(), B->S, sizeof(BProb) * np, cudaMemcpyDeviceToHost, st));
-            FV_CUDA_TRY(cudaStreamSynchronize(st));
-            fallback.assign(np, 0);
-            int nfail = 0;
-            for (int p = 0; p < np; ++p)
-                if (hs[p].stagnated || !(hs[p].res64 <= opt->outer_tolerance)) {
-                    fallback[p] = 1;
-                    ++nfail;
-                }
-            if (nfail) {
-                std::vector<BProb> fs(np);
-                for (int p = 0; p < np; ++p) {
-                    BProb q{};
-                    q.tol = opt->outer_tolerance;
-                    q.rtol = opt->outer_tolerance;
-                    q.max_it = opt->max_iterations;
-                    q.done = fallback[p] ? 0 : 1;
-                    q.bnorm64 = hs[p].bnorm64;
-                    fs[p] = q;
-                }
-                FV_CUDA_TRY(cudaMemcpyAsync(B->S, fs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
-                BGlobal g1{nfail, 0, nfail, 0};
-                FV_CUDA_TRY(cudaMemcpyAsync(B->G, &g1, sizeof(BGlobal), cudaMemcpyHostToDevice, st));
-                const size_t need64 = sizeof(double) * 10 * (size_t)n;
-                if (B->vec64_bytes < need64) {
-                    cudaFree(B->vec64);
-                    B->vec64 = nullptr;
-                    B->vec64_bytes = 0;
-                    FV_CUDA_TRY(cudaMalloc(&B->vec64, need64));
-                    B->vec64_bytes = need64;
-                }
-                InnerVecs<double> w = carve<double>(B->vec64, n, x);
-                FV_CUDA_TRY(cudaMemcpyAsync(w.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-                MixedArgs none{MixedCfg{0, 0.0, 0.0}, nullptr, nullptr};
-                s = bicg ? inner_bicg<double>(B, P, B->A->vals, w, G, tl, st, iters_launched, none)
-                         : inner_cg<double>(B, P, B->A->vals, w, G, tl, st, iters_launched, none);
-                if (s == FV_OK) {
-                    std::vector<BProb> f2(np);
-                    FV_CUDA_TRY(cudaMemcpyAsync(f2.data(), B->S, sizeof(BProb) * np, cudaMemcpyDeviceToHost, st));
-                    FV_CUDA_TRY(cudaStreamSynchronize(st));
-                    for (int p = 0; p < np; ++p)
-                        if (fallback[p]) {
-                            hs[p].iter += f2[p].iter;
-                            hs[p].res64 = f2[p].error;  // |r|/|b| of the FP64 CG/BiCGStab
-                            hs[p].breakdown = f2[p].breakdown;
-                        }
-                    FV_CUDA_TRY(cudaMemcpyAsync(B->S, hs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
-                }
+        FV_TRY(inner_start<float>(bicg, B, P, v, G, tl, st));
+    }
+    if (nseg) fv_note_launch(), kb_resume<<<(nseg + 255) / 256, 256, 0, st>>>(B->resume, nseg, B->S, B->G);
+    FV_CUDA_TRY(cudaGetLastError());
+    FV_TRY(download_state(B, st));
+    B->run = true;
+    B->bicg = bicg;
+    B->mixed = mixed;
+    B->P = P;
+    B->b = b;
+    B->x = x;
+    B->opt = *opt;
+    B->launched = 0;
+    return FV_OK;
+}
+
+// Up to max_iterations more iterations (whole groups) until every problem is
+// done; the problems that retired get their result, and the state is read back.
+fv_status run_advance(fv_batch *B, int64_t max_iterations, cudaStream_t st) {
+    if (!B || !B->run || max_iterations < 0) return FV_ERR_INVALID;
+    const int64_t n = B->n;
+    const int G = grid_of(B);
+    const Tiles tl = tiles_of(B);
+    bool done = true;
+    for (const BProb &q : B->hs) done = done && q.done;
+    const int group = B->bicg ? kGroupBiCG : kGroupCG;
+    int64_t it = 0;
+    if (B->mixed) {
+        InnerVecs<float> v = carve<float>(B->vec, n, nullptr);
+        const MixedArgs mx{MixedCfg{1, B->opt.outer_tolerance, B->opt.inner_relative_tolerance}, B->x, B->b};
+        for (; !done && it < max_iterations; it += group) {
+            FV_TRY(inner_group<float>(B->bicg, B, B->P, B->a32, v, G, tl, st, B->launched, mx));
+            FV_TRY(wait_all_done(B, st, done));
+        }
+        fv_note_launch(), kb_finalize<float><<<G, TB, 0, st>>>(tl, v.d, nullptr, B->x, B->S);
+    } else {
+        InnerVecs<double> v = carve<double>(B->vec, n, B->x);
+        const MixedArgs none{MixedCfg{0, 0.0, 0.0}, nullptr, nullptr};
+        for (; !done && it < max_iterations; it += group) {
+            FV_TRY(inner_group<double>(B->bicg, B, B->P, B->A->vals, v, G, tl, st, B->launched, none));
+            FV_TRY(wait_all_done(B, st, done));
+        }
+        fv_note_launch(), kb_finalize<double><<<G, TB, 0, st>>>(tl, v.d, B->bicg ? v.h : nullptr, nullptr, B->S);
+    }
+    fv_note_launch(), kb_mark_fin<<<(B->np + 255) / 256, 256, 0, st>>>(B->np, B->S);
+    FV_CUDA_TRY(cudaGetLastError());
+    return download_state(B, st);
+}
+
+// Per-problem results from the host copy of the state.  fallback[p]: the
+// problem was finished by the FP64 pass (whole-batch solves) -- or, for a
+// stepwise run, the FP32 run stagnated and left it unfinished.
+void fill_info(const fv_batch *B, fv_batch_info *info, const std::vector<int> &fallback) {
+    if (!info) return;
+    info->launched_iterations = B->launched;
+    const bool mixed = B->mixed;
+    for (int p = 0; p < B->np; ++p) {
+        const BProb &q = B->hs[p];
+        if (info->iterations) info->iterations[p] = q.iter;
+        if (info->outer_steps) info->outer_steps[p] = mixed ? q.n_replace : 0;
+        if (info->final_residual) info->final_residual[p] = mixed ? q.res64 : q.error;
+        if (info->status)
+            info->status[p] = (q.breakdown || !std::isfinite(mixed ? q.res64 : q.error)) ? FV_ERR_BREAKDOWN : FV_OK;
+        if (info->fp64_fallback) info->fp64_fallback[p] = fallback.empty() ? 0 : fallback[p];
+    }
+}
+
+fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, double *x, const fv_batch_options *opt,
+                      fv_batch_info *info, cudaStream_t st) {
+    if (!B || !P || !b || !x || !opt || opt->max_iterations < 0) return FV_ERR_INVALID;
+    const int64_t n = B->n;
+    const int np = B->np;
+    const int G = grid_of(B);
+    const Tiles tl = tiles_of(B);
+    const bool mixed = opt->precision == FV_BATCH_MIXED;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    fv_status s = run_begin(B, P, bicg, b, x, opt, nullptr, nullptr, st);
+    if (s == FV_OK) s = run_advance(B, INT64_MAX, st);
+    std::vector<int> fallback;
+    std::vector<BProb> &hs = B->hs;
+    // FP64 pass for the problems the FP32 run could not finish (from x0 = 0)
+    if (s == FV_OK && mixed) {
+        fallback.assign(np, 0);
+        int nfail = 0;
+        for (int p = 0; p < np; ++p)
+            if (hs[p].stagnated || !(hs[p].res64 <= opt->outer_tolerance)) {
+                fallback[p] = 1;
+                ++nfail;
+            }
+        if (nfail) {
+            std::vector<BProb> fs(np);
+            for (int p = 0; p < np; ++p) {
+                BProb q{};
+                q.tol = opt->outer_tolerance;
+                q.rtol = opt->outer_tolerance;
+                q.max_it = opt->max_iterations;
+                q.done = fallback[p] ? 0 : 1;
+                q.bnorm64 = hs[p].bnorm64;
+                fs[p] = q;
+            }
+            FV_CUDA_TRY(cudaMemcpyAsync(B->S, fs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
+            BGlobal g1{nfail, 0, {0, 0}};
+            FV_CUDA_TRY(cudaMemcpyAsync(B->G, &g1, sizeof(BGlobal), cudaMemcpyHostToDevice, st));
+            FV_TRY(ensure_bytes(B->vec64, B->vec64_bytes, sizeof(double) * 10 * (size_t)n));
+            InnerVecs<double> w = carve<double>(B->vec64, n, x);
+            FV_CUDA_TRY(cudaMemcpyAsync(w.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            const MixedArgs none{MixedCfg{0, 0.0, 0.0}, nullptr, nullptr};
+            s = inner_solve<double>(bicg, B, P, B->A->vals, w, G, tl, st, B->launched, none);
+            if (s == FV_OK) {
+                std::vector<BProb> f2(np);
+                FV_CUDA_TRY(cudaMemcpyAsync(f2.data(), B->S, sizeof(BProb) * np, cudaMemcpyDeviceToHost, st));
+                FV_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int p = 0; p < np; ++p)
+                    if (fallback[p]) {
+                        hs[p].iter += f2[p].iter;
+                        hs[p].res64 = f2[p].error;  // |r|/|b| of the FP64 CG/BiCGStab
+                        hs[p].breakdown = f2[p].breakdown;
+                    }
+                FV_CUDA_TRY(cudaMemcpyAsync(B->S, hs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
             }
         }
     }
@@ -959,22 +1172,11 @@ fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, do
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    B->run = false;  // the state was overwritten by the FP64 pass: nothing to carry over
     if (s == FV_OK) s = fv_precond_check_error(P, st);
-    FV_CUDA_TRY(cudaMemcpyAsync(hs.data(), B->S, sizeof(BProb) * np, cudaMemcpyDeviceToHost, st));
-    FV_CUDA_TRY(cudaStreamSynchronize(st));
-    if (info) {
+    if (s == FV_OK && info) {
+        fill_info(B, info, fallback);
         info->device_ms = ms;
-        info->launched_iterations = iters_launched;
-        for (int p = 0; p < np; ++p) {
-            if (info->iterations) info->iterations[p] = hs[p].iter;
-            if (info->outer_steps) info->outer_steps[p] = mixed ? hs[p].n_replace : 0;
-            if (info->final_residual) info->final_residual[p] = mixed ? hs[p].res64 : hs[p].error;
-            if (info->status)
-                info->status[p] = (hs[p].breakdown || !std::isfinite(mixed ? hs[p].res64 : hs[p].error))
-                                      ? FV_ERR_BREAKDOWN
-                                      : FV_OK;
-            if (info->fp64_fallback) info->fp64_fallback[p] = fallback.empty() ? 0 : fallback[p];
-        }
     }
     return s;
 }
@@ -989,4 +1191,38 @@ extern "C" fv_status fv_batch_cg(fv_batch *B, fv_precond *P, const double *b, do
 extern "C" fv_status fv_batch_bicgstab(fv_batch *B, fv_precond *P, const double *b, double *x,
                                        const fv_batch_options *opt, fv_batch_info *info, void *stream) {
     return fv_host_guard([&] { return batch_solve(true, B, P, b, x, opt, info, fv_stream(stream)); });
+}
+
+extern "C" fv_status fv_batch_begin(fv_batch *B, fv_precond *P, int32_t method, const double *b, double *x,
+                                    const fv_batch_options *opt, const fv_batch *from, const int32_t *from_problem,
+                                    void *stream) {
+    if (method != FV_BATCH_CG && method != FV_BATCH_BICGSTAB) return FV_ERR_INVALID;
+    return fv_host_guard([&] {
+        return run_begin(B, P, method == FV_BATCH_BICGSTAB, b, x, opt, from, from_problem, fv_stream(stream));
+    });
+}
+
+extern "C" fv_status fv_batch_advance(fv_batch *B, int64_t max_iterations, int32_t *n_running, int32_t *done,
+                                      void *stream) {
+    return fv_host_guard([&] {
+        FV_TRY(run_advance(B, max_iterations, fv_stream(stream)));
+        int32_t running = 0;
+        for (int p = 0; p < B->np; ++p) {
+            running += B->hs[p].done ? 0 : 1;
+            if (done) done[p] = B->hs[p].done ? 1 : 0;
+        }
+        if (n_running) *n_running = running;
+        return FV_OK;
+    });
+}
+
+extern "C" fv_status fv_batch_report(const fv_batch *B, fv_batch_info *info) {
+    if (!B || !B->run || !info) return FV_ERR_INVALID;
+    return fv_host_guard([&] {
+        std::vector<int> stalled(B->np, 0);
+        for (int p = 0; p < B->np; ++p) stalled[p] = B->mixed && B->hs[p].stagnated;
+        fill_info(B, info, stalled);
+        info->device_ms = 0.0;
+        return FV_OK;
+    });
 }

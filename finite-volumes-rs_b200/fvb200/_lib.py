@@ -177,6 +177,9 @@ _SIGS = {
     "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_bicgstab": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_destroy": [vp],
+    "fv_batch_begin": [vp, vp, C.c_int32, vp, vp, P(BatchOptions), vp, P(C.c_int32), vp],
+    "fv_batch_advance": [vp, C.c_int64, P(C.c_int32), P(C.c_int32), vp],
+    "fv_batch_report": [vp, P(BatchInfo)],
     "fv_csr_square_block": [vp, vp, P(vp)],
     "fv_dist_create": [vp, i64, ip, i64, P(FvComm), P(vp)],
     "fv_dist_destroy": [vp],

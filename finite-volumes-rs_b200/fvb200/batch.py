@@ -123,25 +123,77 @@ class BatchCG:
         check(lib().fv_batch_create(A.handle, self.n_problems, self.row_offsets.ctypes.data_as(C.POINTER(C.c_int64)),
                                     tile_rows, stream_handle(stream), C.byref(self.handle)), "fv_batch_create")
 
+    @staticmethod
+    def _options(precision, relative_tolerance, absolute_tolerance, max_iterations, inner_relative_tolerance,
+                 outer_tolerance, max_outer):
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', not {precision!r}")
+        return BatchOptions(FV_BATCH_MIXED if precision == "mixed" else FV_BATCH_FP64, relative_tolerance,
+                            absolute_tolerance, max_iterations, inner_relative_tolerance, outer_tolerance, max_outer)
+
+    def _info(self):
+        n = self.n_problems
+        arrs = dict(iterations=np.zeros(n, np.int64), outer_steps=np.zeros(n, np.int32), final_residual=np.zeros(n),
+                    status=np.zeros(n, np.int32), fp64_fallback=np.zeros(n, np.int32))
+        info = BatchInfo(0.0, 0, arrs["iterations"].ctypes.data_as(C.POINTER(C.c_int64)),
+                         arrs["outer_steps"].ctypes.data_as(C.POINTER(C.c_int32)),
+                         arrs["final_residual"].ctypes.data_as(C.POINTER(C.c_double)),
+                         arrs["status"].ctypes.data_as(C.POINTER(C.c_int32)),
+                         arrs["fp64_fallback"].ctypes.data_as(C.POINTER(C.c_int32)))
+        return info, arrs
+
     def solve(self, P, b, x, precision: str = "mixed", relative_tolerance=1e-8, absolute_tolerance=1e-8,
               max_iterations=10000, inner_relative_tolerance=1e-2, outer_tolerance=1e-10, max_outer=30,
               stream=None, solver: str = "cg"):
-        o = BatchOptions(FV_BATCH_MIXED if precision == "mixed" else FV_BATCH_FP64, relative_tolerance,
-                         absolute_tolerance, max_iterations, inner_relative_tolerance, outer_tolerance, max_outer)
-        n = self.n_problems
-        its = np.zeros(n, np.int64)
-        outer = np.zeros(n, np.int32)
-        res = np.zeros(n)
-        stat = np.zeros(n, np.int32)
-        fb = np.zeros(n, np.int32)
-        info = BatchInfo(0.0, 0, its.ctypes.data_as(C.POINTER(C.c_int64)), outer.ctypes.data_as(C.POINTER(C.c_int32)),
-                         res.ctypes.data_as(C.POINTER(C.c_double)), stat.ctypes.data_as(C.POINTER(C.c_int32)),
-                         fb.ctypes.data_as(C.POINTER(C.c_int32)))
+        if solver not in ("cg", "bicgstab"):
+            raise ValueError(f"solver must be 'cg' or 'bicgstab', not {solver!r}")
+        o = self._options(precision, relative_tolerance, absolute_tolerance, max_iterations,
+                          inner_relative_tolerance, outer_tolerance, max_outer)
+        info, arrs = self._info()
         fn = lib().fv_batch_bicgstab if solver == "bicgstab" else lib().fv_batch_cg
         check(fn(self.handle, P.handle, C.c_void_p(b.data.data_ptr()), C.c_void_p(x.data.data_ptr()), C.byref(o),
                  C.byref(info), stream_handle(stream)), "fv_batch_" + solver)
-        return dict(iterations=its, outer_steps=outer, final_residual=res, status=stat, device_ms=info.device_ms,
-                    launched_iterations=info.launched_iterations, fp64_fallback=fb)
+        return dict(arrs, device_ms=info.device_ms, launched_iterations=info.launched_iterations)
+
+    # ---- stepwise runs (continuous batching): fv_batch_begin / _advance / _report
+    def begin(self, P, b, x, precision: str = "mixed", relative_tolerance=1e-8, absolute_tolerance=1e-8,
+              max_iterations=10000, inner_relative_tolerance=1e-2, outer_tolerance=1e-10, stream=None,
+              solver: str = "cg", carry_from: "BatchCG | None" = None, carry=None):
+        """Start a run.  carry[p] = q >= 0 continues problem q of the running
+        batch `carry_from` as problem p (its state copied bit for bit); -1
+        starts p from x0 = 0.  P, b and x must stay alive for the whole run."""
+        if solver not in ("cg", "bicgstab"):
+            raise ValueError(f"solver must be 'cg' or 'bicgstab', not {solver!r}")
+        o = self._options(precision, relative_tolerance, absolute_tolerance, max_iterations,
+                          inner_relative_tolerance, outer_tolerance, 0)
+        cmap = None
+        if carry is not None:
+            cmap = np.ascontiguousarray(carry, dtype=np.int32)
+            if cmap.shape != (self.n_problems,) or carry_from is None:
+                raise ValueError("carry needs one entry per problem and carry_from")
+        method = 1 if solver == "bicgstab" else 0
+        check(lib().fv_batch_begin(self.handle, P.handle, method, C.c_void_p(b.data.data_ptr()),
+                                   C.c_void_p(x.data.data_ptr()), C.byref(o),
+                                   carry_from.handle if carry_from is not None else None,
+                                   cmap.ctypes.data_as(C.POINTER(C.c_int32)) if cmap is not None else None,
+                                   stream_handle(stream)), "fv_batch_begin")
+        self._run = (P, b, x)  # keep the run's operands alive
+
+    def advance(self, max_iterations: int, stream=None):
+        """Up to max_iterations more iterations; returns (running count, done flags)."""
+        done = np.zeros(self.n_problems, np.int32)
+        running = C.c_int32(0)
+        check(lib().fv_batch_advance(self.handle, int(max_iterations), C.byref(running),
+                                     done.ctypes.data_as(C.POINTER(C.c_int32)), stream_handle(stream)),
+              "fv_batch_advance")
+        return int(running.value), done.astype(bool)
+
+    def report(self):
+        """Per-problem iterations / residuals / status of the current run
+        (fp64_fallback: the FP32 run stagnated and left the problem unfinished)."""
+        info, arrs = self._info()
+        check(lib().fv_batch_report(self.handle, C.byref(info)), "fv_batch_report")
+        return dict(arrs, launched_iterations=info.launched_iterations)
 
     def close(self):
         if self.handle:

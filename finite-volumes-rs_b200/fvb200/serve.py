@@ -56,6 +56,7 @@ class Request:
     residual: float = float("nan")
     solution: np.ndarray | None = None
     error: str | None = None
+    fields: tuple | None = dataclasses.field(default=None, repr=False, compare=False)  # while in a run
 
 
 def request_stream(rate: float, duration: float, seed: int, mix_3d: float = 0.5, lo: float = 1e4,
@@ -144,34 +145,52 @@ def request_fields(m, req: Request):
 BYTES_PER_CELL = {"2d": 700, "3d": 1100}   # resident estimate: mesh, CSR, factors, FP32 copies, vectors
 
 
+def wave_system(fv, cache, reqs: list[Request], stream, ordering="boxes", keep_fields=False):
+    """The block-diagonal system of requests of one kind on `stream`: the
+    joined mesh, A, b and the IC(0) (2D) / ILU(0) (3D) of A.  ordering "boxes":
+    every request's factor in its own box-colour order (the union then has the
+    largest request's level count); None: natural order.  Every request's rows
+    are the same bits in any wave.  keep_fields: the request's generated fields
+    stay on it (r.fields) for the next wave it joins."""
+    kind = reqs[0].kind
+    meshes = [cache.get(r.kind, r.side) for r in reqs]
+    todo = [k for k, r in enumerate(reqs) if r.fields is None]
+    if todo:  # per-request fields on host threads (the generator releases the GIL)
+        with ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
+            got = list(ex.map(lambda k: request_fields(meshes[k], reqs[k]), todo))
+    else:
+        got = []
+    fields = [r.fields for r in reqs]
+    for k, f in zip(todo, got):
+        fields[k] = f
+        if keep_fields:
+            reqs[k].fields = f
+    kfs, fls, scs = (list(x) for x in zip(*fields))
+    mb = MeshBatch(meshes)
+    kf = mb.face_field(kfs)
+    sc = mb.cell_field(scs)
+    nb = mb.n_boundary_faces
+    bc = (np.zeros(nb), np.zeros(nb))
+    if kind == "2d":
+        eq = -fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+    else:
+        fl = mb.face_field(fls)
+        eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
+    A, b = fv.assemble(eq, bc, mb, stream=stream)
+    P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(
+        A, 0, stream=stream, ordering=ordering, offsets=mb.cell_offsets if ordering else None)
+    return mb, A, b, P
+
+
 def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol=1e-10, keep_solution=False,
                precision="mixed", ordering="boxes"):
     """Pack requests of one kind into one batch and solve it on `stream` to
     |b - A x| / |b| <= outer_tol per request: FP32 Krylov inside FP64
-    refinement (precision "mixed") or FP64 throughout ("fp64").  ordering
-    "boxes": every request's IC(0)/ILU(0) in its own box-colour order (the
-    union then has the largest request's level count); None: natural order."""
+    refinement (precision "mixed") or FP64 throughout ("fp64")."""
     import torch
     kind = reqs[0].kind
     with torch.cuda.stream(stream):
-        meshes = [cache.get(r.kind, r.side) for r in reqs]
-        # per-request fields on host threads (the generator releases the GIL)
-        with ThreadPoolExecutor(max_workers=min(8, len(reqs))) as ex:
-            fields = list(ex.map(lambda mr: request_fields(*mr), zip(meshes, reqs)))
-        kfs, fls, scs = (list(x) for x in zip(*fields))
-        mb = MeshBatch(meshes)
-        kf = mb.face_field(kfs)
-        sc = mb.cell_field(scs)
-        nb = mb.n_boundary_faces
-        bc = (np.zeros(nb), np.zeros(nb))
-        if kind == "2d":
-            eq = -fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
-        else:
-            fl = mb.face_field(fls)
-            eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
-        A, b = fv.assemble(eq, bc, mb, stream=stream)
-        P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(
-            A, 0, stream=stream, ordering=ordering, offsets=mb.cell_offsets if ordering else None)
+        mb, A, b, P = wave_system(fv, cache, reqs, stream, ordering)
         x = fv.DistributedVector.from_size(mb.n_cells)
         solver = BatchCG(A, mb.cell_offsets, tile_rows, stream=stream)
         if precision == "mixed":
@@ -197,16 +216,115 @@ def solve_wave(fv, cache, reqs: list[Request], stream, tile_rows=1024, outer_tol
     return out
 
 
+class WaveRun:
+    """A running wave of requests of one kind, solved stepwise
+    (fv_batch_begin / fv_batch_advance).  Built over `reqs`; the requests that
+    were running in `prev` continue from their state there (their rows of x and
+    of the Krylov vectors and their scalars are carried over bit for bit), the
+    others start from x0 = 0.  So a request admitted into a running wave, and
+    the requests it joins, give the same result as alone."""
+
+    def __init__(self, fv, cache, reqs: list[Request], stream, prev: "WaveRun | None" = None, tile_rows=1024,
+                 outer_tol=1e-10, precision="mixed", ordering="boxes", keep_solution=False):
+        import torch
+        self.fv, self.stream, self.reqs = fv, stream, list(reqs)
+        self.kind = reqs[0].kind
+        self.keep_solution = keep_solution
+        self.precision = precision
+        self.index = {r.rid: k for k, r in enumerate(self.reqs)}
+        self.done = np.zeros(len(self.reqs), bool)
+        with torch.cuda.stream(stream):
+            self.mb, self.A, self.b, self.P = wave_system(fv, cache, self.reqs, stream, ordering, keep_fields=True)
+            self.x = fv.DistributedVector.from_size(self.mb.n_cells)
+            self.solver = BatchCG(self.A, self.mb.cell_offsets, tile_rows, stream=stream)
+            carry = None
+            if prev is not None:
+                carry = np.array([prev.index.get(r.rid, -1) for r in self.reqs], np.int32)
+                for k, q in enumerate(carry):
+                    if q >= 0 and prev.done[q]:
+                        raise ValueError(f"request {self.reqs[k].rid} has finished in the previous wave")
+            common = dict(max_iterations=20000, stream=stream, solver="cg" if self.kind == "2d" else "bicgstab",
+                          carry_from=prev.solver if prev is not None else None, carry=carry)
+            if precision == "mixed":
+                self.solver.begin(self.P, self.b, self.x, precision="mixed", outer_tolerance=outer_tol,
+                                  inner_relative_tolerance=1e-2, **common)
+            else:
+                self.solver.begin(self.P, self.b, self.x, precision="fp64", relative_tolerance=outer_tol,
+                                  absolute_tolerance=outer_tol, **common)
+
+    @property
+    def cells(self) -> int:
+        return int(sum(r.cells for r, d in zip(self.reqs, self.done) if not d))
+
+    def running(self) -> list[Request]:
+        return [r for r, d in zip(self.reqs, self.done) if not d]
+
+    def advance(self, iterations: int):
+        """Up to `iterations` more iterations.  Returns (finished, stalled): the
+        requests that finished (iterations, residual and, with keep_solution,
+        the solution recorded on them) and those whose FP32 run stagnated
+        (mixed precision; to be solved again in FP64)."""
+        running, done = self.solver.advance(iterations, stream=self.stream)
+        new = np.flatnonzero(done & ~self.done)
+        if len(new) == 0:
+            return [], []
+        rep = self.solver.report()
+        off = self.mb.cell_offsets
+        finished, stalled = [], []
+        for k in new:
+            r = self.reqs[k]
+            r.iterations = int(rep["iterations"][k])
+            r.residual = float(rep["final_residual"][k])
+            r.fields = None
+            if rep["status"][k] != 0:
+                r.error = f"status {int(rep['status'][k])}"
+            if self.keep_solution:
+                r.solution = self.x.data[off[k]:off[k + 1]].cpu().numpy()
+            (stalled if rep["fp64_fallback"][k] else finished).append(r)
+        self.done[new] = True
+        return finished, stalled
+
+    def close(self):
+        self.solver.close()
+        self.P.close()
+        self.A.close()
+        self.mb = None
+
+
 class Server:
     """solve_fn(fv, cache, wave, stream) solves a wave in place (default: solve_wave);
-    it is a parameter so the scheduling can be exercised without a GPU."""
+    it is a parameter so the scheduling can be exercised without a GPU.
+
+    refill=True serves with slot refill instead of whole waves: a worker runs
+    a WaveRun (run_fn(fv, cache, reqs, stream, prev=...), default WaveRun) of
+    one kind, advancing it `advance_iterations` iterations at a time; every
+    request that finished leaves at once, and when the requests finished since
+    the wave was last built hold `refill_fraction` of its cells (or of its
+    requests) and admitted requests of the same kind wait, the wave is rebuilt
+    over its running requests -- which continue from their state -- plus the
+    waiting requests, in arrival order, up to max_wave_cells /
+    max_wave_requests.  A wave takes refills for `run_max_s` seconds, then
+    drains, so that the other kind is served too; worker k prefers kind
+    ("3d", "2d")[k % 2].  A request whose FP32 run stagnated is solved again
+    with fallback_fn (default: solve_wave in FP64)."""
 
     def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
                  max_wave_requests: int = 512, solve_fn=None, make_stream=None, wave_order: str = "size",
                  size_ratio: float = 4.0, aging_s: float = 30.0,
-                 batch_window_s: float = 0.05):
+                 batch_window_s: float = 0.05, refill: bool = False, run_fn=None, fallback_fn=None,
+                 refill_fraction: float = 0.25, advance_iterations: int = 32, run_max_s: float = 10.0):
         if wave_order not in ("size", "fifo"):
             raise ValueError(f"wave_order must be 'size' or 'fifo', not {wave_order!r}")
+        self.refill = bool(refill)
+        self.run_fn = run_fn or WaveRun
+        if fallback_fn is None:
+            def fallback_fn(fv_, cache_, reqs_, stream_):
+                return solve_wave(fv_, cache_, reqs_, stream_, precision="fp64")
+        self.fallback_fn = fallback_fn
+        self.refill_fraction = float(refill_fraction)
+        self.advance_iterations = int(advance_iterations)
+        self.run_max_s = float(run_max_s)
+        self.refills = 0
         self.wave_order = wave_order
         self.size_ratio = float(size_ratio)
         self.aging_s = float(aging_s)
@@ -266,6 +384,33 @@ class Server:
         self.admitted = collections.deque(r for r in q if id(r) not in taken)
         return wave
 
+    def _take_first(self, worker: int) -> list[Request]:
+        """Refill mode: the first requests of a new wave -- the worker's
+        preferred kind if any is admitted, else the other -- in arrival order
+        (caller holds the lock)."""
+        kinds = {r.kind for r in self.admitted}
+        pref = ("3d", "2d")[worker % 2]
+        kind = pref if pref in kinds else next(iter(sorted(kinds)))
+        return self._take_kind(kind, self.max_wave_cells, self.max_wave_requests)
+
+    def _take_kind(self, kind: str, room_cells: int, room_requests: int) -> list[Request]:
+        """Admitted requests of `kind` in arrival order while they fit (caller holds the lock)."""
+        out, cells = [], 0
+        for r in self.admitted:
+            if len(out) == room_requests:
+                break
+            if r.kind != kind:
+                continue
+            if out and cells + r.cells > room_cells:
+                continue
+            if not out and r.cells > room_cells and room_cells < self.max_wave_cells:
+                continue  # a refill takes only what fits; a new wave takes its first request whatever its size
+            out.append(r)
+            cells += r.cells
+        taken = {id(r) for r in out}
+        self.admitted = collections.deque(r for r in self.admitted if id(r) not in taken)
+        return out
+
     def run(self, requests: list[Request], time_limit: float = 120.0, warm: bool = True, drain: bool = True) -> dict:
         """Serve `requests` (arrival times relative to now).  Returns latency and
         throughput statistics over the completed requests.  At time_limit
@@ -274,7 +419,14 @@ class Server:
         requests left (admitted or still to arrive) are the backlog."""
         if warm:  # one small wave of each kind brings the driver and the caches up
             for kind, side in (("2d", 8), ("3d", 3)):
-                self.solve_fn(self.fv, self.cache, [Request(-1, 0.0, kind, side, 1, cells=1)], self.make_stream())
+                w = [Request(-1, 0.0, kind, side, 1, cells=1)]
+                if self.refill:
+                    wr = self.run_fn(self.fv, self.cache, w, self.make_stream(), prev=None)
+                    while wr.running():
+                        wr.advance(self.advance_iterations)
+                    wr.close()
+                else:
+                    self.solve_fn(self.fv, self.cache, w, self.make_stream())
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter()
         stop = threading.Event()
@@ -337,8 +489,102 @@ class Server:
                     self.done.extend(wave)
                     self.lock.notify_all()
 
+        def finish(reqs):
+            fin = time.perf_counter() - t0
+            with self.lock:
+                for r in reqs:
+                    r.finish = fin
+                    self.reserved -= self._cost(r)
+                    if r.error is not None:
+                        self.failed += 1
+                self.done.extend(reqs)
+                self.lock.notify_all()
+
+        def worker_refill(index):
+            stream = self.make_stream()
+            run = None
+            built_cells = built_count = freed_cells = freed_count = 0
+            run_t0 = 0.0
+            while True:
+                new = []
+                with self.lock:
+                    if run is None:
+                        while not stop.is_set():
+                            if self.admitted:
+                                wait = self.admitted[0].arrival + self.batch_window_s - (time.perf_counter() - t0)
+                                full = sum(r.cells for r in self.admitted) >= self.max_wave_cells
+                                if wait <= 0 or full or not pending:
+                                    break
+                                self.lock.wait(min(wait, 0.01))
+                            else:
+                                self.lock.wait(0.01)
+                        if stop.is_set() and (not drain or not self.admitted):
+                            return
+                        new = self._take_first(index)
+                        run_t0 = time.perf_counter()
+                    elif (self.admitted and not stop.is_set() and time.perf_counter() - run_t0 < self.run_max_s
+                          and (freed_cells >= self.refill_fraction * built_cells
+                               or freed_count >= self.refill_fraction * built_count)):
+                        new = self._take_kind(run.kind, self.max_wave_cells - run.cells,
+                                              self.max_wave_requests - len(run.running()))
+                        if new:
+                            self.refills += 1
+                    if new:
+                        wid = self.waves
+                        self.waves += 1
+                if new:
+                    start = time.perf_counter() - t0
+                    for r in new:
+                        r.start = start
+                        r.wave = wid
+                    try:
+                        nxt = self.run_fn(self.fv, self.cache, (run.running() if run is not None else []) + new,
+                                          stream, prev=run)
+                    except Exception as e:  # the new requests fail; a running wave carries on
+                        for r in new:
+                            r.error = f"{type(e).__name__}: {e}"
+                            r.residual = float("nan")
+                        finish(new)
+                        if run is None:
+                            continue
+                    else:
+                        if run is not None:
+                            run.close()
+                        run = nxt
+                        built_cells, built_count = run.cells, len(run.running())
+                        freed_cells = freed_count = 0
+                try:
+                    finished, stalled = run.advance(self.advance_iterations)
+                except Exception as e:  # a failed wave fails its running requests, not the server
+                    lost = run.running()
+                    for r in lost:
+                        r.error = f"{type(e).__name__}: {e}"
+                        r.residual = float("nan")
+                    finish(lost)
+                    try:
+                        run.close()
+                    finally:
+                        run = None
+                    continue
+                for r in stalled:  # the FP32 run stagnated: FP64 from x0 = 0
+                    try:
+                        r.error = None
+                        self.fallback_fn(self.fv, self.cache, [r], stream)
+                    except Exception as e:
+                        r.error = f"{type(e).__name__}: {e}"
+                        r.residual = float("nan")
+                out = finished + stalled
+                if out:
+                    freed_cells += sum(r.cells for r in out)
+                    freed_count += len(out)
+                    finish(out)
+                if not run.running():
+                    run.close()
+                    run = None
+
         adm = threading.Thread(target=admit_loop, daemon=True)
-        ws = [threading.Thread(target=worker, args=(k,), daemon=True) for k in range(self.workers)]
+        ws = [threading.Thread(target=worker_refill if self.refill else worker, args=(k,), daemon=True)
+              for k in range(self.workers)]
         adm.start()
         for w in ws:
             w.start()
@@ -359,6 +605,7 @@ class Server:
         span = (max(r.finish for r in fin) - min(r.arrival for r in fin)) if fin else 0.0
         return {
             "completed": len(fin), "offered": len(requests), "failed": self.failed, "waves": self.waves,
+            "refills": self.refills,
             "backlog": len(requests) - len(fin) - self.failed,
             "arrived_by_cap": sum(1 for r in requests if r.arrival <= time_limit),
             "wall_s": wall, "peak_reserved_bytes": self.peak_reserved, "budget_bytes": self.budget,

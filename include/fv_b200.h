@@ -450,6 +450,42 @@ fv_status fv_batch_bicgstab(fv_batch *B, fv_precond *P, const double *b, double 
                             fv_batch_info *info, void *stream);
 fv_status fv_batch_destroy(fv_batch *B);
 
+/* Stepwise runs (continuous batching): the iterations of fv_batch_cg /
+ * fv_batch_bicgstab, split at iteration boundaries so a caller can take the
+ * finished problems out and carry the running ones into another batch (built
+ * over the running problems plus newly admitted ones) without changing any
+ * bit of their iterations.
+ *
+ * fv_batch_begin starts a run of `method` (FV_BATCH_CG / FV_BATCH_BICGSTAB).
+ * Problem p starts from x0 = 0 unless from_problem (optional, np entries) maps
+ * it to a running problem from_problem[p] >= 0 of the batch `from`: that
+ * problem's state (the rows of x and of the Krylov vectors, its iteration
+ * count and scalars) is copied and it continues where it stopped.  Its matrix,
+ * right-hand side and preconditioner rows must be the same bits in both
+ * batches (the same request assembled again), and both runs must use the same
+ * method, precision, mixed-precision settings and tile_rows; otherwise, or
+ * when a mapped problem is not running or has another size, FV_ERR_INVALID.
+ * `from` (and its b, x) must stay alive until fv_batch_begin returns; it does
+ * not change.  b, x and P must stay alive for the whole run.
+ *
+ * fv_batch_advance runs up to max_iterations more iterations (whole groups of
+ * 8 CG / 4 BiCGStab iterations; fewer when every problem finished), applies
+ * the pending result of every problem that finished (x final in its rows) and
+ * returns the number of running problems and per problem done[p] (optional).
+ * fv_batch_report fills the per-problem fields of info for the state after the
+ * last begin / advance (device_ms = 0).  A stepwise mixed run does not run the
+ * FP64 pass: fp64_fallback[p] = 1 marks a problem whose FP32 run stagnated
+ * (done, unconverged); its caller solves it again in FP64.
+ * A problem gives the same bits through any sequence of stepwise batches as
+ * alone in fv_batch_cg / fv_batch_bicgstab (mixed: when it does not stagnate). */
+#define FV_BATCH_CG 0
+#define FV_BATCH_BICGSTAB 1
+fv_status fv_batch_begin(fv_batch *B, fv_precond *P, int32_t method, const double *b, double *x,
+                         const fv_batch_options *opt, const fv_batch *from, const int32_t *from_problem,
+                         void *stream);
+fv_status fv_batch_advance(fv_batch *B, int64_t max_iterations, int32_t *n_running, int32_t *done, void *stream);
+fv_status fv_batch_report(const fv_batch *B, fv_batch_info *info);
+
 /* ------------------------------------------------------------------------ */
 /* Reordered factorisations (the perf mode of the triangular sweeps).
  *

@@ -183,3 +183,83 @@ def test_capped_run_stops_at_the_cap_and_reports_the_backlog():
     assert st["arrived_by_cap"] < len(reqs)
     # the last waves started before the cap; no wave is longer than a few seconds here
     assert wall < 1.0 + 10.0
+
+
+class _FakeRun:
+    """A stepwise wave: request r needs r.seed % 5 + 1 advances in total; a
+    carried request keeps what it has done (a restart would show as extra
+    advances); rid 7 stagnates, a wave holding rid 13 fails to build."""
+    builds = []
+
+    def __init__(self, fv, cache, reqs, stream, prev=None):
+        if any(r.rid == 13 for r in reqs):
+            raise RuntimeError("injected build failure")
+        assert len({r.kind for r in reqs}) == 1
+        self.kind = reqs[0].kind
+        self.reqs = list(reqs)
+        self.steps = {r.rid: (prev.steps[r.rid] if prev is not None and r.rid in prev.steps else 0) for r in reqs}
+        carried = [r.rid for r in reqs if prev is not None and r.rid in prev.steps]
+        if prev is not None:
+            assert all(not prev.finished.get(rid, False) for rid in carried)
+        self.finished = {}
+        _FakeRun.builds.append(([r.rid for r in reqs], carried))
+
+    @property
+    def cells(self):
+        return sum(r.cells for r in self.running())
+
+    def running(self):
+        return [r for r in self.reqs if not self.finished.get(r.rid)]
+
+    def advance(self, iterations):
+        time.sleep(0.002)
+        fin, stalled = [], []
+        for r in self.running():
+            self.steps[r.rid] += 1
+            if self.steps[r.rid] == r.seed % 5 + 1:
+                self.finished[r.rid] = True
+                r.iterations = self.steps[r.rid]
+                r.residual = 1e-11
+                (stalled if r.rid == 7 else fin).append(r)
+        return fin, stalled
+
+    def close(self):
+        pass
+
+
+def test_refill_carries_running_requests_and_refills_freed_slots(fv):
+    """Refill mode: finished requests leave at once, waiting requests of the
+    same kind join the running wave, carried requests never restart, every
+    wave has one kind and at most max_wave_requests requests, a failed build
+    fails only the newly admitted requests, a stagnated request is solved by
+    the fallback."""
+    from fvb200.serve import Request, Server
+    _FakeRun.builds = []
+    reqs = [Request(k, 0.001 * k, "2d" if k % 3 else "3d", 10, k, cells=1000 + 10 * k) for k in range(80)]
+    fell_back = []
+
+    def fallback(fv_, cache_, wave, stream):
+        fell_back.extend(r.rid for r in wave)
+        for r in wave:
+            r.residual = 1e-12
+
+    srv = Server(None, workers=2, budget_bytes=10 ** 12, refill=True, run_fn=_FakeRun, fallback_fn=fallback,
+                 make_stream=_Stream, max_wave_requests=6, max_wave_cells=10 ** 9, refill_fraction=0.2,
+                 batch_window_s=0.0)
+    st = srv.run(reqs, time_limit=60.0, warm=False)
+    assert st["refills"] > 0
+    assert st["completed"] + st["failed"] == len(reqs)
+    failed = {r.rid for r in reqs if r.error}
+    assert 13 in failed and len(failed) <= 6       # only the build that held 13 failed (its new requests)
+    assert fell_back == [7]
+    for r in reqs:
+        if r.error is None:
+            assert r.iterations == r.seed % 5 + 1, r.rid   # carried over, never restarted
+            assert r.finish >= r.start >= r.arrival
+    seen_carried = False
+    for rids, carried in _FakeRun.builds:
+        assert len(rids) <= 6
+        kinds = {reqs[i].kind for i in rids}
+        assert len(kinds) == 1
+        seen_carried |= bool(carried)
+    assert seen_carried
