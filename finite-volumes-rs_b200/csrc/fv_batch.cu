@@ -352,10 +352,10 @@ __global__ void __launch_bounds__(TB) kbb_spmv1(Tiles tl, const int32_t *__restr
     }
 }
 
-// h = d + y alpha; s = r - v alpha; |s| test
+// s = r - v alpha; |s| test.  h = d + y alpha is not stored: it is recomputed,
+// with the same rounding, where it is used (kbb_update, kbb_finish).
 template <typename T>
-__global__ void __launch_bounds__(TB) kbb_s(Tiles tl, const T *__restrict__ d, const T *__restrict__ y,
-                                            const T *__restrict__ r, const T *__restrict__ vv, T *__restrict__ h,
+__global__ void __launch_bounds__(TB) kbb_s(Tiles tl, const T *__restrict__ r, const T *__restrict__ vv,
                                             T *__restrict__ sv, double *partial, BProb *S, BGlobal *G, MixedCfg mx) {
     for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int p = tl.prob[t];
@@ -363,7 +363,6 @@ __global__ void __launch_bounds__(TB) kbb_s(Tiles tl, const T *__restrict__ d, c
         const T alpha = (T)S[p].alpha;
         T acc = T(0);
         for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) {
-            h[i] = d[i] + y[i] * alpha;
             const T si = r[i] - vv[i] * alpha;
             sv[i] = si;
             acc += si * si;
@@ -405,20 +404,21 @@ __global__ void __launch_bounds__(TB) kbb_spmv2(Tiles tl, const int32_t *__restr
     }
 }
 
-// d = h + z omega; r = s - t omega; |r| test; beta and the restart (:122-171)
+// d = h + z omega with h = d + y alpha; r = s - t omega; |r| test; beta and the restart (:122-171)
 template <typename T>
 __global__ void __launch_bounds__(TB) kbb_update(Tiles tl, T *__restrict__ d, T *__restrict__ r,
-                                                 const T *__restrict__ h, const T *__restrict__ z,
+                                                 const T *__restrict__ y, const T *__restrict__ z,
                                                  const T *__restrict__ sv, const T *__restrict__ tv,
                                                  const T *__restrict__ rh, double *partial, BProb *S, BGlobal *G,
                                                  MixedCfg mx) {
     for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int p = tl.prob[t];
         if (S[p].done) continue;
-        const T omega = (T)S[p].omega;
+        const T alpha = (T)S[p].alpha, omega = (T)S[p].omega;
         T a0 = T(0), a1 = T(0);
         for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) {
-            d[i] = h[i] + z[i] * omega;
+            const T hi = d[i] + y[i] * alpha;
+            d[i] = hi + z[i] * omega;
             const T ri = sv[i] - tv[i] * omega;
             r[i] = ri;
             a0 += ri * ri;
@@ -478,13 +478,14 @@ __global__ void __launch_bounds__(TB) kbb_p(Tiles tl, const T *__restrict__ r, c
     }
 }
 
-// d = h for problems whose |s| test ended the solve
+// d = h = d + y alpha for problems whose |s| test ended the solve
 template <typename T>
-__global__ void kbb_finish(Tiles tl, T *__restrict__ d, const T *__restrict__ h, BProb *S) {
+__global__ void kbb_finish(Tiles tl, T *__restrict__ d, const T *__restrict__ y, BProb *S) {
     for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int p = tl.prob[t];
         if (S[p].finish_h != 1) continue;
-        for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) d[i] = h[i];
+        const T alpha = (T)S[p].alpha;
+        for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) d[i] = d[i] + y[i] * alpha;
     }
 }
 
@@ -612,19 +613,20 @@ __global__ void kbm_flush(Tiles tl, double *__restrict__ x, T *__restrict__ d) {
 }
 
 // ---- stepwise runs
-// The result of every problem that retired since the last call: d = h where
-// BiCGStab's |s| test ended the solve (h non-null), x64 += d (mixed, x64
-// non-null).  Per problem these are the operations kbb_finish and kbm_flush
-// apply at the end of a whole-batch solve.
+// The result of every problem that retired since the last call: d = h = d +
+// y alpha where BiCGStab's |s| test ended the solve (y non-null), x64 += d
+// (mixed, x64 non-null).  Per problem these are the operations kbb_finish and
+// kbm_flush apply at the end of a whole-batch solve.
 template <typename T>
-__global__ void kb_finalize(Tiles tl, T *__restrict__ d, const T *__restrict__ h, double *__restrict__ x64,
+__global__ void kb_finalize(Tiles tl, T *__restrict__ d, const T *__restrict__ y, double *__restrict__ x64,
                             const BProb *S) {
     for (int64_t t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int p = tl.prob[t];
         if (!S[p].done || S[p].fin) continue;
-        const bool take_h = h && S[p].finish_h == 1;
+        const bool take_h = y && S[p].finish_h == 1;
+        const T alpha = (T)S[p].alpha;
         for (int64_t i = tl.row0[t] + threadIdx.x; i < tl.row1[t]; i += blockDim.x) {
-            if (take_h) d[i] = h[i];
+            if (take_h) d[i] = d[i] + y[i] * alpha;
             if (x64) {
                 x64[i] += (double)d[i];
                 d[i] = T(0);
@@ -785,7 +787,7 @@ namespace {
 template <typename T>
 struct InnerVecs {
     T *r, *z, *p, *ap, *d;       // CG: residual, M^-1 r, direction, A p, solution
-    T *rh, *y, *v, *s, *t, *h;   // BiCGStab (p, r, z, d shared)
+    T *rh, *y, *v, *s, *t;       // BiCGStab (p, r, z, d shared)
 };
 
 fv_row_skip row_skip(fv_batch *B);
@@ -858,12 +860,11 @@ fv_status inner_group(bool bicg, fv_batch *B, fv_precond *P, const T *vals, Inne
             FV_TRY(precond<T>(B, P, v.p, v.y, st, skip));
             fv_note_launch(), kbb_spmv1<T><<<G, TB, 0, st>>>(tl, A->row_ptr, A->cols, vals, v.y, v.v, v.rh,
                                                             B->partial, B->S, B->G);
-            fv_note_launch(), kbb_s<T><<<G, TB, 0, st>>>(tl, v.d, v.y, v.r, v.v, v.h, v.s, B->partial, B->S, B->G,
-                                                        mx.cfg);
+            fv_note_launch(), kbb_s<T><<<G, TB, 0, st>>>(tl, v.r, v.v, v.s, B->partial, B->S, B->G, mx.cfg);
             FV_TRY(precond<T>(B, P, v.s, v.z, st, skip));
             fv_note_launch(), kbb_spmv2<T><<<G, TB, 0, st>>>(tl, A->row_ptr, A->cols, vals, v.z, v.t, v.s,
                                                             B->partial, B->S, B->G);
-            fv_note_launch(), kbb_update<T><<<G, TB, 0, st>>>(tl, v.d, v.r, v.h, v.z, v.s, v.t, v.rh, B->partial,
+            fv_note_launch(), kbb_update<T><<<G, TB, 0, st>>>(tl, v.d, v.r, v.y, v.z, v.s, v.t, v.rh, B->partial,
                                                              B->S, B->G, mx.cfg);
             if (mx.cfg.on) {
                 fv_note_launch(), kbm_rep1<T><<<G, TB, 0, st>>>(tl, mx.x64, v.d, B->S);
@@ -889,7 +890,7 @@ fv_status inner_solve(bool bicg, fv_batch *B, fv_precond *P, const T *vals, Inne
         FV_TRY(inner_group<T>(bicg, B, P, vals, v, G, tl, st, launched_iters, mx));
         FV_TRY(wait_all_done(B, st, done));
     }
-    if (bicg) fv_note_launch(), kbb_finish<T><<<G, TB, 0, st>>>(tl, v.d, v.h, B->S);
+    if (bicg) fv_note_launch(), kbb_finish<T><<<G, TB, 0, st>>>(tl, v.d, v.y, B->S);
     if (mx.cfg.on) fv_note_launch(), kbm_flush<T><<<G, TB, 0, st>>>(tl, mx.x64, v.d);
     FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
@@ -922,12 +923,17 @@ InnerVecs<T> carve(void *mem, int64_t n, T *d) {
     v.v = a + 6 * n;
     v.s = a + 7 * n;
     v.t = a + 8 * n;
-    v.h = a + 9 * n;
-    v.d = d ? d : a + 10 * n;
+    v.d = d ? d : a + 9 * n;
     return v;
 }
 
-int grid_of(const fv_batch *B) { return (int)std::min<int64_t>(B->ntiles, 148 * 8); }
+// Blocks of the tile kernels: at most 8 per SM, and the tiles spread evenly
+// over them (a block takes every G-th tile), so the last round is not a tail.
+int grid_of(const fv_batch *B) {
+    const int64_t cap = 148 * 8;
+    const int64_t rounds = (B->ntiles + cap - 1) / cap;
+    return (int)std::max<int64_t>(1, (B->ntiles + rounds - 1) / rounds);
+}
 
 Tiles tiles_of(const fv_batch *B) { return Tiles{B->ntiles, B->tile_prob, B->tile_row0, B->tile_row1, B->ptile}; }
 
@@ -997,7 +1003,7 @@ fv_status run_begin(fv_batch *B, fv_precond *P, bool bicg, const double *b, doub
     }
     const int nfresh = np - (int)list.size();
     B->run = false;
-    FV_TRY(ensure_bytes(B->vec, B->vec_bytes, mixed ? sizeof(float) * 11 * (size_t)n : sizeof(double) * 10 * (size_t)n));
+    FV_TRY(ensure_bytes(B->vec, B->vec_bytes, mixed ? sizeof(float) * 10 * (size_t)n : sizeof(double) * 9 * (size_t)n));
     FV_CUDA_TRY(cudaMemcpyAsync(B->S, hs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
     BGlobal g0{nfresh, nfresh == 0 ? 1 : 0, {0, 0}};
     FV_CUDA_TRY(cudaMemcpyAsync(B->G, &g0, sizeof(BGlobal), cudaMemcpyHostToDevice, st));
@@ -1083,7 +1089,7 @@ fv_status run_advance(fv_batch *B, int64_t max_iterations, cudaStream_t st) {
             FV_TRY(inner_group<double>(B->bicg, B, B->P, B->A->vals, v, G, tl, st, B->launched, none));
             FV_TRY(wait_all_done(B, st, done));
         }
-        fv_note_launch(), kb_finalize<double><<<G, TB, 0, st>>>(tl, v.d, B->bicg ? v.h : nullptr, nullptr, B->S);
+        fv_note_launch(), kb_finalize<double><<<G, TB, 0, st>>>(tl, v.d, B->bicg ? v.y : nullptr, nullptr, B->S);
     }
     fv_note_launch(), kb_mark_fin<<<(B->np + 255) / 256, 256, 0, st>>>(B->np, B->S);
     FV_CUDA_TRY(cudaGetLastError());
@@ -1147,7 +1153,7 @@ fv_status batch_solve(bool bicg, fv_batch *B, fv_precond *P, const double *b, do
             FV_CUDA_TRY(cudaMemcpyAsync(B->S, fs.data(), sizeof(BProb) * np, cudaMemcpyHostToDevice, st));
             BGlobal g1{nfail, 0, {0, 0}};
             FV_CUDA_TRY(cudaMemcpyAsync(B->G, &g1, sizeof(BGlobal), cudaMemcpyHostToDevice, st));
-            FV_TRY(ensure_bytes(B->vec64, B->vec64_bytes, sizeof(double) * 10 * (size_t)n));
+            FV_TRY(ensure_bytes(B->vec64, B->vec64_bytes, sizeof(double) * 9 * (size_t)n));
             InnerVecs<double> w = carve<double>(B->vec64, n, x);
             FV_CUDA_TRY(cudaMemcpyAsync(w.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
             const MixedArgs none{MixedCfg{0, 0.0, 0.0}, nullptr, nullptr};
