@@ -15,6 +15,7 @@
 // (identical arithmetic, identical bits); the second read of its data hits L2
 // because face ids follow element order.
 #include <algorithm>
+#include <cstdlib>
 #include <cub/device/device_scan.cuh>
 #include <vector>
 
@@ -427,38 +428,29 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
 // output value receives the same additions in the same order as in k_assemble.
 constexpr int kAsmBlock = 128;
 
-template <int DIM, int MAXF, bool CORR>
-__global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
-    extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
-    const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
-    const int64_t i = b0 + threadIdx.x;
-    const int64_t bend = min(b0 + (int64_t)kAsmBlock, a.n);
-    const int base = a.row_ptr[b0];
-    const int top = a.row_ptr[bend];
-    const bool live = i < a.n;
-    // the cell's incidences, padded to MAXF slots: no dependent load of cf_ptr
-    int fe[MAXF], jj[MAXF];
-#pragma unroll
-    for (int k = 0; k < MAXF; k += 2) {
-        int4 q = make_int4(0, -2, 0, -2);
-        if (live) q = *reinterpret_cast<const int4 *>(&a.cf_pad[i * MAXF + k]);
-        fe[k] = q.x;
-        jj[k] = q.y;
-        fe[k + 1] = q.z;
-        jj[k + 1] = q.w;
-    }
+// The cell's incidences, padded to MAXF slots (jj = -2 marks a pad): the
+// degree, and pads turned into jj = -1.
+template <int MAXF>
+__device__ __forceinline__ int unpad(int (&jj)[MAXF]) {
     int deg = 0;
 #pragma unroll
     for (int k = 0; k < MAXF; ++k) deg += jj[k] != -2 ? 1 : 0;
 #pragma unroll
     for (int k = 0; k < MAXF; ++k)
         if (jj[k] == -2) jj[k] = -1;
-    double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
-    double srci = 0.0;
-    if (live) {
-        ci4 = a.cell[i];
-        if (a.c_src != 0.0) srci = a.src[i];
-    }
+    return deg;
+}
+
+// The values of row i (one cell): every gather of the cell is issued before
+// any of them is used, the slot of each neighbour in the sorted row is a count
+// of smaller distinct neighbours instead of a sort, and the row is written to
+// the block's staging area (stage[row_ptr[i] - base ...]) so the stores of the
+// values are coalesced.  fe / jj: the cell's incidences (face id with the
+// neighbour-side bit, the other cell or -1), deg of them.
+template <int DIM, int MAXF, bool CORR>
+__device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, bool live, const int (&fe)[MAXF],
+                                           const int (&jj)[MAXF], int deg, const double4 &ci4, double srci,
+                                           double *stage, int base) {
     double3 oc[MAXF];
     double ar[MAXF], kp[MAXF], fl[MAXF];
 #pragma unroll
@@ -607,9 +599,127 @@ __global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(A
         a.rhs[i] = rhs;
     }
     (void)ndist;
+}
+
+// One row per thread, each output value receiving the same additions in the
+// same order as in k_assemble (MAXF is small: 4 for triangles and
+// tetrahedra, 8 up to hexahedra).
+template <int DIM, int MAXF, bool CORR>
+__global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
+    extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
+    const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
+    const int64_t i = b0 + threadIdx.x;
+    const int64_t bend = min(b0 + (int64_t)kAsmBlock, a.n);
+    const int base = a.row_ptr[b0];
+    const int top = a.row_ptr[bend];
+    const bool live = i < a.n;
+    // the cell's incidences, padded to MAXF slots: no dependent load of cf_ptr
+    int fe[MAXF], jj[MAXF];
+#pragma unroll
+    for (int k = 0; k < MAXF; k += 2) {
+        int4 q = make_int4(0, -2, 0, -2);
+        if (live) q = *reinterpret_cast<const int4 *>(&a.cf_pad[i * MAXF + k]);
+        fe[k] = q.x;
+        jj[k] = q.y;
+        fe[k + 1] = q.z;
+        jj[k + 1] = q.w;
+    }
+    const int deg = unpad<MAXF>(jj);
+    double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    double srci = 0.0;
+    if (live) {
+        ci4 = a.cell[i];
+        if (a.c_src != 0.0) srci = a.src[i];
+    }
+    row_values<DIM, MAXF, CORR>(a, i, live, fe, jj, deg, ci4, srci, stage, base);
     __syncthreads();
     double *out = a.vals + base;
     for (int q = threadIdx.x; q < top - base; q += kAsmBlock) out[q] = stage[q];
+}
+
+__device__ __forceinline__ void asm_cp16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void asm_cp8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void asm_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void asm_cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Per-thread prefetch slot of one cell: incidences, centre and volume, source.
+template <int MAXF>
+struct AsmSlot {
+    int2 cf[MAXF];
+    double4 cell;
+    double src;
+    double pad;
+};
+
+// The same rows, a block walking tiles of kAsmBlock cells: while a tile's
+// rows are computed, the next tile's incidences, cell centres and sources are
+// already on their way into shared memory (cp.async, one slot per thread,
+// read back only by the thread that copied it), so the first of the two
+// dependent memory round trips of a row is off the critical path.
+template <int DIM, int MAXF, int MINB>
+__global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs a, int64_t ntiles) {
+    extern __shared__ __align__(32) double smem[];
+    double *stage = smem;  // kAsmBlock * (MAXF + 1) values
+    AsmSlot<MAXF> *slot = reinterpret_cast<AsmSlot<MAXF> *>(smem + kAsmBlock * (MAXF + 1));  // [2][kAsmBlock]
+    const bool use_src = a.c_src != 0.0;
+    auto prefetch = [&](int64_t tile, int buf) {
+        const int64_t c = tile * kAsmBlock + threadIdx.x;
+        if (tile < ntiles && c < a.n) {
+            AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
+#pragma unroll
+            for (int k = 0; k < MAXF; k += 2) asm_cp16(&q.cf[k], &a.cf_pad[c * MAXF + k]);
+            asm_cp16(&q.cell, &a.cell[c]);
+            asm_cp16(reinterpret_cast<double *>(&q.cell) + 2, reinterpret_cast<const double *>(&a.cell[c]) + 2);
+            if (use_src) asm_cp8(&q.src, &a.src[c]);
+        }
+        asm_cp_commit();
+    };
+    int buf = 0;
+    prefetch(blockIdx.x, 0);
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        prefetch(tile + gridDim.x, buf ^ 1);
+        asm_cp_wait1();  // this thread's copies of `tile` have landed
+        const int64_t b0 = tile * kAsmBlock;
+        const int64_t i = b0 + threadIdx.x;
+        const int64_t bend = min(b0 + (int64_t)kAsmBlock, a.n);
+        const int base = a.row_ptr[b0];
+        const int top = a.row_ptr[bend];
+        const bool live = i < a.n;
+        int fe[MAXF], jj[MAXF];
+        double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
+        double srci = 0.0;
+        const AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
+#pragma unroll
+        for (int k = 0; k < MAXF; ++k) {
+            fe[k] = live ? q.cf[k].x : 0;
+            jj[k] = live ? q.cf[k].y : -2;
+        }
+        if (live) {
+            ci4 = q.cell;
+            if (use_src) srci = q.src;
+        }
+        const int deg = unpad<MAXF>(jj);
+        row_values<DIM, MAXF, false>(a, i, live, fe, jj, deg, ci4, srci, stage, base);
+        __syncthreads();
+        double *out = a.vals + base;
+        for (int r = threadIdx.x; r < top - base; r += kAsmBlock) out[r] = stage[r];
+        __syncthreads();  // the stage is rewritten by the next tile
+        buf ^= 1;
+    }
+}
+
+static int asm_pipe_choice() {
+    static int v = [] {
+        const char *e = getenv("FV_ASM_PIPE");
+        return e ? atoi(e) : 0;
+    }();
+    return v;
 }
 
 template <int DIM, int MAXF>
@@ -618,12 +728,29 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
-        if (a.grad)
+        if (a.grad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
-        else if (a.cf_pad)
+        } else if (a.cf_pad && asm_pipe_choice()) {
+            const size_t smem_p = smem + 2 * B * sizeof(AsmSlot<MAXF>);
+            constexpr int MB = MAXF <= 4 ? 6 : 3;
+            const bool wide = asm_pipe_choice() == 2;  // fewer blocks, no register cap below the need
+            auto kern = wide ? k_assemble_pipe<DIM, MAXF, MB == 6 ? 4 : 2> : k_assemble_pipe<DIM, MAXF, MB>;
+            static int per_sm[2] = {0, 0};
+            if (!per_sm[wide]) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[wide], kern, B, smem_p);
+                if (per_sm[wide] < 1) per_sm[wide] = 1;
+            }
+            int sms = 148;
+            int dev = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const int64_t ntiles = G;
+            const unsigned Gp = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm[wide]);
+            fv_note_launch(), kern<<<Gp, B, smem_p, st>>>(a, ntiles);
+        } else if (a.cf_pad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, false><<<G, B, smem, st>>>(a);
-        else
+        } else {
             fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
+        }
     } else {
         fv_note_launch(), k_assemble<DIM, MAXF><<<G, B, 0, st>>>(a);
     }

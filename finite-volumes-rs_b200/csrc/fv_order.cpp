@@ -240,6 +240,19 @@ extern "C" fv_status fv_order_boxes_host(int64_t n, int32_t dim, const double *c
     }
 }
 
+extern "C" fv_status fv_order_boxes_host_levels(int64_t n, int32_t dim, const double *cell_center,
+                                                int64_t center_stride, const double *lo, const double *hi,
+                                                const int32_t *row_ptr, const int32_t *cols, int32_t rows_per_box,
+                                                int32_t *perm, int32_t *level, fv_order_info *info) {
+    if (!row_ptr || row_ptr[0] != 0 || !level) return FV_ERR_INVALID;
+    try {
+        return order_one(n, dim, cell_center, center_stride, lo, hi, row_ptr, cols, 0, rows_per_box, perm, level,
+                         info);
+    } catch (const std::bad_alloc &) {
+        return FV_ERR_ALLOC;
+    }
+}
+
 // A block-diagonal union of independent problems (rows [off[p], off[p+1]) of
 // problem p, coupled to nothing outside): every problem ordered on its own,
 // with its own domain box (lo/hi per problem, or NULL for the centres'

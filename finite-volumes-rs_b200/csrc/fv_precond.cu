@@ -2392,8 +2392,10 @@ extern "C" fv_status fv_precond_perm(const fv_precond *P, int32_t *perm_host, vo
 // cell centres from the mesh, the domain box of every problem from its
 // boundary faces' centres (a face belongs to its owner's problem).
 static fv_status order_boxes_impl(const fv_csr *A, int32_t n_problems, const int64_t *offsets,
-                                  int32_t rows_per_box, int32_t *perm_host, fv_order_info *info, cudaStream_t st) {
+                                  int32_t rows_per_box, int32_t *perm_host, int32_t *level_host, fv_order_info *info,
+                                  cudaStream_t st) {
     if (!A || !perm_host || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
+    if (level_host && n_problems > 1) return FV_ERR_INVALID;
     const fv_mesh *m = A->mesh;
     if (!m || m->n_cells != A->nrows) {
         fv_internal_set_error_text("fv_order_boxes: the matrix was not assembled on a mesh (use fv_order_boxes_host)");
@@ -2440,6 +2442,9 @@ static fv_status order_boxes_impl(const fv_csr *A, int32_t n_problems, const int
     bool all_seen = true;
     for (int p = 0; p < np; ++p) all_seen = all_seen && seen[p];
     const double *lo_p = all_seen ? lo.data() : nullptr, *hi_p = all_seen ? hi.data() : nullptr;
+    if (np == 1 && level_host)
+        return fv_order_boxes_host_levels(n, dim, &cell[0].x, 4, lo_p, hi_p, ptr.data(), col.data(), rows_per_box,
+                                          perm_host, level_host, info);
     if (np == 1)
         return fv_order_boxes_host(n, dim, &cell[0].x, 4, lo_p, hi_p, ptr.data(), col.data(), rows_per_box,
                                    perm_host, info);
@@ -2449,8 +2454,17 @@ static fv_status order_boxes_impl(const fv_csr *A, int32_t n_problems, const int
 
 extern "C" fv_status fv_order_boxes(const fv_csr *A, int32_t n_problems, const int64_t *offsets,
                                     int32_t rows_per_box, int32_t *perm_host, fv_order_info *info, void *stream) {
-    return fv_host_guard(
-        [&] { return order_boxes_impl(A, n_problems, offsets, rows_per_box, perm_host, info, fv_stream(stream)); });
+    return fv_host_guard([&] {
+        return order_boxes_impl(A, n_problems, offsets, rows_per_box, perm_host, nullptr, info, fv_stream(stream));
+    });
+}
+
+extern "C" fv_status fv_order_boxes_levels(const fv_csr *A, int32_t rows_per_box, int32_t *perm_host,
+                                           int32_t *level_host, fv_order_info *info, void *stream) {
+    if (!level_host) return FV_ERR_INVALID;
+    return fv_host_guard([&] {
+        return order_boxes_impl(A, 1, nullptr, rows_per_box, perm_host, level_host, info, fv_stream(stream));
+    });
 }
 
 // Blocks (of 8 warps) per sweep launch and rows per thread of the reordered

@@ -173,6 +173,8 @@ _SIGS = {
     "fv_order_boxes_batch_host": [C.c_int32, P(i64), C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip,
                                   P(OrderInfo)],
     "fv_order_boxes": [vp, C.c_int32, P(i64), C.c_int32, ip, P(OrderInfo), vp],
+    "fv_order_boxes_levels": [vp, C.c_int32, ip, ip, P(OrderInfo), vp],
+    "fv_order_boxes_host_levels": [i64, C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip, ip, P(OrderInfo)],
     "fv_batch_create": [vp, C.c_int32, P(i64), C.c_int32, vp, P(vp)],
     "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],
     "fv_batch_bicgstab": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],

@@ -408,15 +408,26 @@ def _fill_pattern(kind: int, level: int, row_ptr, cols):
     return fptr, fcol[:nnz.value], amap[:len(col)], fill[:nnz.value]
 
 
-def order_boxes(matrix: "DistributedMatrix", rows_per_box: int = 0, offsets=None, stream=None):
+def order_boxes(matrix: "DistributedMatrix", rows_per_box: int = 0, offsets=None, stream=None, levels=False):
     """Box-colour ordering of a matrix assembled on a mesh (fv_order_boxes):
     (perm, info) with perm[i] = the row of the matrix that becomes row i of
     the reordered one, info = dict(n_boxes, boxes_per_axis, n_colours,
     n_levels).  rows_per_box 0: 32 in 2D, 384 in 3D.  offsets: the row
-    offsets of the independent problems of a batch (each ordered on its own)."""
+    offsets of the independent problems of a batch (each ordered on its own).
+    levels (one problem only): also return level[i] of row i of the
+    reordered matrix (fv_order_boxes_levels), for merge_orders."""
     n = matrix.nrows()
     perm = np.empty(n, np.int32)
     info = OrderInfo()
+    if levels:
+        if offsets is not None and len(offsets) > 2:
+            raise ValueError("levels: one problem only")
+        lev = np.empty(n, np.int32)
+        ip = C.POINTER(C.c_int32)
+        check(lib().fv_order_boxes_levels(matrix.handle, int(rows_per_box), perm.ctypes.data_as(ip),
+                                          lev.ctypes.data_as(ip), C.byref(info), stream_handle(stream)),
+              "order_boxes_levels")
+        return perm, _order_info(info), lev
     np_, offp = 1, None
     if offsets is not None:
         off = np.ascontiguousarray(offsets, np.int64)
@@ -427,9 +438,10 @@ def order_boxes(matrix: "DistributedMatrix", rows_per_box: int = 0, offsets=None
     return perm, _order_info(info)
 
 
-def order_boxes_host(cell_center, row_ptr, cols, rows_per_box: int = 0, lo=None, hi=None):
+def order_boxes_host(cell_center, row_ptr, cols, rows_per_box: int = 0, lo=None, hi=None, levels=False):
     """The same ordering from host arrays (fv_order_boxes_host): cell_center
-    n x dim, a CSR pattern, optional domain box lo / hi."""
+    n x dim, a CSR pattern, optional domain box lo / hi; levels: also the
+    level of every reordered row (fv_order_boxes_host_levels)."""
     cc = np.ascontiguousarray(cell_center, np.float64)
     n, dim = cc.shape
     ptr = np.ascontiguousarray(row_ptr, np.int32)
@@ -440,12 +452,39 @@ def order_boxes_host(cell_center, row_ptr, cols, rows_per_box: int = 0, lo=None,
     ip = C.POINTER(C.c_int32)
     lo_a = np.ascontiguousarray(lo, np.float64) if lo is not None else None
     hi_a = np.ascontiguousarray(hi, np.float64) if hi is not None else None
-    check(lib().fv_order_boxes_host(n, dim, cc.ctypes.data_as(dp), dim,
-                                    lo_a.ctypes.data_as(dp) if lo_a is not None else None,
-                                    hi_a.ctypes.data_as(dp) if hi_a is not None else None,
-                                    ptr.ctypes.data_as(ip), col.ctypes.data_as(ip), int(rows_per_box),
-                                    perm.ctypes.data_as(ip), C.byref(info)), "order_boxes_host")
+    box = (lo_a.ctypes.data_as(dp) if lo_a is not None else None, hi_a.ctypes.data_as(dp) if hi_a is not None else None)
+    if levels:
+        lev = np.empty(n, np.int32)
+        check(lib().fv_order_boxes_host_levels(n, dim, cc.ctypes.data_as(dp), dim, *box, ptr.ctypes.data_as(ip),
+                                               col.ctypes.data_as(ip), int(rows_per_box), perm.ctypes.data_as(ip),
+                                               lev.ctypes.data_as(ip), C.byref(info)), "order_boxes_host_levels")
+        return perm, _order_info(info), lev
+    check(lib().fv_order_boxes_host(n, dim, cc.ctypes.data_as(dp), dim, *box, ptr.ctypes.data_as(ip),
+                                    col.ctypes.data_as(ip), int(rows_per_box), perm.ctypes.data_as(ip),
+                                    C.byref(info)), "order_boxes_host")
     return perm, _order_info(info)
+
+
+def merge_orders(parts, offsets):
+    """The union order of independent problems from each problem's own order:
+    parts[k] = (perm_k, level_k) as order_boxes(..., levels=True) gives them
+    for problem k alone, offsets = the problems' first rows in the union.
+    For each level, every problem's rows of that level in problem order --
+    the order fv_order_boxes gives the union (rows sorted stably by level,
+    then problem, then position)."""
+    ptrs = []
+    nlev = 0
+    for perm_k, lev_k in parts:
+        top = int(lev_k[-1]) + 1 if len(lev_k) else 0
+        ptrs.append(np.searchsorted(lev_k, np.arange(top + 1), side="left"))
+        nlev = max(nlev, top)
+    segs = []
+    for lv in range(nlev):
+        for k, (perm_k, _) in enumerate(parts):
+            lp = ptrs[k]
+            if lv + 1 < len(lp) and lp[lv + 1] > lp[lv]:
+                segs.append(perm_k[lp[lv]:lp[lv + 1]] + np.int32(offsets[k]))
+    return np.concatenate(segs).astype(np.int32) if segs else np.zeros(0, np.int32)
 
 
 def _order_info(info):

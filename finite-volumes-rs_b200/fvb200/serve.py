@@ -23,8 +23,14 @@ packs requests in arrival order.  A wave is formed once its oldest request
 has waited `batch_window_s` (or the admitted requests fill a wave, or no
 more requests are due), so a wave does not start with the first arrival alone.
 
-Meshes are built on the host per (kind, size) and cached; the request's seed
-drives its diffusivity and source fields.
+Slot refill (Server(refill=True), what the bench serves with): a worker's
+wave runs stepwise (fv_batch_begin / fv_batch_advance); a request leaves as
+soon as it has finished, and the wave is rebuilt over its running requests
+-- which carry their Krylov state over, bit for bit -- plus waiting requests
+of its kind (WaveRun), so freed slots are refilled while the others run.
+
+Meshes are built on the device per (kind, size) and cached; the request's
+seed drives its diffusivity and source fields.
 """
 from __future__ import annotations
 
@@ -133,6 +139,23 @@ class MeshCache:
                 ev.set()
 
 
+def mesh_order(fv, m, stream=None):
+    """The box-colour order of mesh m alone and the level of every reordered
+    row (fvb200.order_boxes(..., levels=True) on the mesh's pattern), computed
+    once and kept on the mesh: a wave merges its requests' orders
+    (fvb200.merge_orders) instead of ordering the whole union again."""
+    o = getattr(m, "_box_order", None)
+    if o is None:
+        nb = m.n_boundary_faces
+        A, _ = fv.assemble(-fv.laplacian(fv.Orthogonal(), np.ones(m.n_faces)), (np.zeros(nb), np.zeros(nb)), m,
+                           stream=stream)
+        perm, _, lev = fv.order_boxes(A, levels=True, stream=stream)
+        A.close()
+        o = (perm, lev)
+        m._box_order = o
+    return o
+
+
 def request_fields(m, req: Request):
     if req.kind == "2d":
         kf, _, sc = m.fields(req.seed, 1.0, 1.0, source_const=1.0)
@@ -177,8 +200,12 @@ def wave_system(fv, cache, reqs: list[Request], stream, ordering="boxes", keep_f
         fl = mb.face_field(fls)
         eq = fv.convection(fv.Upwind(fl), fl) - fv.laplacian(fv.Orthogonal(), kf) - fv.source(sc)
     A, b = fv.assemble(eq, bc, mb, stream=stream)
-    P = (fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper).from_matrix(
-        A, 0, stream=stream, ordering=ordering, offsets=mb.cell_offsets if ordering else None)
+    make = fv.IncompleteCholesky if kind == "2d" else fv.IncompleteLowerUpper
+    if ordering == "boxes":  # the union's order from the meshes' own (the order fv_order_boxes gives the union)
+        perm = fv.merge_orders([mesh_order(fv, m, stream) for m in meshes], mb.cell_offsets)
+        P = make.from_matrix(A, 0, stream=stream, ordering=perm)
+    else:
+        P = make.from_matrix(A, 0, stream=stream, ordering=ordering)
     return mb, A, b, P
 
 
@@ -305,14 +332,17 @@ class Server:
     waiting requests, in arrival order, up to max_wave_cells /
     max_wave_requests.  A wave takes refills for `run_max_s` seconds, then
     drains, so that the other kind is served too; worker k prefers kind
-    ("3d", "2d")[k % 2].  A request whose FP32 run stagnated is solved again
+    ("3d", "2d")[k % 2].  A rebuild also waits until the wave has run
+    `rebuild_ratio` times as long as its last build took, which bounds the
+    share of a worker's time spent rebuilding.  A request whose FP32 run stagnated is solved again
     with fallback_fn (default: solve_wave in FP64)."""
 
     def __init__(self, fv, workers: int = 2, budget_bytes: int | None = None, max_wave_cells: int = 48_000_000,
                  max_wave_requests: int = 512, solve_fn=None, make_stream=None, wave_order: str = "size",
                  size_ratio: float = 4.0, aging_s: float = 30.0,
                  batch_window_s: float = 0.05, refill: bool = False, run_fn=None, fallback_fn=None,
-                 refill_fraction: float = 0.25, advance_iterations: int = 32, run_max_s: float = 10.0):
+                 refill_fraction: float = 0.25, advance_iterations: int = 32, run_max_s: float = 10.0,
+                 rebuild_ratio: float = 3.0):
         if wave_order not in ("size", "fifo"):
             raise ValueError(f"wave_order must be 'size' or 'fifo', not {wave_order!r}")
         self.refill = bool(refill)
@@ -324,6 +354,7 @@ class Server:
         self.refill_fraction = float(refill_fraction)
         self.advance_iterations = int(advance_iterations)
         self.run_max_s = float(run_max_s)
+        self.rebuild_ratio = float(rebuild_ratio)
         self.refills = 0
         self.wave_order = wave_order
         self.size_ratio = float(size_ratio)
@@ -504,7 +535,7 @@ class Server:
             stream = self.make_stream()
             run = None
             built_cells = built_count = freed_cells = freed_count = 0
-            run_t0 = 0.0
+            run_t0 = built_at = build_s = 0.0
             while True:
                 new = []
                 with self.lock:
@@ -523,6 +554,7 @@ class Server:
                         new = self._take_first(index)
                         run_t0 = time.perf_counter()
                     elif (self.admitted and not stop.is_set() and time.perf_counter() - run_t0 < self.run_max_s
+                          and time.perf_counter() - built_at >= self.rebuild_ratio * build_s
                           and (freed_cells >= self.refill_fraction * built_cells
                                or freed_count >= self.refill_fraction * built_count)):
                         new = self._take_kind(run.kind, self.max_wave_cells - run.cells,
@@ -538,8 +570,11 @@ class Server:
                         r.start = start
                         r.wave = wid
                     try:
+                        tb = time.perf_counter()
                         nxt = self.run_fn(self.fv, self.cache, (run.running() if run is not None else []) + new,
                                           stream, prev=run)
+                        built_at = time.perf_counter()
+                        build_s = built_at - tb
                     except Exception as e:  # the new requests fail; a running wave carries on
                         for r in new:
                             r.error = f"{type(e).__name__}: {e}"

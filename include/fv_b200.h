@@ -546,6 +546,17 @@ fv_status fv_order_boxes_batch_host(int32_t n_problems, const int64_t *offsets, 
  * mesh).  n_problems <= 1: one problem; else offsets as above. */
 fv_status fv_order_boxes(const fv_csr *A, int32_t n_problems, const int64_t *offsets, int32_t rows_per_box,
                          int32_t *perm, fv_order_info *info, void *stream);
+/* One problem's ordering plus level[i], the level of row i of the reordered
+ * matrix (non-decreasing in i): a caller that keeps each mesh's order can
+ * merge several meshes' orders into the order fv_order_boxes gives their
+ * union -- for each level, every problem's rows of that level in problem
+ * order, offset by the problem's first row. */
+fv_status fv_order_boxes_host_levels(int64_t n, int32_t dim, const double *cell_center, int64_t center_stride,
+                                     const double *lo, const double *hi, const int32_t *row_ptr,
+                                     const int32_t *cols, int32_t rows_per_box, int32_t *perm, int32_t *level,
+                                     fv_order_info *info);
+fv_status fv_order_boxes_levels(const fv_csr *A, int32_t rows_per_box, int32_t *perm, int32_t *level,
+                                fv_order_info *info, void *stream);
 
 /* Allocation-free conjugate gradient.  No counterpart in the reference crate.
  *

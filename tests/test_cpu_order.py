@@ -105,6 +105,45 @@ def test_box_ordering_batch(fv, orc):
                      for k, m in enumerate(meshes))
 
 
+def test_merged_orders_equal_the_batch_order(fv, orc):
+    """merge_orders over each problem's own order and levels (computed alone,
+    fv_order_boxes_host_levels) is the batch order of the union, 2D and 3D;
+    the levels are those of the reordered matrix."""
+    import ctypes as C
+
+    from fvb200._lib import OrderInfo, lib
+    from oracle import pattern
+    for dim, meshes in ((2, [fv.Mesh.square(s, 0.2, 10 + s) for s in (8, 16, 12, 5)]),
+                        (3, [fv.Mesh.cube(n, 0.15, 20 + n) for n in (4, 6, 3)])):
+        parts, offs, cc, own = [], [0], [], []
+        for m in meshes:
+            ptr, cols = pattern(m)
+            parts.append((ptr, cols))
+            offs.append(offs[-1] + m.n_cells)
+            cc.append(m.cell_center)
+            perm_k, info_k, lev_k = fv.order_boxes_host(m.cell_center, ptr, cols, 0, np.zeros(dim), np.ones(dim),
+                                                        levels=True)
+            lv, nl = orc.levels(*orc.permute(ptr, cols, np.ones(len(cols)), perm_k)[:2])
+            assert np.array_equal(lev_k, lv) and nl == info_k["n_levels"] == lev_k[-1] + 1
+            own.append((perm_k, lev_k))
+        N = offs[-1]
+        uptr = np.concatenate([[0]] + [p[0][1:] + sum(len(q[1]) for q in parts[:k]) for k, p in enumerate(parts)])
+        ucol = np.concatenate([p[1] + offs[k] for k, p in enumerate(parts)]).astype(np.int32)
+        uptr = uptr.astype(np.int32)
+        cen = np.ascontiguousarray(np.concatenate(cc))
+        off = np.array(offs, np.int64)
+        lo, hi = np.zeros(dim * len(meshes)), np.ones(dim * len(meshes))
+        perm = np.empty(N, np.int32)
+        info = OrderInfo()
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        st = lib().fv_order_boxes_batch_host(len(meshes), off.ctypes.data_as(C.POINTER(C.c_int64)), dim,
+                                             cen.ctypes.data_as(dp), dim, lo.ctypes.data_as(dp),
+                                             hi.ctypes.data_as(dp), uptr.ctypes.data_as(ip), ucol.ctypes.data_as(ip),
+                                             0, perm.ctypes.data_as(ip), C.byref(info))
+        assert st == 0
+        assert np.array_equal(fv.merge_orders(own, offs[:-1]), perm)
+
+
 def test_box_ordering_rejects_bad_input(fv):
     from fvb200 import FvError
     with pytest.raises(FvError):

@@ -71,8 +71,11 @@ def test_admitted_mid_flight_same_as_alone(fv, solver, precision):
     if solver == "cg":
         probs = {k: _square(fv, s, 40 + i) for i, (k, s) in enumerate(zip("abcde", [14, 9, 20, 11, 16]))}
     else:
-        probs = {k: _cube(fv, n, 60 + i) for i, (k, n) in enumerate(zip("abcde", [6, 4, 7, 5, 6]))}
+        probs = {k: _cube(fv, n, 60 + i) for i, (k, n) in enumerate(zip("abcde", [8, 5, 16, 6, 10]))}
     alone = {k: _alone(fv, p, solver, precision, ordering, tile) for k, p in probs.items()}
+    group = 8 if solver == "cg" else 4  # iterations per advance group
+    # c runs in three waves: 8 iterations, one group, then the rest
+    assert alone["c"][1] > 8 + 2 * group
     kw = dict(precision=precision, solver=solver, **{k: v for k, v in OPTS.items()})
     got = {}
 
@@ -102,7 +105,7 @@ def test_admitted_mid_flight_same_as_alone(fv, solver, precision):
     b1.close()
     rep = b2.report()
     assert rep["iterations"][1] >= 8 and rep["iterations"][2] >= 8 and rep["iterations"][0] == 0
-    b2.advance(12)
+    b2.advance(group)
     done2 = collect(w2, names2, b2)
     assert not done2[1], "c must still be running to be carried again"
 
@@ -193,3 +196,20 @@ def test_invalid_carry_is_refused(fv):
     ok2 = BatchCG(w2["A"], w2["mb"].cell_offsets, 256)
     with pytest.raises(FvError):
         ok2.begin(w2["P"], w2["b"], w2["x"], precision="fp64", carry_from=ok, carry=[0, -1])
+
+
+def test_merged_mesh_orders_equal_the_union_order(fv):
+    """A wave's order merged from its meshes' own orders (each computed once
+    per mesh) is the order fv_order_boxes gives the union, 2D and 3D."""
+    from fvb200.serve import mesh_order
+    for probs in ([_square(fv, s, 80 + s) for s in (12, 30, 7, 21)], [_cube(fv, n, 90 + n) for n in (5, 9, 3)]):
+        w = _system(fv, probs, None)
+        ref, info = fv.order_boxes(w["A"], offsets=w["mb"].cell_offsets)
+        merged = fv.merge_orders([mesh_order(fv, p[0]) for p in probs], w["mb"].cell_offsets)
+        assert np.array_equal(merged, ref)
+        # the levels reported for one mesh alone are those of its reordered factor
+        perm, _, lev = fv.order_boxes(_system(fv, probs[1:2], None)["A"], levels=True)
+        assert np.all(np.diff(lev) >= 0) and lev[0] == 0
+        P = (fv.IncompleteCholesky if probs[0][2] is None else fv.IncompleteLowerUpper).from_matrix(
+            _system(fv, probs[1:2], None)["A"], 0, ordering=perm)
+        assert P.levels()[2] == int(lev[-1]) + 1
