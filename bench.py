@@ -272,7 +272,8 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
             marks[-1].record(stream)
         x.data.zero_()
         if mixed:
-            o = single.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol, inner_relative_tolerance=1e-2,
+            o = single.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol,
+                             inner_relative_tolerance=ctx.get("mixed_delta", 1e-2),
                              max_iterations=20000, solver=wl["solver"])
             return SimpleNamespace(iterations=int(o["iterations"][0]), refinements=int(o["outer_steps"][0]),
                                    fallback=int(o["fp64_fallback"][0]), final=float(o["final_residual"][0]))
@@ -978,6 +979,8 @@ def main():
     ap.add_argument("--workload", default="cube128_convdiff", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-delta", type=float, default=1e-2,
+                    help="mixed precision: FP32 residual reduction that triggers an FP64 residual replacement")
     ap.add_argument("--ordering", default="boxes", choices=["boxes", "natural"],
                     help="factorisation order of the single-problem workloads: the reordered perf mode (boxes) "
                          "or the reference's natural order")
@@ -1027,6 +1030,7 @@ def main():
     ordering = None if args.ordering == "natural" else args.ordering
     precision = wl.get("precision", "fp64")
     ctx = setup_single(args, wl, rank, world, local_rank)
+    ctx["mixed_delta"] = args.mixed_delta
     res = measure_single(ctx, ordering, args.steps, args.warmup, precision=precision, e2e=True, kernels=True)
     K = args.steps
     solves = K * world

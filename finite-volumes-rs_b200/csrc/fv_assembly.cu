@@ -604,8 +604,8 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
 // One row per thread, each output value receiving the same additions in the
 // same order as in k_assemble (MAXF is small: 4 for triangles and
 // tetrahedra, 8 up to hexahedra).
-template <int DIM, int MAXF, bool CORR>
-__global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
+template <int DIM, int MAXF, bool CORR, int MINB = (MAXF <= 4 ? 6 : 3)>
+__global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_reg(AssembleArgs a) {
     extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
     const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
     const int64_t i = b0 + threadIdx.x;
@@ -730,6 +730,8 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
         if (a.grad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
+        } else if (a.cf_pad && asm_pipe_choice() == 3) {
+            fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MAXF <= 4 ? 4 : 2><<<G, B, smem, st>>>(a);
         } else if (a.cf_pad && asm_pipe_choice()) {
             const size_t smem_p = smem + 2 * B * sizeof(AsmSlot<MAXF>);
             constexpr int MB = MAXF <= 4 ? 6 : 3;
