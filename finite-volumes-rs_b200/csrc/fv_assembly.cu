@@ -86,6 +86,8 @@ struct AssembleArgs {
     const double *prev, *prev2, *dens, *densp, *densp2;
     double c_lin, c_div;
     const double *lin, *divflux;
+    // Orthogonal scheme with the mesh's cached geometry: 1/|d| per face, volume per cell
+    const double *invd, *vol;
 };
 
 // Cell terms of the expression (assembly.rs:26-32): lhs and rhs per unit
@@ -447,23 +449,32 @@ __device__ __forceinline__ int unpad(int (&jj)[MAXF]) {
 // the block's staging area (stage[row_ptr[i] - base ...]) so the stores of the
 // values are coalesced.  fe / jj: the cell's incidences (face id with the
 // neighbour-side bit, the other cell or -1), deg of them.
-template <int DIM, int MAXF, bool CORR>
+//
+// GEO (Orthogonal scheme only): 1/|d| of every face comes from the mesh's
+// cached a.invd (k_face_invd: the same expression, evaluated once per face) and
+// the cell's volume is V, so no cell centre is gathered.
+template <int DIM, int MAXF, bool CORR, bool GEO = false>
 __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, bool live, const int (&fe)[MAXF],
                                            const int (&jj)[MAXF], int deg, const double4 &ci4, double srci,
-                                           double *stage, int base) {
+                                           double *stage, int base, double Vgeo = 0.0) {
+    static_assert(!(GEO && CORR), "cached geometry serves the Orthogonal scheme");
     double3 oc[MAXF];
-    double ar[MAXF], kp[MAXF], fl[MAXF];
+    double ar[MAXF], kp[MAXF], fl[MAXF], tv[MAXF];
 #pragma unroll
     for (int k = 0; k < MAXF; ++k) {
         oc[k] = make_double3(0.0, 0.0, 0.0);
-        ar[k] = kp[k] = fl[k] = 0.0;
+        ar[k] = kp[k] = fl[k] = tv[k] = 0.0;
         if (k < deg) {
             const int f = fe[k] & 0x7fffffff;
             ar[k] = a.area[f];
             if (a.c_lap != 0.0) kp[k] = a.kappa[f];
             if (a.c_conv != 0.0) fl[k] = a.flux[f];
-            const double4 o = jj[k] >= 0 ? a.cell[jj[k]] : a.bfc[f - a.fb0];
-            oc[k] = make_double3(o.x, o.y, o.z);
+            if (GEO) {
+                tv[k] = a.invd[f];
+            } else {
+                const double4 o = jj[k] >= 0 ? a.cell[jj[k]] : a.bfc[f - a.fb0];
+                oc[k] = make_double3(o.x, o.y, o.z);
+            }
         }
     }
     // distinct neighbours: the first incidence of each other cell carries its slot
@@ -478,7 +489,7 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
         ndist += f1 ? 1 : 0;
         pd += (f1 && jj[k] < (int)i) ? 1 : 0;
     }
-    const double V = ci4.w;
+    const double V = GEO ? Vgeo : ci4.w;
     double lcell = 0.0, rcell = 0.0;  // cell loop (assembly.rs:26-32)
     if (live) cell_terms(a, i, srci, lcell, rcell);
     double diag = lcell * V;
@@ -499,7 +510,9 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
                 pj = make_double3(oc[k].x, oc[k].y, oc[k].z);
             }
             double t, rsch = 0.0;
-            if (!CORR) {  // Orthogonal (orthogonal.rs:26-46): 1/|d|
+            if (GEO) {
+                t = tv[k];
+            } else if (!CORR) {  // Orthogonal (orthogonal.rs:26-46): 1/|d|
                 double d2 = 0.0;
                 double dd = pj.x - pi.x;
                 d2 += dd * dd;
@@ -604,7 +617,7 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
 // One row per thread, each output value receiving the same additions in the
 // same order as in k_assemble (MAXF is small: 4 for triangles and
 // tetrahedra, 8 up to hexahedra).
-template <int DIM, int MAXF, bool CORR, int MINB = (MAXF <= 4 ? 6 : 3)>
+template <int DIM, int MAXF, bool CORR, int MINB = (MAXF <= 4 ? 6 : 3), bool GEO = false>
 __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_reg(AssembleArgs a) {
     extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
     const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
@@ -626,12 +639,15 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_reg(AssembleArgs a
     }
     const int deg = unpad<MAXF>(jj);
     double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
-    double srci = 0.0;
+    double srci = 0.0, vol = 0.0;
     if (live) {
-        ci4 = a.cell[i];
+        if (GEO)
+            vol = a.vol[i];
+        else
+            ci4 = a.cell[i];
         if (a.c_src != 0.0) srci = a.src[i];
     }
-    row_values<DIM, MAXF, CORR>(a, i, live, fe, jj, deg, ci4, srci, stage, base);
+    row_values<DIM, MAXF, CORR, GEO>(a, i, live, fe, jj, deg, ci4, srci, stage, base, vol);
     __syncthreads();
     double *out = a.vals + base;
     for (int q = threadIdx.x; q < top - base; q += kAsmBlock) out[q] = stage[q];
@@ -654,7 +670,7 @@ struct AsmSlot {
     int2 cf[MAXF];
     double4 cell;
     double src;
-    double pad;
+    double vol;  // cached-geometry kernels: the volume instead of the cell record
 };
 
 // The same rows, a block walking tiles of kAsmBlock cells: while a tile's
@@ -662,7 +678,7 @@ struct AsmSlot {
 // already on their way into shared memory (cp.async, one slot per thread,
 // read back only by the thread that copied it), so the first of the two
 // dependent memory round trips of a row is off the critical path.
-template <int DIM, int MAXF, int MINB>
+template <int DIM, int MAXF, int MINB, bool GEO = false>
 __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs a, int64_t ntiles) {
     extern __shared__ __align__(32) double smem[];
     double *stage = smem;  // kAsmBlock * (MAXF + 1) values
@@ -674,8 +690,12 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
             AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
 #pragma unroll
             for (int k = 0; k < MAXF; k += 2) asm_cp16(&q.cf[k], &a.cf_pad[c * MAXF + k]);
-            asm_cp16(&q.cell, &a.cell[c]);
-            asm_cp16(reinterpret_cast<double *>(&q.cell) + 2, reinterpret_cast<const double *>(&a.cell[c]) + 2);
+            if (GEO) {
+                asm_cp8(&q.vol, &a.vol[c]);
+            } else {
+                asm_cp16(&q.cell, &a.cell[c]);
+                asm_cp16(reinterpret_cast<double *>(&q.cell) + 2, reinterpret_cast<const double *>(&a.cell[c]) + 2);
+            }
             if (use_src) asm_cp8(&q.src, &a.src[c]);
         }
         asm_cp_commit();
@@ -693,7 +713,7 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
         const bool live = i < a.n;
         int fe[MAXF], jj[MAXF];
         double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
-        double srci = 0.0;
+        double srci = 0.0, vol = 0.0;
         const AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
 #pragma unroll
         for (int k = 0; k < MAXF; ++k) {
@@ -701,17 +721,49 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
             jj[k] = live ? q.cf[k].y : -2;
         }
         if (live) {
-            ci4 = q.cell;
+            if (GEO)
+                vol = q.vol;
+            else
+                ci4 = q.cell;
             if (use_src) srci = q.src;
         }
         const int deg = unpad<MAXF>(jj);
-        row_values<DIM, MAXF, false>(a, i, live, fe, jj, deg, ci4, srci, stage, base);
+        row_values<DIM, MAXF, false, GEO>(a, i, live, fe, jj, deg, ci4, srci, stage, base, vol);
         __syncthreads();
         double *out = a.vals + base;
         for (int r = threadIdx.x; r < top - base; r += kAsmBlock) out[r] = stage[r];
         __syncthreads();  // the stage is rewritten by the next tile
         buf ^= 1;
     }
+}
+
+// 1/|d| of every face with the expression of the assembly kernels (pi the
+// owner's centre, pj the neighbour's or the boundary face's), and the cells'
+// volumes: the Orthogonal scheme's geometry, cached on the mesh.
+template <int DIM>
+__global__ void k_face_invd(int64_t nf, int64_t fb0, const int2 *__restrict__ fc, const double4 *__restrict__ cell,
+                            const double4 *__restrict__ bfc, double *__restrict__ invd) {
+    for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x) {
+        const int2 oc = fc[f];
+        const double4 o = cell[oc.x];
+        const double4 q = oc.y >= 0 ? cell[oc.y] : bfc[f - fb0];
+        const double3 pi = make_double3(o.x, o.y, o.z), pj = make_double3(q.x, q.y, q.z);
+        double d2 = 0.0;
+        double dd = pj.x - pi.x;
+        d2 += dd * dd;
+        dd = pj.y - pi.y;
+        d2 += dd * dd;
+        if (DIM == 3) {
+            dd = pj.z - pi.z;
+            d2 += dd * dd;
+        }
+        invd[f] = 1.0 / sqrt(d2);
+    }
+}
+
+__global__ void k_cell_vol(int64_t n, const double4 *__restrict__ cell, double *__restrict__ vol) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        vol[i] = cell[i].w;
 }
 
 static int asm_pipe_choice() {
@@ -728,8 +780,26 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
+        const int v = asm_pipe_choice();
         if (a.grad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
+        } else if (a.cf_pad && a.invd && v >= 4) {
+            constexpr int MB = MAXF <= 4 ? 6 : 3, MBW = MAXF <= 4 ? 4 : 2;
+            if (v == 4) {
+                fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MB, true><<<G, B, smem, st>>>(a);
+            } else if (v == 7) {
+                fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MBW, true><<<G, B, smem, st>>>(a);
+            } else {
+                const size_t smem_p = smem + 2 * B * sizeof(AsmSlot<MAXF>);
+                auto kern = v == 5 ? k_assemble_pipe<DIM, MAXF, MBW, true> : k_assemble_pipe<DIM, MAXF, MB, true>;
+                int per_sm = 1;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, B, smem_p);
+                int sms = 148, dev = 0;
+                if (cudaGetDevice(&dev) == cudaSuccess)
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                const unsigned Gp = (unsigned)std::min<int64_t>(G, (int64_t)sms * std::max(per_sm, 1));
+                fv_note_launch(), kern<<<Gp, B, smem_p, st>>>(a, (int64_t)G);
+            }
         } else if (a.cf_pad && asm_pipe_choice() == 3) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MAXF <= 4 ? 4 : 2><<<G, B, smem, st>>>(a);
         } else if (a.cf_pad && asm_pipe_choice()) {
@@ -838,6 +908,8 @@ extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
     cudaFree(m->gcf_face);
     cudaFree(m->gcoef);
     cudaFree(m->gdiag);
+    cudaFree(m->face_invd);
+    cudaFree(m->cell_vol);
     cudaFree(m->row_ptr);
     cudaFree(m->cols);
     delete m;
@@ -1052,6 +1124,43 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
     return FV_OK;
 }
 
+// The Orthogonal scheme's cached geometry of a mesh (1/|d| per face, volume per
+// cell), built on first use.  Meshes are shared by host threads (a server's
+// mesh cache), so the build holds a lock and the pointers are published only
+// after the kernels have finished.
+static fv_status ensure_orth_geometry(fv_mesh *m, cudaStream_t st) {
+    static std::mutex lock;
+    std::lock_guard<std::mutex> g(lock);
+    if (m->face_invd && m->cell_vol) return FV_OK;
+    double *invd = nullptr, *vol = nullptr;
+    cudaError_t e = cudaMalloc(&invd, sizeof(double) * (m->n_faces ? m->n_faces : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&vol, sizeof(double) * (m->n_cells ? m->n_cells : 1));
+    if (e == cudaSuccess && m->n_faces) {
+        const unsigned G = (unsigned)std::min<int64_t>((m->n_faces + 255) / 256, 148 * 16);
+        if (m->dim == 2)
+            fv_note_launch(), k_face_invd<2><<<G, 256, 0, st>>>(m->n_faces, m->n_faces - m->n_bfaces, m->face_cells,
+                                                                 m->cell, m->bface_center, invd);
+        else
+            fv_note_launch(), k_face_invd<3><<<G, 256, 0, st>>>(m->n_faces, m->n_faces - m->n_bfaces, m->face_cells,
+                                                                 m->cell, m->bface_center, invd);
+    }
+    if (e == cudaSuccess && m->n_cells) {
+        const unsigned G = (unsigned)std::min<int64_t>((m->n_cells + 255) / 256, 148 * 16);
+        fv_note_launch(), k_cell_vol<<<G, 256, 0, st>>>(m->n_cells, m->cell, vol);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(invd);
+        cudaFree(vol);
+        fv_internal_set_cuda_error(e, "fv_assemble geometry");
+        return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
+    }
+    m->face_invd = invd;
+    m->cell_vol = vol;
+    return FV_OK;
+}
+
 extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const fv_bc_desc *bc, fv_csr **A,
                                  double *b, void *stream) {
     if (!m || !terms || !A || !b) return FV_ERR_INVALID;
@@ -1140,6 +1249,13 @@ extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const f
         args.grad = terms->gradients;
     } else if (terms->scheme != FV_SCHEME_ORTHOGONAL && terms->scheme != FV_SCHEME_CORRECTED) {
         return FV_ERR_INVALID;
+    }
+    args.invd = nullptr;
+    args.vol = nullptr;
+    if (!args.grad && m->cf_pad) {
+        FV_TRY(ensure_orth_geometry(m, st));
+        args.invd = m->face_invd;
+        args.vol = m->cell_vol;
     }
     const int mf = m->maxf;
     if (m->dim == 2) {
