@@ -402,7 +402,10 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
         bytes_prec = (12 * nnz + 40 * N) if wl["solver"] == "bicgstab" else (12 * (nnz + N) + 56 * N)
         if ordering is not None:
             bytes_prec += 8 * N
-        bytes_asm = 32 * F + 24 * Fb + 40 * N + 8 * (F - Fb) + 8 * nnz + 8 * N
+        # assembly (Orthogonal scheme, the mesh's cached geometry): per face area, kappa, flux, 1/|d| and the
+        # owner/neighbour pair; per boundary face the two constraint values; per cell volume and source;
+        # the values and the right-hand side written
+        bytes_asm = 40 * F + 16 * Fb + 16 * N + 8 * nnz + 8 * N
         it_mean = float(np.mean(iters))
         per_it = 2 if wl["solver"] == "bicgstab" else 1
         step_s = elapsed / steps

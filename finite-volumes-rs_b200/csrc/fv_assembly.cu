@@ -617,8 +617,8 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
 // One row per thread, each output value receiving the same additions in the
 // same order as in k_assemble (MAXF is small: 4 for triangles and
 // tetrahedra, 8 up to hexahedra).
-template <int DIM, int MAXF, bool CORR, int MINB = (MAXF <= 4 ? 6 : 3), bool GEO = false>
-__global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_reg(AssembleArgs a) {
+template <int DIM, int MAXF, bool CORR>
+__global__ void __launch_bounds__(kAsmBlock, MAXF <= 4 ? 6 : 3) k_assemble_reg(AssembleArgs a) {
     extern __shared__ double stage[];  // kAsmBlock * (MAXF + 1) values
     const int64_t b0 = (int64_t)blockIdx.x * kAsmBlock;
     const int64_t i = b0 + threadIdx.x;
@@ -639,15 +639,12 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_reg(AssembleArgs a
     }
     const int deg = unpad<MAXF>(jj);
     double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
-    double srci = 0.0, vol = 0.0;
+    double srci = 0.0;
     if (live) {
-        if (GEO)
-            vol = a.vol[i];
-        else
-            ci4 = a.cell[i];
+        ci4 = a.cell[i];
         if (a.c_src != 0.0) srci = a.src[i];
     }
-    row_values<DIM, MAXF, CORR, GEO>(a, i, live, fe, jj, deg, ci4, srci, stage, base, vol);
+    row_values<DIM, MAXF, CORR>(a, i, live, fe, jj, deg, ci4, srci, stage, base);
     __syncthreads();
     double *out = a.vals + base;
     for (int q = threadIdx.x; q < top - base; q += kAsmBlock) out[q] = stage[q];
@@ -664,21 +661,22 @@ __device__ __forceinline__ void asm_cp8(void *smem, const void *gmem) {
 __device__ __forceinline__ void asm_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void asm_cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// Per-thread prefetch slot of one cell: incidences, centre and volume, source.
+// Per-thread prefetch slot of one cell: incidences, source, volume.
 template <int MAXF>
 struct AsmSlot {
     int2 cf[MAXF];
-    double4 cell;
     double src;
-    double vol;  // cached-geometry kernels: the volume instead of the cell record
+    double vol;
 };
 
-// The same rows, a block walking tiles of kAsmBlock cells: while a tile's
-// rows are computed, the next tile's incidences, cell centres and sources are
-// already on their way into shared memory (cp.async, one slot per thread,
-// read back only by the thread that copied it), so the first of the two
-// dependent memory round trips of a row is off the critical path.
-template <int DIM, int MAXF, int MINB, bool GEO = false>
+// The Orthogonal scheme's rows with the mesh's cached geometry, a block
+// walking tiles of kAsmBlock cells: while a tile's rows are computed, the
+// next tile's incidences, sources and volumes are already on their way into
+// shared memory (cp.async, one slot per thread, read back only by the thread
+// that copied it), so only the face gathers (area, kappa, flux, 1/|d|) remain
+// between a row's start and its values; no cell centre is read and no
+// square root is taken.
+template <int DIM, int MAXF, int MINB>
 __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs a, int64_t ntiles) {
     extern __shared__ __align__(32) double smem[];
     double *stage = smem;  // kAsmBlock * (MAXF + 1) values
@@ -690,12 +688,7 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
             AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
 #pragma unroll
             for (int k = 0; k < MAXF; k += 2) asm_cp16(&q.cf[k], &a.cf_pad[c * MAXF + k]);
-            if (GEO) {
-                asm_cp8(&q.vol, &a.vol[c]);
-            } else {
-                asm_cp16(&q.cell, &a.cell[c]);
-                asm_cp16(reinterpret_cast<double *>(&q.cell) + 2, reinterpret_cast<const double *>(&a.cell[c]) + 2);
-            }
+            asm_cp8(&q.vol, &a.vol[c]);
             if (use_src) asm_cp8(&q.src, &a.src[c]);
         }
         asm_cp_commit();
@@ -712,7 +705,7 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
         const int top = a.row_ptr[bend];
         const bool live = i < a.n;
         int fe[MAXF], jj[MAXF];
-        double4 ci4 = make_double4(0.0, 0.0, 0.0, 0.0);
+        const double4 none = make_double4(0.0, 0.0, 0.0, 0.0);
         double srci = 0.0, vol = 0.0;
         const AsmSlot<MAXF> &q = slot[buf * kAsmBlock + threadIdx.x];
 #pragma unroll
@@ -721,14 +714,11 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
             jj[k] = live ? q.cf[k].y : -2;
         }
         if (live) {
-            if (GEO)
-                vol = q.vol;
-            else
-                ci4 = q.cell;
+            vol = q.vol;
             if (use_src) srci = q.src;
         }
         const int deg = unpad<MAXF>(jj);
-        row_values<DIM, MAXF, false, GEO>(a, i, live, fe, jj, deg, ci4, srci, stage, base, vol);
+        row_values<DIM, MAXF, false, true>(a, i, live, fe, jj, deg, none, srci, stage, base, vol);
         __syncthreads();
         double *out = a.vals + base;
         for (int r = threadIdx.x; r < top - base; r += kAsmBlock) out[r] = stage[r];
@@ -766,12 +756,26 @@ __global__ void k_cell_vol(int64_t n, const double4 *__restrict__ cell, double *
         vol[i] = cell[i].w;
 }
 
-static int asm_pipe_choice() {
+static int asm_minb_choice() {
     static int v = [] {
-        const char *e = getenv("FV_ASM_PIPE");
-        return e ? atoi(e) : 0;
+        const char *e = getenv("FV_ASM_MINB");
+        return e ? atoi(e) : 6;
     }();
     return v;
+}
+
+template <int DIM, int MAXF, int MINB>
+void launch_pipe(const AssembleArgs &a, unsigned G, size_t smem, cudaStream_t st) {
+    const size_t smem_p = smem + 2 * kAsmBlock * sizeof(AsmSlot<MAXF>);
+    static int per_sm = 0;  // resident blocks per SM (launch bounds, registers, shared memory)
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_pipe<DIM, MAXF, MINB>, kAsmBlock, smem_p);
+        if (per_sm < 1) per_sm = 1;
+    }
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned Gp = (unsigned)std::min<int64_t>(G, (int64_t)sms * per_sm);
+    fv_note_launch(), k_assemble_pipe<DIM, MAXF, MINB><<<Gp, kAsmBlock, smem_p, st>>>(a, (int64_t)G);
 }
 
 template <int DIM, int MAXF>
@@ -780,44 +784,17 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
-        const int v = asm_pipe_choice();
         if (a.grad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
-        } else if (a.cf_pad && a.invd && v >= 4) {
-            constexpr int MB = MAXF <= 4 ? 6 : 3, MBW = MAXF <= 4 ? 4 : 2;
-            if (v == 4) {
-                fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MB, true><<<G, B, smem, st>>>(a);
-            } else if (v == 7) {
-                fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MBW, true><<<G, B, smem, st>>>(a);
+        } else if (a.cf_pad && a.invd) {
+            if constexpr (MAXF <= 4) {
+                if (asm_minb_choice() == 8)
+                    launch_pipe<DIM, MAXF, 8>(a, G, smem, st);
+                else
+                    launch_pipe<DIM, MAXF, 6>(a, G, smem, st);
             } else {
-                const size_t smem_p = smem + 2 * B * sizeof(AsmSlot<MAXF>);
-                auto kern = v == 5 ? k_assemble_pipe<DIM, MAXF, MBW, true> : k_assemble_pipe<DIM, MAXF, MB, true>;
-                int per_sm = 1;
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, B, smem_p);
-                int sms = 148, dev = 0;
-                if (cudaGetDevice(&dev) == cudaSuccess)
-                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-                const unsigned Gp = (unsigned)std::min<int64_t>(G, (int64_t)sms * std::max(per_sm, 1));
-                fv_note_launch(), kern<<<Gp, B, smem_p, st>>>(a, (int64_t)G);
+                launch_pipe<DIM, MAXF, 3>(a, G, smem, st);
             }
-        } else if (a.cf_pad && asm_pipe_choice() == 3) {
-            fv_note_launch(), k_assemble_reg<DIM, MAXF, false, MAXF <= 4 ? 4 : 2><<<G, B, smem, st>>>(a);
-        } else if (a.cf_pad && asm_pipe_choice()) {
-            const size_t smem_p = smem + 2 * B * sizeof(AsmSlot<MAXF>);
-            constexpr int MB = MAXF <= 4 ? 6 : 3;
-            const bool wide = asm_pipe_choice() == 2;  // fewer blocks, no register cap below the need
-            auto kern = wide ? k_assemble_pipe<DIM, MAXF, MB == 6 ? 4 : 2> : k_assemble_pipe<DIM, MAXF, MB>;
-            static int per_sm[2] = {0, 0};
-            if (!per_sm[wide]) {
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[wide], kern, B, smem_p);
-                if (per_sm[wide] < 1) per_sm[wide] = 1;
-            }
-            int sms = 148;
-            int dev = 0;
-            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            const int64_t ntiles = G;
-            const unsigned Gp = (unsigned)std::min<int64_t>(ntiles, (int64_t)sms * per_sm[wide]);
-            fv_note_launch(), kern<<<Gp, B, smem_p, st>>>(a, ntiles);
         } else if (a.cf_pad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, false><<<G, B, smem, st>>>(a);
         } else {
