@@ -175,6 +175,8 @@ def sweep_schedule(P):
     act, st = P.schedule()
     if act == 3:
         return {"kind": "level chunks, next chunk prefetched"}
+    if act == 4:
+        return {"kind": "permuted system: rows sorted by level, consecutive rows, block tickets (k_sweep_seq)"}
     if act != 2:
         return {"kind": "level chunks"}
     return {"kind": "box tiles", "box_edge_cells": float(st[0]), "boxes": int(st[1]),
@@ -222,13 +224,17 @@ def setup_single(args, wl, rank, world, local_rank):
                 local_rank=local_rank, A=None)
 
 
-def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, kernels=True, tol=None):
+def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, kernels=True, tol=None,
+                   reorder="system"):
     """Time `steps` steps (after `warmup`) of one single-problem workload:
     value assembly into the resident pattern, refactorisation and a solve from
     x0 = 0 (BiCGStab + ILU(0) in 3D, CG + IC(0) in 2D) to rtol = atol = 1e-8
     (FP64), or the FP32 Krylov + FP32 factors inside FP64 reliable updates to
     |b - Ax|/|b| <= 1e-10 (precision "mixed").  ordering None = the
-    reference's natural order; "boxes" = the reordered factorisation.  tol
+    reference's natural order; "boxes" = the box-colour order, either as the
+    permuted system (reorder "system": B = Q A Q^T factorised and solved in
+    its own numbering, b permuted in and x back every step) or as the
+    reordered factorisation applied in A's numbering (reorder "precond").  tol
     replaces the target: rtol = atol (FP64) or the outer tolerance (mixed)."""
     fv, torch, wl = ctx["fv"], ctx["torch"], ctx["wl"]
     from fvb200._lib import lib
@@ -246,8 +252,19 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
         ctx["A"], _ = fv.assemble(eq, bc, mesh)
     A = ctx["A"]
     _, b = fv.assemble(eq, bc, mesh, lhs=A)
+    system = ordering is not None and reorder == "system"
     t0 = time.perf_counter()
-    P = Pcls.from_matrix(A, 0, ordering=ordering)
+    order_info = None
+    if system:
+        perm, order_info = fv.order_boxes(A)
+        S = A.permuted(perm)  # the system solved: Q A Q^T
+        P = Pcls.from_matrix(S, 0)
+        bq = fv.DistributedVector.from_size(N)
+        y = fv.DistributedVector.from_size(N)
+    else:
+        S = A
+        P = Pcls.from_matrix(A, 0, ordering=ordering)
+        order_info = P.order_info
     torch.cuda.synchronize()
     t_factor_setup = time.perf_counter() - t0
     x = fv.DistributedVector.from_size(N)
@@ -257,7 +274,7 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
         from types import SimpleNamespace
 
         from fvb200.batch import BatchCG
-        single = BatchCG(A, [0, N], 2048)
+        single = BatchCG(S, [0, N], 2048)
 
     # one step: value assembly (new rhs), refactorisation, solve from x0 = 0
     def step_b(marks=None):
@@ -266,18 +283,27 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
         if marks is not None:
             marks.append(torch.cuda.Event(enable_timing=True))
             marks[-1].record(stream)
+        if system:
+            S.refresh_permuted()
         P.refactor()
         if marks is not None:
             marks.append(torch.cuda.Event(enable_timing=True))
             marks[-1].record(stream)
-        x.data.zero_()
+        rhs, sol = (bq, y) if system else (b, x)
+        if system:
+            S.to_permuted(b, bq)
+        sol.data.zero_()
         if mixed:
-            o = single.solve(P, b, x, precision="mixed", outer_tolerance=outer_tol,
+            o = single.solve(P, rhs, sol, precision="mixed", outer_tolerance=outer_tol,
                              inner_relative_tolerance=ctx.get("mixed_delta", 1e-2),
                              max_iterations=20000, solver=wl["solver"])
-            return SimpleNamespace(iterations=int(o["iterations"][0]), refinements=int(o["outer_steps"][0]),
-                                   fallback=int(o["fp64_fallback"][0]), final=float(o["final_residual"][0]))
-        return solve(x, A, b, P, None, opts)
+            out = SimpleNamespace(iterations=int(o["iterations"][0]), refinements=int(o["outer_steps"][0]),
+                                  fallback=int(o["fp64_fallback"][0]), final=float(o["final_residual"][0]))
+        else:
+            out = solve(sol, S, rhs, P, None, opts)
+        if system:
+            S.from_permuted(y, x)
+        return out
 
     for _ in range(warmup):
         info = step_b()
@@ -334,7 +360,8 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
                       "final_fp64_residual": info.final}
     res = dict(elapsed=elapsed, steps=steps, N=N, nnz=A.shape()[2], iters=iters, lat_ms=lat_ms, relres=relres,
                err_tight=err_tight, launches=launches, clocks=clocks, phase_ms=phase_ms, mixed_info=mixed_info,
-               order_info=P.order_info, levels=P.levels()[2:], schedule=sweep_schedule(P),
+               order_info=order_info, levels=P.levels()[2:], schedule=sweep_schedule(P),
+               reorder=(reorder if ordering is not None else None),
                factor_setup_s=round(t_factor_setup, 3), x=x.numpy())
 
     if e2e:
@@ -385,11 +412,11 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
     if kernels:
         # ---- per-kernel timing of the hot kernels (roofline)
         nnz = res["nnz"]
-        y = fv.DistributedVector.from_size(N)
-        z = fv.DistributedVector.from_size(N)
+        yk = fv.DistributedVector.from_size(N)
+        zk = fv.DistributedVector.from_size(N)
         hbm, peak_kind = peaks()
-        t_spmv = time_kernel(torch, lambda: A.imul(y, x), 20, stream)
-        t_prec = time_kernel(torch, lambda: P.precondition(z, b), 10, stream)
+        t_spmv = time_kernel(torch, lambda: S.imul(yk, x), 20, stream)  # the solved system's matrix
+        t_prec = time_kernel(torch, lambda: P.precondition(zk, b), 10, stream)
         # the assembly kernel alone: the fv_assemble C call with prebuilt descriptors into a preallocated rhs
         from fvb200.linalg import assembly_launcher
         b_fixed = fv.DistributedVector.from_size(N)
@@ -398,9 +425,9 @@ def measure_single(ctx, ordering, steps, warmup, precision="fp64", e2e=True, ker
         F, Fb = mesh.n_faces, mesh.n_boundary_faces
         bytes_spmv = 12 * nnz + 20 * N
         # ILU(0) apply: 12 nnz + 40 N; IC(0): 2 (12 (nnz + N) / 2 + 28 N); the reordered
-        # sweeps also read the permutation twice (8 N)
+        # factorisation applied in A's numbering also reads the permutation twice (8 N)
         bytes_prec = (12 * nnz + 40 * N) if wl["solver"] == "bicgstab" else (12 * (nnz + N) + 56 * N)
-        if ordering is not None:
+        if ordering is not None and not system:
             bytes_prec += 8 * N
         # assembly (Orthogonal scheme, the mesh's cached geometry): per face area, kappa, flux, 1/|d| and the
         # owner/neighbour pair; per boundary face the two constraint values; per cell volume and source;
@@ -982,6 +1009,9 @@ def main():
     ap.add_argument("--workload", default="cube128_convdiff", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reorder", default="system", choices=["system", "precond"],
+                    help="box order as the permuted system Q A Q^T (default) or as the reordered factorisation "
+                         "applied in A's numbering")
     ap.add_argument("--mixed-delta", type=float, default=1e-2,
                     help="mixed precision: FP32 residual reduction that triggers an FP64 residual replacement")
     ap.add_argument("--ordering", default="boxes", choices=["boxes", "natural"],
@@ -1034,7 +1064,8 @@ def main():
     precision = wl.get("precision", "fp64")
     ctx = setup_single(args, wl, rank, world, local_rank)
     ctx["mixed_delta"] = args.mixed_delta
-    res = measure_single(ctx, ordering, args.steps, args.warmup, precision=precision, e2e=True, kernels=True)
+    res = measure_single(ctx, ordering, args.steps, args.warmup, precision=precision, e2e=True, kernels=True,
+                         reorder=args.reorder)
     K = args.steps
     solves = K * world
     value = solves / res["elapsed"]
@@ -1043,6 +1074,9 @@ def main():
     lat = sorted(res["lat_ms"])
     cfg = config_of(args, wl, N, res["nnz"])
     cfg["ordering"] = args.ordering
+    if ordering is not None:
+        cfg["reorder"] = {"system": "permuted system Q A Q^T solved in its own numbering",
+                          "precond": "reordered factorisation applied in A's numbering"}[args.reorder]
     line = {
         "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(res["elapsed"] / K * 1e3, 3), "higher_is_better": True,
@@ -1077,6 +1111,14 @@ def main():
         line["orderings"] = {args.ordering: single_summary(res, world, f"{wl['solver']}, {args.ordering} order, FP64"),
                              other: single_summary(ro, world, f"{wl['solver']}, {other} order, FP64")}
         del ro
+        if ordering is not None:  # the box order's other form
+            alt = "precond" if args.reorder == "system" else "system"
+            ra = measure_single(ctx, ordering, max(3, K // 4), 2, e2e=False, kernels=True, reorder=alt)
+            line["orderings"][f"{args.ordering}_{alt}"] = single_summary(
+                ra, world, f"{wl['solver']}, {args.ordering} order as the "
+                + ("reordered factorisation applied in A's numbering" if alt == "precond" else "permuted system")
+                + ", FP64")
+            del ra
         if precision == "fp64":
             rm = measure_single(ctx, ordering, max(3, K // 4), 2, precision="mixed", e2e=False, kernels=False)
             line["configs"] = {f"{args.workload}_mixed": single_summary(
@@ -1138,7 +1180,7 @@ def square_configs(args):
     ptr, cols, vals, rhs = oracle.assemble(p["mesh"], c[0], c[1], c[2], kappa=p["kappa"], flux=p["flux"],
                                            source=p["source"], bndi=p["bndi"], bnde=p["bnde"])
     for name, ordering in (("natural", None), ("boxes", "boxes")):
-        r = measure_single(ctx, ordering, args.steps, args.warmup, e2e=False, kernels=True)
+        r = measure_single(ctx, ordering, args.steps, args.warmup, e2e=False, kernels=True, reorder=args.reorder)
         sm = single_summary(r, 1, f"cg+ic0, {name} order, FP64")
         if ordering is None:
             pc = oracle.Precond("ic", ptr, cols, vals)

@@ -157,6 +157,11 @@ struct fv_csr {
     std::vector<uint8_t> fill_mask;
     const fv_mesh *mesh = nullptr;
     fv_symbolic *sym = nullptr;   // cached symbolic analysis (value independent)
+    // a permuted copy Q A Q^T (fv_csr_permute): the matrix its values come from,
+    // the permutation (row i = src row perm[i]) and src's entry k's position here
+    const fv_csr *perm_src = nullptr;
+    int32_t *perm = nullptr;
+    int32_t *perm_amap = nullptr;
 };
 
 // ------------------------------------------------------------------ helpers

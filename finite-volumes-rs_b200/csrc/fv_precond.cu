@@ -91,7 +91,9 @@ struct fv_precond {
     unsigned *done = nullptr;     // factorisation flags
     unsigned epoch = 0;
     int schedule = 1;             // 1: level chunks (default); 2: box tiles (when planned);
-                                  // 3: level chunks, next chunk prefetched
+                                  // 3: level chunks, next chunk prefetched; 4: consecutive rows
+                                  // (the default when the rows are sorted by forward level)
+    bool contiguous = false;      // the rows are sorted by forward level
     int sweep_blocks = 0;         // blocks of 8 warps per sweep launch (0: the kernels' default)
     int sweep_rpt = 0;            // rows per thread of the reordered sweeps (0: default)
     unsigned *ctrl = nullptr;     // [0,1] fwd ticket/exit  [2,3] bwd ticket/exit  [4,5] factor ticket/exit
@@ -1803,6 +1805,24 @@ fv_status fv_precond_apply_dev(fv_precond *P, const double *r, double *z, cudaSt
         FV_CUDA_TRY(cudaGetLastError());
         return FV_OK;
     }
+    if (P->schedule == 4) {  // rows in index order: consecutive chunks, block tickets
+        const int R = seq_rpt(P), Gs = seq_grid(P, n, R);
+        const SweepPerm<double> none;
+        if (P->kind == 2)
+            launch_sweep_seq<double, true, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                  P->l_val, nullptr, r, P->tmp, nullptr, z, P->ctrl, P->err, skip,
+                                                  rs, none);
+        else
+            launch_sweep_seq<double, false, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                   P->l_val, P->dinv, r, P->tmp, nullptr, z, P->ctrl, P->err, skip,
+                                                   rs, none);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_sweep_seq<double, false, true>(s->max_upper, R, Gs, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u_val,
+                                              P->dinv, P->tmp, z, P->tmp, nullptr, P->ctrl + 2, P->err, skip, rs,
+                                              none);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (use_tiles(P)) return tiled_apply<double>(P, r, z, P->tmp, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1909,6 +1929,24 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
         FV_CUDA_TRY(cudaGetLastError());
         return FV_OK;
     }
+    if (P->schedule == 4) {  // rows in index order: consecutive chunks, block tickets
+        const int R = seq_rpt(P), Gs = seq_grid(P, n, R);
+        const SweepPerm<float> none;
+        if (P->kind == 2)
+            launch_sweep_seq<float, true, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                 P->l32, nullptr, r, P->tmp32, nullptr, z, P->ctrl, P->err, skip, rs,
+                                                 none);
+        else
+            launch_sweep_seq<float, false, false>(s->max_lower, R, Gs, st, n, s->fwd_order, s->l_ptr, s->l_col,
+                                                  P->l32, P->dinv32, r, P->tmp32, nullptr, z, P->ctrl, P->err, skip,
+                                                  rs, none);
+        FV_CUDA_TRY(cudaGetLastError());
+        launch_sweep_seq<float, false, true>(s->max_upper, R, Gs, st, n, s->bwd_order, s->u_ptr, s->u_col, P->u32,
+                                             P->dinv32, P->tmp32, z, P->tmp32, nullptr, P->ctrl + 2, P->err, skip, rs,
+                                             none);
+        FV_CUDA_TRY(cudaGetLastError());
+        return FV_OK;
+    }
     if (use_tiles(P)) return tiled_apply<float>(P, r, z, P->tmp32, st, skip, rs);
     const bool pf = P->schedule == 3;
     if (P->kind == 2)
@@ -1925,7 +1963,7 @@ fv_status fv_precond_apply_dev_f32(fv_precond *P, const float *r, float *z, cuda
 }
 
 extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t *active, double *stats) {
-    if (!P || request < -1 || request > 3) return FV_ERR_INVALID;
+    if (!P || request < -1 || request > 4) return FV_ERR_INVALID;
     if (P->kind == 3) {  // no sweeps to schedule
         if (active) *active = 1;
         if (stats) std::fill(stats, stats + 6, 0.0);
@@ -1934,8 +1972,9 @@ extern "C" fv_status fv_precond_schedule(fv_precond *P, int32_t request, int32_t
     fv_symbolic *s = P->sym;
     if (request == 2) FV_TRY(build_tiles(s, P->A, fv_stream(nullptr)));
     if (request == 2 && !s->tiled) return FV_ERR_UNSUPPORTED;
+    if (request == 4 && (P->perm || P->fill)) return FV_ERR_UNSUPPORTED;
     if (request >= 0) P->schedule = request <= 1 ? 1 : request;
-    if (active) *active = use_tiles(P) ? 2 : (P->schedule == 3 ? 3 : 1);
+    if (active) *active = use_tiles(P) ? 2 : (P->schedule == 3 || P->schedule == 4 ? P->schedule : 1);
     if (stats) {
         stats[0] = s->t_edge;
         stats[1] = s->t_nb[0];
@@ -1994,6 +2033,13 @@ static fv_status precond_alloc(fv_precond *P, cudaStream_t st) {
     return FV_OK;
 }
 
+namespace {
+__global__ void k_order_not_identity(int64_t n, const int32_t *__restrict__ order, int *flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (order[i] != (int32_t)i) *flag = 1;
+}
+}  // namespace
+
 static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_precond **out) {
     if (!Ac || !out) return FV_ERR_INVALID;
     if (Ac->nrows != Ac->ncols) return FV_ERR_INVALID;
@@ -2014,6 +2060,20 @@ static fv_status factor_common(const fv_csr *Ac, int kind, cudaStream_t st, fv_p
         if (s != FV_OK) {
             fv_precond_destroy(P);
             return s;
+        }
+        // rows already sorted by forward level (a matrix permuted by a level-sorted
+        // order): the sweeps take consecutive rows (schedule 4), no order array
+        if (A->fill_mask.empty() && sym->max_lower <= 8 && sym->max_upper <= 8) {
+            int notid = 0;
+            FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+            fv_note_launch(), k_order_not_identity<<<(unsigned)std::min<int64_t>((A->nrows + 255) / 256, 148 * 8), 256,
+                                                     0, st>>>(A->nrows, sym->fwd_order, P->err);
+            FV_CUDA_TRY(cudaGetLastError());
+            FV_CUDA_TRY(cudaMemcpyAsync(&notid, P->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            FV_CUDA_TRY(cudaMemsetAsync(P->err, 0, sizeof(int), st));
+            FV_CUDA_TRY(cudaStreamSynchronize(st));
+            if (!notid) P->schedule = 4;
+            P->contiguous = !notid;
         }
     } else if (P->A != A || P->kind != kind) {
         return FV_ERR_INVALID;
@@ -2181,6 +2241,7 @@ static fv_status fill_factor(const fv_csr *Ac, int kind, int level, cudaStream_t
     tmp.amap = nullptr;
     fv_precond *P = nullptr;
     if (s == FV_OK) s = factor_common(F, kind, st, &P);
+    if (s == FV_OK) P->schedule = 1;  // fill patterns keep the level chunks
     if (s != FV_OK) {
         cudaFree(damap);
         fv_csr_destroy(F);
@@ -2278,10 +2339,12 @@ __global__ void k_perm_rows(int64_t n, const int32_t *__restrict__ perm, const i
 }
 }  // namespace
 
-static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, int kind, cudaStream_t st,
-                                  fv_precond **out) {
-    fv_csr *A = const_cast<fv_csr *>(Ac);
-    if (!A || !perm_host || !out || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
+// B = Q A Q^T (B's row i is A's row perm[i], columns renumbered and sorted):
+// its pattern, the permutation on the device and amap (A's entry k sits at
+// B's entry amap[k]); B's values are not filled.
+static fv_status build_permuted(fv_csr *A, const int32_t *perm_host, cudaStream_t st, fv_csr **Bout,
+                                int32_t **perm_out, int32_t **amap_out) {
+    if (!A || !perm_host || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
     const int64_t n = A->nrows, nnz = A->nnz;
     fv_csr *B = new (std::nothrow) fv_csr();
     if (!B) return FV_ERR_ALLOC;
@@ -2326,7 +2389,7 @@ static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, in
     if (bad) cudaFreeAsync(bad, st);
     if (scan_tmp) cudaFreeAsync(scan_tmp, st);
     if (e != cudaSuccess || hbad) {
-        if (e != cudaSuccess) fv_internal_set_cuda_error(e, "reordered factorisation");
+        if (e != cudaSuccess) fv_internal_set_cuda_error(e, "matrix permutation");
         if (hbad & 1) fv_internal_set_error_text("perm is not a permutation of 0..n-1");
         if (hbad & 2) fv_internal_set_error_text("a row has more than 32 entries");
         cudaFree(perm);
@@ -2335,6 +2398,21 @@ static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, in
         if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
         return (hbad & 2) ? FV_ERR_UNSUPPORTED : FV_ERR_INVALID;
     }
+    *Bout = B;
+    *perm_out = perm;
+    *amap_out = amap;
+    return FV_OK;
+}
+
+static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, int kind, cudaStream_t st,
+                                  fv_precond **out) {
+    fv_csr *A = const_cast<fv_csr *>(Ac);
+    if (!A || !perm_host || !out || A->nrows != A->ncols || A->nrows <= 0) return FV_ERR_INVALID;
+    const int64_t n = A->nrows;
+    fv_csr *B = nullptr;
+    int32_t *perm = nullptr, *amap = nullptr;
+    FV_TRY(build_permuted(A, perm_host, st, &B, &perm, &amap));
+    cudaError_t e = cudaSuccess;
     fv_precond tmp;  // scatter through a stand-in so the values are in place before factorising
     tmp.fill = B;
     tmp.orig = A;
@@ -2344,6 +2422,7 @@ static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, in
     tmp.amap = nullptr;
     fv_precond *P = nullptr;
     if (s == FV_OK) s = factor_common(B, kind, st, &P);
+    if (s == FV_OK) P->schedule = 1;  // the reordered sweeps have their own kernels (P->perm)
     if (s == FV_OK) {
         e = cudaMalloc(&P->zint, sizeof(double) * n);
         if (e == cudaSuccess) e = cudaMemsetAsync(P->zint, 0xFF, sizeof(double) * n, st);
@@ -2365,6 +2444,65 @@ static fv_status perm_factor_impl(const fv_csr *Ac, const int32_t *perm_host, in
     P->amap = amap;
     P->perm = perm;
     *out = P;
+    return FV_OK;
+}
+
+namespace {
+// y[i] = x[perm[i]] (to the permuted numbering) or y[perm[i]] = x[i] (back)
+__global__ void k_vec_permute(int64_t n, const int32_t *__restrict__ perm, const double *__restrict__ x,
+                              double *__restrict__ y, int back) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (back)
+            y[perm[i]] = x[i];
+        else
+            y[i] = x[perm[i]];
+    }
+}
+}  // namespace
+
+static fv_status csr_permute_impl(const fv_csr *Ac, const int32_t *perm_host, cudaStream_t st, fv_csr **out) {
+    fv_csr *A = const_cast<fv_csr *>(Ac);
+    if (!A || !out || A->perm_src) return FV_ERR_INVALID;
+    fv_csr *B = nullptr;
+    int32_t *perm = nullptr, *amap = nullptr;
+    FV_TRY(build_permuted(A, perm_host, st, &B, &perm, &amap));
+    B->perm_src = A;
+    B->perm = perm;
+    B->perm_amap = amap;
+    if (A->nnz) fv_note_launch(), k_scatter_vals<<<592, 256, 0, st>>>(A->nnz, amap, A->vals, B->vals);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fv_internal_set_cuda_error(e, "fv_csr_permute");
+        fv_csr_destroy(B);
+        return FV_ERR_CUDA;
+    }
+    *out = B;
+    return FV_OK;
+}
+
+extern "C" fv_status fv_csr_permute(const fv_csr *A, const int32_t *perm, void *stream, fv_csr **out) {
+    if (!out) return FV_ERR_INVALID;
+    *out = nullptr;
+    return fv_host_guard([&] { return csr_permute_impl(A, perm, fv_stream(stream), out); });
+}
+
+extern "C" fv_status fv_csr_permute_values(fv_csr *B, void *stream) {
+    if (!B || !B->perm_src || !B->perm_amap) return FV_ERR_INVALID;
+    cudaStream_t st = fv_stream(stream);
+    if (B->perm_src->nnz)
+        fv_note_launch(), k_scatter_vals<<<592, 256, 0, st>>>(B->perm_src->nnz, B->perm_amap, B->perm_src->vals,
+                                                               B->vals);
+    FV_CUDA_TRY(cudaGetLastError());
+    return FV_OK;
+}
+
+extern "C" fv_status fv_vec_permute(const fv_csr *B, const double *x, double *y, int32_t back, void *stream) {
+    if (!B || !B->perm || !x || !y || x == y) return FV_ERR_INVALID;
+    const int64_t n = B->nrows;
+    const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8));
+    fv_note_launch(), k_vec_permute<<<G, 256, 0, fv_stream(stream)>>>(n, B->perm, x, y, back ? 1 : 0);
+    FV_CUDA_TRY(cudaGetLastError());
     return FV_OK;
 }
 

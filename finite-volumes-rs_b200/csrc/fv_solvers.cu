@@ -92,6 +92,8 @@ extern "C" fv_status fv_csr_destroy(fv_csr *A) {
         cudaFree(A->cols);
     }
     cudaFree(A->vals);
+    cudaFree(A->perm);
+    cudaFree(A->perm_amap);
     fv_symbolic_free(A->sym);
     delete A;
     return FV_OK;

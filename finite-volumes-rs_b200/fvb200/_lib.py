@@ -174,6 +174,9 @@ _SIGS = {
                                   P(OrderInfo)],
     "fv_order_boxes": [vp, C.c_int32, P(i64), C.c_int32, ip, P(OrderInfo), vp],
     "fv_order_boxes_levels": [vp, C.c_int32, ip, ip, P(OrderInfo), vp],
+    "fv_csr_permute": [vp, ip, vp, P(vp)],
+    "fv_csr_permute_values": [vp, vp],
+    "fv_vec_permute": [vp, vp, vp, C.c_int32, vp],
     "fv_order_boxes_host_levels": [i64, C.c_int32, dp, i64, dp, dp, ip, ip, C.c_int32, ip, ip, P(OrderInfo)],
     "fv_batch_create": [vp, C.c_int32, P(i64), C.c_int32, vp, P(vp)],
     "fv_batch_cg": [vp, vp, vp, vp, P(BatchOptions), P(BatchInfo), vp],

@@ -172,6 +172,36 @@ class DistributedMatrix:
         x = _dev_f64(rhs)
         check(lib().fv_spmv(self.handle, C.c_void_p(x.data_ptr()), result.ptr(), stream_handle(stream)), "fv_spmv")
 
+    def permuted(self, perm, stream=None) -> "DistributedMatrix":
+        """Q A Q^T (fv_csr_permute): row i is this matrix's row perm[i], columns
+        renumbered the same way.  The copy keeps this matrix alive and takes its
+        current values again with refresh_permuted()."""
+        p = np.ascontiguousarray(perm, np.int32)
+        if p.shape != (self.nrows(),):
+            raise ValueError("perm needs one entry per row")
+        h = C.c_void_p()
+        check(lib().fv_csr_permute(self.handle, p.ctypes.data_as(C.POINTER(C.c_int32)), stream_handle(stream),
+                                   C.byref(h)), "fv_csr_permute")
+        B = DistributedMatrix(h, keepalive=self)
+        B.perm = p
+        return B
+
+    def refresh_permuted(self, stream=None) -> None:
+        """A permuted copy takes the current values of the matrix it was made from."""
+        check(lib().fv_csr_permute_values(self.handle, stream_handle(stream)), "fv_csr_permute_values")
+
+    def to_permuted(self, x, out: "DistributedVector", stream=None) -> None:
+        """out[i] = x[perm[i]]: a vector of the source numbering in this permuted copy's numbering."""
+        xs = _dev_f64(x)
+        check(lib().fv_vec_permute(self.handle, C.c_void_p(xs.data_ptr()), out.ptr(), 0, stream_handle(stream)),
+              "fv_vec_permute")
+
+    def from_permuted(self, y, out: "DistributedVector", stream=None) -> None:
+        """out[perm[i]] = y[i]: back to the source numbering."""
+        ys = _dev_f64(y)
+        check(lib().fv_vec_permute(self.handle, C.c_void_p(ys.data_ptr()), out.ptr(), 1, stream_handle(stream)),
+              "fv_vec_permute")
+
     def close(self):
         if self.handle:
             lib().fv_csr_destroy(self.handle)
@@ -356,9 +386,10 @@ class Preconditioner:
     def schedule(self, request: int = -1):
         """Sweep schedule: request -1 = query, 0 or 1 = level chunks (default),
         2 = box tiles (matrices assembled on a mesh), 3 = level chunks with
-        the next chunk prefetched.  Returns (active, stats) with active 1, 2
-        or 3 and stats = (box edge in cell sizes, boxes, lane use fwd/bwd,
-        ring share fwd/bwd)."""
+        the next chunk prefetched, 4 = consecutive rows (the default when the
+        rows are sorted by level, e.g. a matrix permuted by order_boxes'
+        order).  Returns (active, stats) with active 1..4 and stats = (box
+        edge in cell sizes, boxes, lane use fwd/bwd, ring share fwd/bwd)."""
         act = C.c_int32()
         st = np.zeros(6)
         check(lib().fv_precond_schedule(self.handle, int(request), C.byref(act),

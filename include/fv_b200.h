@@ -353,10 +353,14 @@ fv_status fv_precond_export(const fv_precond *P, int64_t *nnz, int32_t *row_ptr,
 fv_status fv_precond_levels(const fv_precond *P, int32_t *fwd_level, int32_t *bwd_level,
                             int32_t *n_fwd_levels, int32_t *n_bwd_levels, void *stream);
 /* Sweep schedule of P.  request: -1 query only; 0 or 1 level chunks (the
- * default); 2 box tiles, available when the matrix was assembled on a mesh
- * whose box order exists (FV_ERR_UNSUPPORTED otherwise); 3 level chunks with
- * each warp loading its next chunk's rows before waiting on the current one.
- * *active receives 1, 2 or 3.  stats (optional, 6 doubles): box edge
+ * default for rows not sorted by level); 2 box tiles, available when the
+ * matrix was assembled on a mesh whose box order exists (FV_ERR_UNSUPPORTED
+ * otherwise); 3 level chunks with each warp loading its next chunk's rows
+ * before waiting on the current one; 4 consecutive rows in index order, block
+ * tickets (the default when the factorised matrix's rows are already sorted
+ * by forward level, e.g. a matrix permuted by fv_order_boxes' order; any
+ * level-0 factorisation accepts it, FV_ERR_UNSUPPORTED for reordered or fill
+ * factorisations).  *active receives 1, 2, 3 or 4.  stats (optional, 6 doubles): box edge
  * in mean cell sizes, number of boxes, lane use of the forward / backward
  * steps, share of dependencies read from shared memory forward / backward
  * (zeros without a tiling).  Both schedules give the same bits. */
@@ -557,6 +561,21 @@ fv_status fv_order_boxes_host_levels(int64_t n, int32_t dim, const double *cell_
                                      fv_order_info *info);
 fv_status fv_order_boxes_levels(const fv_csr *A, int32_t rows_per_box, int32_t *perm, int32_t *level,
                                 fv_order_info *info, void *stream);
+
+/* A permuted copy B = Q A Q^T of a square matrix: B's row i is A's row
+ * perm[i] (host array of n entries, a permutation; FV_ERR_INVALID otherwise),
+ * columns renumbered the same way and sorted.  With perm from fv_order_boxes,
+ * B's rows are sorted by level and its IC(0)/ILU(0) (fv_ic0_factor /
+ * fv_ilu0_factor on B) sweeps consecutive rows (schedule 4) with no gather or
+ * scatter: solving B y = Q b and x = Q^T y is the reordered perf mode without
+ * the permutation inside every preconditioner apply.  No counterpart in the
+ * reference.  B keeps a pointer to A (A must outlive B);
+ * fv_csr_permute_values copies A's current values into B (after A is
+ * re-assembled), fv_vec_permute maps vectors: back = 0: y[i] = x[perm[i]];
+ * back = 1: y[perm[i]] = x[i] (x and y distinct device vectors of n). */
+fv_status fv_csr_permute(const fv_csr *A, const int32_t *perm, void *stream, fv_csr **B);
+fv_status fv_csr_permute_values(fv_csr *B, void *stream);
+fv_status fv_vec_permute(const fv_csr *B, const double *x, double *y, int32_t back, void *stream);
 
 /* Allocation-free conjugate gradient.  No counterpart in the reference crate.
  *
