@@ -105,11 +105,29 @@ namespace {
 constexpr int RB = 256;  // block size of every reduction kernel
 
 // Row dot: y_i = sum_k a_k x_col(k), left to right from 0.0 (dmatrix.rs:138-145).
+// The first 8 entries' column, value and x loads are all issued before the
+// sum starts (the x gathers of a row are independent), the sum still runs in
+// entry order.
 __device__ __forceinline__ double row_dot(const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                           const double *__restrict__ val, const double *__restrict__ x, int64_t i) {
+    constexpr int E = 8;
+    const int k0 = ptr[i], k1 = ptr[i + 1];
+    const int len = k1 - k0;
+    double av[E], xv[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        av[q] = 0.0;
+        xv[q] = 0.0;
+        if (q < len) {
+            av[q] = val[k0 + q];
+            xv[q] = __ldg(&x[col[k0 + q]]);
+        }
+    }
     double s = 0.0;
-    const int k1 = ptr[i + 1];
-    for (int k = ptr[i]; k < k1; ++k) s += val[k] * __ldg(&x[col[k]]);
+#pragma unroll
+    for (int q = 0; q < E; ++q)
+        if (q < len) s += av[q] * xv[q];
+    for (int k = k0 + E; k < k1; ++k) s += val[k] * __ldg(&x[col[k]]);
     return s;
 }
 
