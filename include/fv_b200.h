@@ -563,8 +563,9 @@ fv_status fv_order_boxes_levels(const fv_csr *A, int32_t rows_per_box, int32_t *
                                 fv_order_info *info, void *stream);
 
 /* A permuted copy B = Q A Q^T of a square matrix: B's row i is A's row
- * perm[i] (host array of n entries, a permutation; FV_ERR_INVALID otherwise),
- * columns renumbered the same way and sorted.  With perm from fv_order_boxes,
+ * perm[i] (host array of n entries, a permutation; FV_ERR_INVALID otherwise;
+ * rows of more than 32 entries: FV_ERR_UNSUPPORTED), columns renumbered the
+ * same way and sorted.  With perm from fv_order_boxes,
  * B's rows are sorted by level and its IC(0)/ILU(0) (fv_ic0_factor /
  * fv_ilu0_factor on B) sweeps consecutive rows (schedule 4) with no gather or
  * scatter: solving B y = Q b and x = Q^T y is the reordered perf mode without
