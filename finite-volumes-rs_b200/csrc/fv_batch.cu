@@ -107,31 +107,12 @@ __device__ __forceinline__ void retire(BProb &s, BGlobal *G) {
 }
 
 // Row dot y_i = sum_k a_k x_col(k), left to right from 0 (dmatrix.rs:138-145).
-// The first 8 entries of the row are loaded before any is summed -- all their
-// column, value and x loads in flight at once -- which matters for FP32, whose
-// rows carry too few bytes to keep HBM busy one dependent load at a time; the
-// sum still runs in entry order.
 template <typename T>
 __device__ __forceinline__ T row_dot_t(const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
                                        const T *__restrict__ val, const T *__restrict__ x, int64_t i) {
-    constexpr int E = 8;
-    const int k0 = ptr[i], k1 = ptr[i + 1];
-    const int len = k1 - k0;
-    T av[E], xv[E];
-#pragma unroll
-    for (int q = 0; q < E; ++q) {
-        av[q] = T(0);
-        xv[q] = T(0);
-        if (q < len) {
-            av[q] = val[k0 + q];
-            xv[q] = __ldg(&x[col[k0 + q]]);
-        }
-    }
     T s = T(0);
-#pragma unroll
-    for (int q = 0; q < E; ++q)
-        if (q < len) s += av[q] * xv[q];
-    for (int k = k0 + E; k < k1; ++k) s += val[k] * __ldg(&x[col[k]]);
+    const int k1 = ptr[i + 1];
+    for (int k = ptr[i]; k < k1; ++k) s += val[k] * __ldg(&x[col[k]]);
     return s;
 }
 
