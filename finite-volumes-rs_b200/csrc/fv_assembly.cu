@@ -85,8 +85,9 @@ struct AssembleArgs {
     const double *prev, *prev2, *dens, *densp, *densp2;
     double c_lin, c_div;
     const double *lin, *divflux;
-    // Orthogonal scheme with the mesh's cached geometry: 1/|d| per face, volume per cell
-    const double *invd, *vol;
+    // Orthogonal scheme with the mesh's cached geometry: (area, 1/|d|) per face, volume per cell
+    const double2 *geo;
+    const double *vol;
 };
 
 // Cell terms of the expression (assembly.rs:26-32): lhs and rhs per unit
@@ -450,7 +451,7 @@ __device__ __forceinline__ int unpad(int (&jj)[MAXF]) {
 // neighbour-side bit, the other cell or -1), deg of them.
 //
 // GEO (Orthogonal scheme only): 1/|d| of every face comes from the mesh's
-// cached a.invd (k_face_invd: the same expression, evaluated once per face) and
+// cached a.geo (k_face_invd: the same expression, evaluated once per face) and
 // the cell's volume is V, so no cell centre is gathered.
 template <int DIM, int MAXF, bool CORR, bool GEO = false>
 __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, bool live, const int (&fe)[MAXF],
@@ -465,12 +466,16 @@ __device__ __forceinline__ void row_values(const AssembleArgs &a, int64_t i, boo
         ar[k] = kp[k] = fl[k] = tv[k] = 0.0;
         if (k < deg) {
             const int f = fe[k] & 0x7fffffff;
-            ar[k] = a.area[f];
+            if (GEO) {
+                const double2 g = a.geo[f];  // area and 1/|d| in one load
+                ar[k] = g.x;
+                tv[k] = g.y;
+            } else {
+                ar[k] = a.area[f];
+            }
             if (a.c_lap != 0.0) kp[k] = a.kappa[f];
             if (a.c_conv != 0.0) fl[k] = a.flux[f];
-            if (GEO) {
-                tv[k] = a.invd[f];
-            } else {
+            if (!GEO) {
                 const double4 o = jj[k] >= 0 ? a.cell[jj[k]] : a.bfc[f - a.fb0];
                 oc[k] = make_double3(o.x, o.y, o.z);
             }
@@ -731,7 +736,8 @@ __global__ void __launch_bounds__(kAsmBlock, MINB) k_assemble_pipe(AssembleArgs 
 // volumes: the Orthogonal scheme's geometry, cached on the mesh.
 template <int DIM>
 __global__ void k_face_invd(int64_t nf, int64_t fb0, const int2 *__restrict__ fc, const double4 *__restrict__ cell,
-                            const double4 *__restrict__ bfc, double *__restrict__ invd) {
+                            const double4 *__restrict__ bfc, const double *__restrict__ area,
+                            double2 *__restrict__ geo) {
     for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x) {
         const int2 oc = fc[f];
         const double4 o = cell[oc.x];
@@ -746,7 +752,7 @@ __global__ void k_face_invd(int64_t nf, int64_t fb0, const int2 *__restrict__ fc
             dd = pj.z - pi.z;
             d2 += dd * dd;
         }
-        invd[f] = 1.0 / sqrt(d2);
+        geo[f] = make_double2(area[f], 1.0 / sqrt(d2));
     }
 }
 
@@ -777,7 +783,7 @@ void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
         const size_t smem = sizeof(double) * B * (MAXF + 1);
         if (a.grad) {
             fv_note_launch(), k_assemble_reg<DIM, MAXF, true><<<G, B, smem, st>>>(a);
-        } else if (a.cf_pad && a.invd) {
+        } else if (a.cf_pad && a.geo) {
             // 6 blocks/SM at 80 registers measured fastest for tets (8 at 64 spills and is 23 % slower)
             launch_pipe<DIM, MAXF, MAXF <= 4 ? 6 : 3>(a, G, smem, st);
         } else if (a.cf_pad) {
@@ -870,7 +876,7 @@ extern "C" fv_status fv_mesh_destroy(fv_mesh *m) {
     cudaFree(m->gcf_face);
     cudaFree(m->gcoef);
     cudaFree(m->gdiag);
-    cudaFree(m->face_invd);
+    cudaFree(m->face_geo);
     cudaFree(m->cell_vol);
     cudaFree(m->row_ptr);
     cudaFree(m->cols);
@@ -1093,18 +1099,19 @@ static fv_status build_pattern(fv_mesh *m, cudaStream_t st) {
 static fv_status ensure_orth_geometry(fv_mesh *m, cudaStream_t st) {
     static std::mutex lock;
     std::lock_guard<std::mutex> g(lock);
-    if (m->face_invd && m->cell_vol) return FV_OK;
-    double *invd = nullptr, *vol = nullptr;
-    cudaError_t e = cudaMalloc(&invd, sizeof(double) * (m->n_faces ? m->n_faces : 1));
+    if (m->face_geo && m->cell_vol) return FV_OK;
+    double2 *geo = nullptr;
+    double *vol = nullptr;
+    cudaError_t e = cudaMalloc(&geo, sizeof(double2) * (m->n_faces ? m->n_faces : 1));
     if (e == cudaSuccess) e = cudaMalloc(&vol, sizeof(double) * (m->n_cells ? m->n_cells : 1));
     if (e == cudaSuccess && m->n_faces) {
         const unsigned G = (unsigned)std::min<int64_t>((m->n_faces + 255) / 256, 148 * 16);
         if (m->dim == 2)
             fv_note_launch(), k_face_invd<2><<<G, 256, 0, st>>>(m->n_faces, m->n_faces - m->n_bfaces, m->face_cells,
-                                                                 m->cell, m->bface_center, invd);
+                                                                 m->cell, m->bface_center, m->face_area, geo);
         else
             fv_note_launch(), k_face_invd<3><<<G, 256, 0, st>>>(m->n_faces, m->n_faces - m->n_bfaces, m->face_cells,
-                                                                 m->cell, m->bface_center, invd);
+                                                                 m->cell, m->bface_center, m->face_area, geo);
     }
     if (e == cudaSuccess && m->n_cells) {
         const unsigned G = (unsigned)std::min<int64_t>((m->n_cells + 255) / 256, 148 * 16);
@@ -1113,12 +1120,12 @@ static fv_status ensure_orth_geometry(fv_mesh *m, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
-        cudaFree(invd);
+        cudaFree(geo);
         cudaFree(vol);
         fv_internal_set_cuda_error(e, "fv_assemble geometry");
         return e == cudaErrorMemoryAllocation ? FV_ERR_ALLOC : FV_ERR_CUDA;
     }
-    m->face_invd = invd;
+    m->face_geo = geo;
     m->cell_vol = vol;
     return FV_OK;
 }
@@ -1212,11 +1219,11 @@ extern "C" fv_status fv_assemble(fv_mesh *m, const fv_terms_desc *terms, const f
     } else if (terms->scheme != FV_SCHEME_ORTHOGONAL && terms->scheme != FV_SCHEME_CORRECTED) {
         return FV_ERR_INVALID;
     }
-    args.invd = nullptr;
+    args.geo = nullptr;
     args.vol = nullptr;
     if (!args.grad && m->cf_pad) {
         FV_TRY(ensure_orth_geometry(m, st));
-        args.invd = m->face_invd;
+        args.geo = m->face_geo;
         args.vol = m->cell_vol;
     }
     const int mf = m->maxf;

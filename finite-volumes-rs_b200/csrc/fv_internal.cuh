@@ -89,9 +89,9 @@ struct fv_mesh {
     double4 *gcoef = nullptr;          // gradient coefficient of each (cell, face) in that order
     double4 *gdiag = nullptr;          // gradient coefficient of the cell itself
     // Orthogonal-scheme geometry cached on the first assembly that uses it:
-    // 1/|d| per face (owner centre to neighbour centre or boundary face centre)
-    // and the cells' volumes
-    double *face_invd = nullptr;
+    // (area, 1/|d|) per face (|d| from the owner centre to the neighbour centre
+    // or boundary face centre) and the cells' volumes
+    double2 *face_geo = nullptr;
     double *cell_vol = nullptr;
     // CSR pattern of cell_to_cell (built on the first assemble)
     int32_t *row_ptr = nullptr;
