@@ -902,6 +902,33 @@ def serve_arm(args, rank, world, local_rank):
     stats = srv.run(reqs, time_limit=cap, drain=False)
     launches = lib().fv_launch_count() - L0
     clocks = clk.stop()
+    # the same server below its capacity: latency of a request that does not queue behind thousands
+    sustain = None
+    if args.serve_sustain_rate > 0:
+        sreqs = request_stream(rate=args.serve_sustain_rate, duration=args.serve_sustain_duration,
+                               seed=4048 + rank)
+        for r in sreqs:
+            if r.kind == "2d":
+                r.side = max(16, int(round(r.side / 16.0)) * 16)
+                r.cells = 2 * r.side ** 2
+            else:
+                r.side = max(4, int(round(r.side / 4.0)) * 4)
+                r.cells = 6 * r.side ** 3
+        srv2 = Server(fv, workers=args.serve_workers, max_wave_cells=wave_cells,
+                      max_wave_requests=args.serve_wave_requests, wave_order=args.serve_wave_order,
+                      solve_fn=functools.partial(solve_wave, precision=args.serve_precision, ordering=ordering),
+                      refill=bool(args.serve_refill),
+                      run_fn=functools.partial(WaveRun, precision=args.serve_precision, ordering=ordering))
+        srv2.cache = srv.cache
+        clk2 = Clocks(local_rank, "_sustain")
+        clk2.start()
+        s2 = srv2.run(sreqs, time_limit=args.serve_sustain_duration + 60.0, warm=False, drain=True)
+        sustain = {"arrival_rate_per_s": args.serve_sustain_rate, "arrival_window_s": args.serve_sustain_duration,
+                   "requests": len(sreqs), "completed": s2["completed"], "failed": s2["failed"],
+                   "backlog": s2["backlog"], "solves_per_s": round(s2["solves_per_s"], 3),
+                   "p50_ms": round(s2["p50_ms"], 1) if s2["p50_ms"] is not None else None,
+                   "p99_ms": round(s2["p99_ms"], 1) if s2["p99_ms"] is not None else None,
+                   "waves": s2["waves"], "refills": s2["refills"], "clocks": clk2.stop()}
     # plain FP64 per-request path on a sample of the same requests, stratified by
     # size: per kind, the requests at evenly spaced quantiles of the cell count
     sample = []
@@ -956,6 +983,7 @@ def serve_arm(args, rank, world, local_rank):
         "plain_fp64_solves_per_s": round(plain_rate, 3),
         "plain_sample": f"{len(sample)} requests at evenly spaced size quantiles per kind, one at a time, rtol 1e-8",
         "speedup_vs_plain_fp64": round(stats["solves_per_s"] / plain_rate, 2) if plain_rate > 0 else None,
+        "below_capacity": sustain,
         "gpu_launches": int(launches), "clocks": clocks, "mesh_build_s": round(t_mesh, 1),
     }
     return line
@@ -1029,6 +1057,9 @@ def main():
                     help="cells per wave (0: 24M with slot refill, 48M with whole waves)")
     ap.add_argument("--serve-wave-requests", type=int, default=512)
     ap.add_argument("--serve-wave-order", default="size", choices=["size", "fifo"])
+    ap.add_argument("--serve-sustain-rate", type=float, default=20.0,
+                    help="a second served run at this arrival rate (below capacity) for unqueued latency; 0: skip")
+    ap.add_argument("--serve-sustain-duration", type=float, default=30.0)
     ap.add_argument("--serve-refill", type=int, default=1, choices=[0, 1],
                     help="1: slot refill (running waves take newly admitted requests); 0: whole waves")
     ap.add_argument("--serve-time-limit", type=float, default=0.0,
