@@ -777,6 +777,7 @@ void launch_pipe(const AssembleArgs &a, unsigned G, size_t smem, cudaStream_t st
 
 template <int DIM, int MAXF>
 void launch_assemble(const AssembleArgs &a, cudaStream_t st) {
+    if (a.n <= 0) return;  // no rows: nothing to launch
     const int B = kAsmBlock;
     const unsigned G = (unsigned)((a.n + B - 1) / B);
     if constexpr (MAXF <= 8) {
