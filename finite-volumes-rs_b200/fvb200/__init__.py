@@ -11,7 +11,7 @@ from .linalg import (  # noqa: F401
     DiagonalPreconditioner, DistributedMatrix, DistributedVector, IdentityPreconditioner, IncompleteCholesky,
     IncompleteLowerUpper,
     LinearSolverInfo, LinearSolverOptions, assemble, bi_conjugate_gradient_stab, compute_gradients,
-    conjugate_gradient, merge_orders, order_boxes, order_boxes_host,
+    PermutedSystem, conjugate_gradient, merge_orders, order_boxes, order_boxes_host,
 )
 from .bcs import FaceConstraints  # noqa: F401
 from .mesh import DeviceMesh, Mesh  # noqa: F401

@@ -668,3 +668,52 @@ def bi_conjugate_gradient_stab(solution: DistributedVector, lhs: DistributedMatr
                                comm=None, options: LinearSolverOptions | None = None,
                                stream=None) -> LinearSolverInfo:
     return _solve(lib().fv_bicgstab, "BiConjugateGradientStab", solution, lhs, rhs, preconditioner, options, stream)
+
+
+class PermutedSystem:
+    """The box-colour order as a permuted system: B = Q A Q^T (rows sorted by
+    level) factorised with IC(0) ("ic") or ILU(0) ("ilu") and solved in its
+    own numbering; b is permuted in and x back on every solve, so callers
+    keep A's numbering.  After A is re-assembled, refresh() takes its new
+    values and refactorises.  perm: an explicit permutation instead of
+    order_boxes' (any permutation; the sweeps are fastest when it sorts the
+    rows by level)."""
+
+    def __init__(self, A: DistributedMatrix, kind: str = "ilu", perm=None, stream=None):
+        if kind not in ("ic", "ilu"):
+            raise ValueError(f"kind must be 'ic' or 'ilu', not {kind!r}")
+        if perm is None:
+            perm, self.order_info = order_boxes(A, stream=stream)
+        else:
+            self.order_info = None
+        self.kind = kind
+        self.A = A
+        self.B = A.permuted(perm, stream=stream)
+        cls = IncompleteCholesky if kind == "ic" else IncompleteLowerUpper
+        self.P = cls.from_matrix(self.B, 0, stream=stream)
+        n = A.nrows()
+        self._b = DistributedVector.from_size(n)
+        self._y = DistributedVector.from_size(n)
+
+    @property
+    def perm(self):
+        return self.B.perm
+
+    def refresh(self, stream=None) -> None:
+        """Take A's current values (after a re-assembly) and refactorise."""
+        self.B.refresh_permuted(stream=stream)
+        self.P.refactor(stream=stream)
+
+    def solve(self, solution: DistributedVector, rhs, options: LinearSolverOptions | None = None,
+              initial_guess: bool = True, stream=None) -> LinearSolverInfo:
+        """CG (IC) or BiCGStab (ILU) on B y = Q rhs from y0 = Q solution
+        (initial_guess) or 0; solution = Q^T y."""
+        self.B.to_permuted(rhs, self._b, stream=stream)
+        if initial_guess:
+            self.B.to_permuted(solution.data, self._y, stream=stream)
+        else:
+            self._y.data.zero_()
+        fn = conjugate_gradient if self.kind == "ic" else bi_conjugate_gradient_stab
+        info = fn(self._y, self.B, self._b, self.P, None, options, stream=stream)
+        self.B.from_permuted(self._y, solution, stream=stream)
+        return info

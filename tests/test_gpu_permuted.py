@@ -131,3 +131,34 @@ def test_permuted_rejects_non_permutation(fv):
         A.permuted(bad)
     with pytest.raises(ValueError):
         A.permuted(np.arange(n - 1, dtype=np.int32))
+
+
+def test_permuted_system_helper(fv, orc):
+    """fvb200.PermutedSystem: the same bits as the steps done by hand, and a
+    refresh after re-assembly gives the solve of the new system."""
+    kind, case = _case(fv, 1, n=12)
+    A, b = fv.assemble(equation(fv, case), (case["bndi"], case["bnde"]), case["mesh"])
+    n = A.nrows()
+    opts = fv.LinearSolverOptions(1e-8, 1e-8, 5000)
+    S = fv.PermutedSystem(A, "ilu")
+    assert S.P.schedule()[0] == 4 and S.order_info["n_colours"] == 2
+    x = fv.DistributedVector.from_size(n)
+    info = S.solve(x, b, opts, initial_guess=False)
+    A2, b2, perm2, B2 = _permuted(fv, case)
+    P2 = fv.IncompleteLowerUpper.from_matrix(B2, 0)
+    bq = fv.DistributedVector.from_size(n)
+    B2.to_permuted(b2, bq)
+    y = fv.DistributedVector.from_size(n)
+    info2 = fv.bi_conjugate_gradient_stab(y, B2, bq, P2, None, opts)
+    x2 = fv.DistributedVector.from_size(n)
+    B2.from_permuted(y, x2)
+    assert info.iterations == info2.iterations and np.array_equal(x.numpy(), x2.numpy())
+    # new values: refresh, then solve from the previous solution
+    case2 = dict(case, kappa=case["kappa"] * 1.3)
+    _, b3 = fv.assemble(equation(fv, case2), (case2["bndi"], case2["bnde"]), case2["mesh"], lhs=A)
+    S.refresh()
+    S.solve(x, b3, opts)
+    ptr, cols, vals, rhs = oracle_system(orc, case2)
+    import scipy.sparse as sp
+    Ah = sp.csr_matrix((vals, cols, ptr))
+    assert np.linalg.norm(rhs - Ah @ x.numpy()) <= 1.01e-8 * np.linalg.norm(rhs)
