@@ -1158,7 +1158,9 @@ def main():
         other = "natural" if ordering is not None else "boxes"
         ro = measure_single(ctx, None if other == "natural" else other, max(3, K // 4), 2, e2e=False, kernels=True)
         x_gpu[other] = ro["x"]
-        line["orderings"] = {args.ordering: single_summary(res, world, f"{wl['solver']}, {args.ordering} order, FP64"),
+        head_label = f"{wl['solver']}, {args.ordering} order" + (
+            " as the permuted system" if ordering is not None and args.reorder == "system" else "") + ", FP64"
+        line["orderings"] = {args.ordering: single_summary(res, world, head_label),
                              other: single_summary(ro, world, f"{wl['solver']}, {other} order, FP64")}
         del ro
         if ordering is not None:  # the box order's other form
